@@ -1,0 +1,479 @@
+"""ORACLE — test infrastructure, not product code.
+
+ctypes front end for the CPU restatement (liboracle.so, built from dd_oracle.c)
+and for the reference's own code built from source (oracle/_ref/libref_cpu.so,
+oracle/_ref/libref_gpu_sb<W>.so).  Only tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline / reference legs import this module, as the checker.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+# Arithmetic variants (dd_oracle.h).  PINNED_* are the forms that reproduce the
+# reference builds; tests/test_oracle_pin.py re-establishes them.
+FMA_DM = 1
+RECIP_TSAMP = 2
+RECIP_1349 = 4
+FMA_VAR = 8
+FMA_ZDM = 16
+CPU_EXPAND = 32
+CPU_EXPFMA = 64
+
+_c_int, _c_long, _c_float, _c_double = ctypes.c_int, ctypes.c_long, ctypes.c_float, ctypes.c_double
+_P = ctypes.c_void_p
+
+_lib = None
+
+
+def _np_dtype(nbits: int):
+    return {8: np.uint8, 16: np.uint16, 32: np.uint32}[nbits]
+
+
+def lib():
+    """Load (building on demand when a compiler is present) liboracle.so."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = os.path.join(HERE, "liboracle.so")
+    if not os.path.exists(path):
+        import subprocess
+
+        subprocess.run(["make", "-C", HERE, "oracle"], check=True, capture_output=True)
+    L = ctypes.CDLL(path)
+    sig = {
+        "orc_freq_table_header": (None, [_c_float, _c_float, _c_int, _P]),
+        "orc_freq_table_fil": (None, [_c_double, _c_double, _c_int, _P]),
+        "orc_chan_range": (_c_int, [_P, _c_int, _c_float, _c_float, _P, _P]),
+        "orc_dm_steps": (_c_long, [_c_float, _c_float, _c_float]),
+        "orc_subband_tables_ieee": (None, [_P, _c_long, _c_long, _c_float, _c_float, _c_long,
+                                           _c_int, _c_int, _c_double, _c_int, _c_int, _P, _P]),
+        "orc_delay_table_fp64": (None, [_P, _c_long, _c_long, _c_float, _c_float, _c_long,
+                                        _c_double, _c_int, _P]),
+        "orc_cpu_delay_table": (None, [_P, _c_long, _c_long, _c_float, _c_float, _c_long,
+                                       _c_double, _c_int, _P]),
+        "orc_bruteforce_cpu": (_c_int, [_P, _c_int, _c_long, _c_int, _P, _c_double, _c_float,
+                                        _c_float, _c_float, _c_float, _c_float, _c_int, _c_float,
+                                        _c_int, _P, _P, _c_long, _P, _P, _c_long, _P]),
+        "orc_subband_sums": (_c_int, [_P, _c_int, _c_long, _c_int, _c_long, _c_long, _c_int,
+                                      _c_int, _c_long, _P, _P, _P]),
+        "orc_time_binning": (_c_int, [_P, _c_int, _c_long, _c_int, _c_int, _P]),
+        "orc_iqrm_windows": (_c_int, [_c_double, _c_double, _c_int, _c_double, ctypes.c_uint,
+                                      _P, _P, _c_int]),
+        "orc_iqrm_window_mask": (_c_int, [_P, _c_int, ctypes.c_uint, ctypes.c_uint,
+                                          ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, _c_int,
+                                          _c_float, _c_float, _c_double, _c_int, _P]),
+        "orc_iqrm_lags": (_c_int, [_c_int, _c_double, _P, _c_int]),
+        "orc_apply_window_masks": (None, [_P, _c_int, ctypes.c_uint, ctypes.c_uint, _c_int, _P,
+                                          _P, _P]),
+        "orc_zero_dm_callsite": (None, [_P, _c_int, ctypes.c_size_t, ctypes.c_size_t,
+                                        ctypes.c_size_t, _c_int]),
+        "orc_zero_dm_range_exact": (None, [_P, _c_int, ctypes.c_uint, ctypes.c_uint,
+                                           ctypes.c_uint, ctypes.c_uint]),
+        "orc_mark_channels": (None, [_P, _c_int, ctypes.c_uint, ctypes.c_uint, _P, _c_int]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+# ---------------------------------------------------------------- plan scalars
+def freq_table_header(fch1: float, foff: float, nchans: int) -> np.ndarray:
+    f = np.zeros(nchans, np.float64)
+    lib().orc_freq_table_header(fch1, foff, nchans, _ptr(f))
+    return f
+
+
+def freq_table_fil(fch1: float, foff: float, nchans: int) -> np.ndarray:
+    f = np.zeros(nchans, np.float64)
+    lib().orc_freq_table_fil(fch1, foff, nchans, _ptr(f))
+    return f
+
+
+def chan_range(freq: np.ndarray, freq_start: float, freq_end: float):
+    cs, ce = _c_long(), _c_long()
+    rc = lib().orc_chan_range(_ptr(freq), len(freq), freq_start, freq_end, ctypes.byref(cs),
+                              ctypes.byref(ce))
+    if rc:
+        raise ValueError("frequency range outside the band")
+    return cs.value, ce.value
+
+
+def dm_steps(dm_low: float, dm_high: float, dm_step: float) -> int:
+    return int(lib().orc_dm_steps(dm_low, dm_high, dm_step))
+
+
+@dataclass
+class SubbandPlan:
+    chan_start: int
+    chan_end: int
+    dm_steps: int
+    nsamp: int
+    nsb: int
+    ndm_nom: int
+    sb_width: int
+    ndm0: int
+
+
+def subband_plan(freq, nsamp_in, dm_low, dm_high, freq_start, freq_end, dm_step, ds,
+                 sb_width=32, ndm0=32) -> SubbandPlan:
+    cs, ce = chan_range(freq, freq_start, freq_end)
+    steps = dm_steps(dm_low, dm_high, dm_step)
+    dch = ce - cs + 1
+    nsb = (dch + sb_width - 1) // sb_width
+    return SubbandPlan(cs, ce, steps, (nsamp_in + ds - 1) // ds, nsb, (steps + ndm0 - 1) // ndm0,
+                       sb_width, ndm0)
+
+
+def subband_tables_ieee(freq, plan: SubbandPlan, dm_low, dm_step, tsamp, ds, variant=FMA_DM):
+    dch = plan.chan_end - plan.chan_start + 1
+    d1 = np.zeros((plan.ndm_nom, dch), np.int32)
+    r2 = np.zeros((plan.dm_steps, plan.nsb), np.int32)
+    lib().orc_subband_tables_ieee(_ptr(freq), plan.chan_start, plan.chan_end, dm_low, dm_step,
+                                  plan.dm_steps, plan.sb_width, plan.ndm0, tsamp, ds, variant,
+                                  _ptr(d1), _ptr(r2))
+    return d1, r2
+
+
+def delay_table_fp64(freq, chan_start, chan_end, dm_low, dm_step, ndm, tsamp, ds):
+    d = np.zeros((ndm, chan_end - chan_start + 1), np.int32)
+    lib().orc_delay_table_fp64(_ptr(freq), chan_start, chan_end, dm_low, dm_step, ndm, tsamp, ds,
+                               _ptr(d))
+    return d
+
+
+def cpu_delay_table(freq, chan_start, chan_end, dm_low, dm_step, steps, tsamp, variant=0):
+    d = np.zeros((steps, chan_end - chan_start), np.int32)
+    lib().orc_cpu_delay_table(_ptr(freq), chan_start, chan_end, dm_low, dm_step, steps, tsamp,
+                              variant, _ptr(d))
+    return d
+
+
+# ---------------------------------------------------------------- dedispersion
+def bruteforce_cpu(data: np.ndarray, nchans: int, freq: np.ndarray, tsamp: float, dm_low,
+                   dm_high, freq_start, freq_end, dm_step, ds, t_sample, variant=0, delay=None):
+    """Raw slices of cpucal::dedispered_fil_omp; returns a list of [ndm, cols] uint64.
+    `delay` ([ndm, chan_end-chan_start] int32) replaces the computed table."""
+    data = np.ascontiguousarray(data)
+    nbits = data.dtype.itemsize * 8
+    ndata = data.size // nchans
+    steps = dm_steps(dm_low, dm_high, dm_step)
+    cap = steps * (ndata + 64) + 1024
+    out = np.zeros(cap, np.uint64)
+    cols = np.zeros(1 << 16, np.int64)
+    ns, nd = _c_long(), _c_long()
+    if delay is not None:
+        delay = np.ascontiguousarray(delay, np.int32)
+    rc = lib().orc_bruteforce_cpu(_ptr(data), nbits, ndata, nchans, _ptr(freq), tsamp, dm_low,
+                                  dm_high, freq_start, freq_end, dm_step, ds, t_sample, variant,
+                                  None if delay is None else _ptr(delay), _ptr(out), cap, ctypes.byref(ns), _ptr(cols), cols.size,
+                                  ctypes.byref(nd))
+    if rc:
+        raise ValueError(f"oracle brute force rejected the arguments (code {rc})")
+    res, off = [], 0
+    for s in range(ns.value):
+        c = int(cols[s])
+        res.append(out[off:off + nd.value * c].reshape(nd.value, c).copy())
+        off += nd.value * c
+    return res
+
+
+def subband_sums(data: np.ndarray, nchans: int, plan: SubbandPlan, delay1, residual2):
+    data = np.ascontiguousarray(data)
+    nbits = data.dtype.itemsize * 8
+    nsamp = data.size // nchans
+    out = np.zeros((plan.dm_steps, nsamp), np.uint64)
+    d1 = np.ascontiguousarray(delay1, np.int32)
+    r2 = np.ascontiguousarray(residual2, np.int32)
+    rc = lib().orc_subband_sums(_ptr(data), nbits, nsamp, nchans, plan.chan_start, plan.chan_end,
+                                plan.sb_width, plan.ndm0, plan.dm_steps, _ptr(d1), _ptr(r2),
+                                _ptr(out))
+    if rc:
+        raise RuntimeError("oracle subband sums failed")
+    return out
+
+
+def time_binning(data: np.ndarray, nchans: int, ds: int) -> np.ndarray:
+    data = np.ascontiguousarray(data)
+    nbits = data.dtype.itemsize * 8
+    ndata = data.size // nchans
+    out = np.zeros(((ndata + ds - 1) // ds) * nchans, data.dtype)
+    lib().orc_time_binning(_ptr(data), nbits, ndata, nchans, ds, _ptr(out))
+    return out.reshape(-1, nchans)
+
+
+# ---------------------------------------------------------------- RFI stages
+def iqrm_windows(win_sec, hop_sec, include_tail, tsamp, nsample):
+    t0 = np.zeros(1 << 16, np.uint32)
+    t1 = np.zeros(1 << 16, np.uint32)
+    n = lib().orc_iqrm_windows(win_sec, hop_sec, int(include_tail), tsamp, nsample, _ptr(t0),
+                               _ptr(t1), t0.size)
+    return t0[:n].copy(), t1[:n].copy()
+
+
+def iqrm_lags(radius, geofactor):
+    buf = np.zeros(256, np.int32)
+    n = lib().orc_iqrm_lags(radius, geofactor, _ptr(buf), 256)
+    return buf[:n].copy()
+
+
+def iqrm_window_mask(data, nchans, t0, t1, chan_start, chan_end, mode, radius_frac, nsigma,
+                     geofactor, variant=FMA_VAR | RECIP_1349):
+    data = np.ascontiguousarray(data)
+    nbits = data.dtype.itemsize * 8
+    m = np.zeros(nchans, np.uint8)
+    rc = lib().orc_iqrm_window_mask(_ptr(data), nbits, nchans, t0, t1, chan_start, chan_end, mode,
+                                    radius_frac, nsigma, geofactor, variant, _ptr(m))
+    if rc:
+        raise RuntimeError(f"oracle IQRM failed ({rc})")
+    return m
+
+
+def iqrm_masks(data, nchans, chan_start, chan_end, tsamp, iq, variant=FMA_VAR | RECIP_1349):
+    """All window masks of iqrm_cuda::rfi_iqrm_gpu; iq has mode, radius_frac, nsigma,
+    geofactor, win_sec, hop_sec, include_tail.  chan_end is exclusive here."""
+    nsample = np.asarray(data).size // nchans
+    t0, t1 = iqrm_windows(iq.win_sec, iq.hop_sec, iq.include_tail, tsamp, nsample)
+    masks = np.zeros((len(t0), nchans), np.uint8)
+    for w in range(len(t0)):
+        masks[w] = iqrm_window_mask(data, nchans, int(t0[w]), int(t1[w]), chan_start, chan_end,
+                                    iq.mode, iq.radius_frac, iq.nsigma, iq.geofactor, variant)
+    return t0, t1, masks
+
+
+def apply_window_masks(data: np.ndarray, nchans, t0, t1, masks):
+    nbits = data.dtype.itemsize * 8
+    nsamp = data.size // nchans
+    t0 = np.ascontiguousarray(t0, np.uint32)
+    t1 = np.ascontiguousarray(t1, np.uint32)
+    masks = np.ascontiguousarray(masks, np.uint8)
+    lib().orc_apply_window_masks(_ptr(data), nbits, nchans, nsamp, len(t0), _ptr(t0), _ptr(t1),
+                                 _ptr(masks))
+
+
+def zero_dm_callsite(data: np.ndarray, chan_start, chan_end, down_ndata, variant=FMA_ZDM):
+    lib().orc_zero_dm_callsite(_ptr(data), data.dtype.itemsize * 8, chan_start, chan_end,
+                               down_ndata, variant)
+
+
+def zero_dm_range_exact(data: np.ndarray, nchans, chan_start, chan_end):
+    lib().orc_zero_dm_range_exact(_ptr(data), data.dtype.itemsize * 8, nchans,
+                                  data.size // nchans, chan_start, chan_end)
+
+
+def mark_channels(data: np.ndarray, nchans, bad):
+    bad = np.ascontiguousarray(bad, np.int32)
+    lib().orc_mark_channels(_ptr(data), data.dtype.itemsize * 8, nchans, data.size // nchans,
+                            _ptr(bad), len(bad))
+
+
+# ---------------------------------------------------------------- reference builds
+_ref_cpu = None
+
+
+def ref_cpu_available() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libref_cpu.so"))
+
+
+def ref_cpu():
+    global _ref_cpu
+    if _ref_cpu is None:
+        L = ctypes.CDLL(os.path.join(REF_DIR, "libref_cpu.so"))
+        f = L.ref_cpu_dedispered_fil_omp
+        f.restype = _c_int
+        f.argtypes = [_c_int, _P, _c_long, _c_int, _c_double, _c_double, _c_double, _c_float,
+                      _c_float, _c_float, _c_float, _c_float, _c_int, _c_float, _P, _c_long, _P,
+                      _P, _c_long, _P, ctypes.c_char_p, _c_int]
+        L.ref_cpu_threads.restype = _c_int
+        _ref_cpu = L
+    return _ref_cpu
+
+
+def ref_cpu_delays(nchans, ndata, fch1, foff, tsamp, dm_low, dm_high, freq_start, freq_end,
+                   dm_step):
+    """Recover the reference CPU build's [ndm, chan_end-chan_start] delay table by probing
+    cpucal::dedispered_fil_omp with unit impulses (a channel-c impulse at the last sample
+    shows up in DM row m at column ndata-1-delay[m][c]).  Several channels are probed per
+    call, separated in time by more than the largest delay."""
+    freq = freq_table_fil(fch1, foff, nchans)
+    cs, ce = chan_range(freq, freq_start, freq_end)
+    steps = dm_steps(dm_low, dm_high, dm_step)
+    nc = ce - cs
+    dmax = int(4148.808 * max(dm_high, 0) * (1 / freq[cs] ** 2 - 1 / freq[ce] ** 2) / tsamp) + 3
+    span = dmax + 2
+    n = max(ndata, span + 2)
+    per = max(1, (n - 1) // span)
+    D = np.full((steps, nc), -1, np.int64)
+    for c0 in range(0, nc, per):
+        chans = list(range(c0, min(nc, c0 + per)))
+        y = np.zeros((n, nchans), np.uint8)
+        for k, c in enumerate(chans):
+            y[n - 1 - k * span, cs + c] = 1
+        full = np.concatenate(ref_bruteforce_cpu(y, nchans, fch1, foff, tsamp, dm_low, dm_high,
+                                                 freq_start, freq_end, dm_step, 1,
+                                                 n * tsamp * 0.9999), axis=1)
+        for k, c in enumerate(chans):
+            t_imp = n - 1 - k * span
+            lo = max(0, t_imp - dmax - 1)
+            seg = full[:, lo:t_imp + 1]
+            nz = seg.argmax(axis=1)
+            has = seg.max(axis=1) > 0
+            D[has, c] = t_imp - (lo + nz[has])
+    return D.astype(np.int32)
+
+
+def ref_bruteforce_cpu(data, nchans, fch1, foff, tsamp, dm_low, dm_high, freq_start, freq_end,
+                       dm_step, ds, t_sample):
+    """The reference's cpucal::dedispered_fil_omp on a Filterbank built from `data`."""
+    data = np.ascontiguousarray(data)
+    nbits = data.dtype.itemsize * 8
+    ndata = data.size // nchans
+    steps = dm_steps(dm_low, dm_high, dm_step)
+    cap = steps * (ndata + 64) + 1024
+    out = np.zeros(cap, np.uint64)
+    cols = np.zeros(1 << 16, np.int64)
+    ns, nd = _c_long(), _c_long()
+    err = ctypes.create_string_buffer(512)
+    rc = ref_cpu().ref_cpu_dedispered_fil_omp(nbits, _ptr(data), ndata, nchans, fch1, foff, tsamp,
+                                              dm_low, dm_high, freq_start, freq_end, dm_step, ds,
+                                              t_sample, _ptr(out), cap, ctypes.byref(ns),
+                                              _ptr(cols), cols.size, ctypes.byref(nd), err, 512)
+    if rc:
+        raise ValueError(f"reference rejected the arguments: {err.value.decode()}")
+    res, off = [], 0
+    for s in range(ns.value):
+        c = int(cols[s])
+        res.append(out[off:off + nd.value * c].reshape(nd.value, c).copy())
+        off += nd.value * c
+    return res
+
+
+class _TapRfi(ctypes.Structure):
+    _fields_ = [("use_mask", _c_int), ("use_zero_dm", _c_int), ("use_iqrm", _c_int),
+                ("iq_mode", _c_int), ("iq_radius_frac", _c_float), ("iq_nsigma", _c_float),
+                ("iq_geofactor", _c_double), ("iq_win_sec", _c_double), ("iq_hop_sec", _c_double),
+                ("iq_include_tail", _c_int)]
+
+
+def _tap_rfi(use_mask, use_zero_dm, use_iqrm, iq):
+    r = _TapRfi()
+    r.use_mask, r.use_zero_dm, r.use_iqrm = int(use_mask), int(use_zero_dm), int(use_iqrm)
+    if iq is not None:
+        r.iq_mode, r.iq_radius_frac, r.iq_nsigma = iq.mode, iq.radius_frac, iq.nsigma
+        r.iq_geofactor, r.iq_win_sec, r.iq_hop_sec = iq.geofactor, iq.win_sec, iq.hop_sec
+        r.iq_include_tail = int(iq.include_tail)
+    else:
+        r.iq_mode, r.iq_radius_frac, r.iq_nsigma, r.iq_geofactor = 0, 0.1, 3.0, 1.5
+        r.iq_win_sec, r.iq_hop_sec, r.iq_include_tail = 5.0, 2.5, 1
+    return r
+
+
+_ref_gpu = {}
+
+
+def ref_gpu_available(sb_width: int) -> bool:
+    return os.path.exists(os.path.join(REF_DIR, f"libref_gpu_sb{sb_width}.so"))
+
+
+def ref_gpu(sb_width: int):
+    if sb_width not in _ref_gpu:
+        L = ctypes.CDLL(os.path.join(REF_DIR, f"libref_gpu_sb{sb_width}.so"))
+        L.ref_gpu_dedisperse_spec.restype = _c_int
+        L.ref_gpu_dedisperse_spec.argtypes = [
+            _c_int, _P, _c_float, _c_float, _c_float, _c_float, _c_int, _c_long, _c_float,
+            _c_float, _c_float, _c_float, _c_float, _c_int, _c_float, _c_int, ctypes.c_char_p, _P,
+            _P, _c_long, _P, _P, ctypes.c_char_p, _c_int]
+        L.ref_gpu_tables.restype = _c_int
+        L.ref_gpu_tables.argtypes = [_c_float, _c_float, _c_float, _c_int, _c_long, _c_float,
+                                     _c_float, _c_float, _c_float, _c_float, _c_int, _P, _c_long,
+                                     _P, _c_long, _P, ctypes.c_char_p, _c_int]
+        L.ref_gpu_rfi.restype = _c_int
+        L.ref_gpu_rfi.argtypes = [_c_int, _P, _c_float, _c_float, _c_float, _c_int, _c_long,
+                                  _c_float, _c_float, _c_int, ctypes.c_char_p, _P, _P, _c_long, _P,
+                                  _P, _P, _c_long, _P, _P, ctypes.c_char_p, _c_int]
+        _ref_gpu[sb_width] = L
+    return _ref_gpu[sb_width]
+
+
+def ref_gpu_dedisperse_spec(data, nchans, tsamp, fch1, foff, dm_low, dm_high, freq_start,
+                            freq_end, dm_step, ds, t_sample=0.5, sb_width=32, mask_file="",
+                            use_mask=False, use_zero_dm=False, use_iqrm=False, iq=None,
+                            device=0):
+    """Raw [dm_steps, down_ndata] output of the reference's gpucal::dedisperse_spec."""
+    data = np.ascontiguousarray(data)
+    nbits = data.dtype.itemsize * 8
+    ndata = data.size // nchans
+    steps = dm_steps(dm_low, dm_high, dm_step)
+    cap = steps * ((ndata + ds - 1) // ds)
+    out = np.zeros(cap, np.uint64)
+    rows, cols = _c_long(), _c_long()
+    err = ctypes.create_string_buffer(512)
+    r = _tap_rfi(use_mask, use_zero_dm, use_iqrm, iq)
+    rc = ref_gpu(sb_width).ref_gpu_dedisperse_spec(
+        nbits, _ptr(data), 0.0, tsamp, fch1, foff, nchans, ndata, dm_low, dm_high, freq_start,
+        freq_end, dm_step, ds, t_sample, device, mask_file.encode(), ctypes.byref(r), _ptr(out),
+        cap, ctypes.byref(rows), ctypes.byref(cols), err, 512)
+    if rc:
+        raise ValueError(f"reference GPU call failed: {err.value.decode()}")
+    return out[:rows.value * cols.value].reshape(rows.value, cols.value)
+
+
+def ref_gpu_tables(nchans, ndata, tsamp, fch1, foff, dm_low, dm_high, freq_start, freq_end,
+                   dm_step, ds, sb_width=32):
+    steps = dm_steps(dm_low, dm_high, dm_step)
+    cap1 = ((steps + 31) // 32 + 1) * nchans
+    cap2 = steps * (nchans // 1 + 1)
+    d1 = np.zeros(cap1, np.int32)
+    r2 = np.zeros(cap2, np.int32)
+    info = np.zeros(8, np.int64)
+    err = ctypes.create_string_buffer(512)
+    rc = ref_gpu(sb_width).ref_gpu_tables(tsamp, fch1, foff, nchans, ndata, dm_low, dm_high,
+                                          freq_start, freq_end, dm_step, ds, _ptr(d1), cap1,
+                                          _ptr(r2), cap2, _ptr(info), err, 512)
+    if rc:
+        raise ValueError(f"reference table build failed: {err.value.decode()}")
+    cs, ce, st_, nout, nsb, ndm_nom = (int(v) for v in info[:6])
+    dch = ce - cs + 1
+    return (d1[:ndm_nom * dch].reshape(ndm_nom, dch).copy(),
+            r2[:st_ * nsb].reshape(st_, nsb).copy(), dict(chan_start=cs, chan_end=ce,
+                                                          dm_steps=st_, nsamp=nout, nsb=nsb,
+                                                          ndm_nom=ndm_nom))
+
+
+def ref_gpu_rfi(data, nchans, tsamp, fch1, foff, freq_start, freq_end, ds, mask_file="",
+                use_mask=False, use_zero_dm=False, use_iqrm=False, iq=None, sb_width=32):
+    data = np.ascontiguousarray(data)
+    nbits = data.dtype.itemsize * 8
+    ndata = data.size // nchans
+    nout = (ndata + ds - 1) // ds
+    out = np.zeros(nout * nchans, data.dtype)
+    wcap = 4096
+    t0 = np.zeros(wcap, np.uint32)
+    t1 = np.zeros(wcap, np.uint32)
+    wm = np.zeros(wcap * nchans, np.uint8)
+    nwin = _c_long()
+    info = np.zeros(4, np.int64)
+    err = ctypes.create_string_buffer(512)
+    r = _tap_rfi(use_mask, use_zero_dm, use_iqrm, iq)
+    rc = ref_gpu(sb_width).ref_gpu_rfi(nbits, _ptr(data), tsamp, fch1, foff, nchans, ndata,
+                                       freq_start, freq_end, ds, mask_file.encode(),
+                                       ctypes.byref(r), _ptr(out), out.size, _ptr(t0), _ptr(t1),
+                                       _ptr(wm), wcap, ctypes.byref(nwin), _ptr(info), err, 512)
+    if rc:
+        raise ValueError(f"reference RFI replay failed: {err.value.decode()}")
+    n = nwin.value
+    return (out.reshape(nout, nchans), t0[:n].copy(), t1[:n].copy(),
+            wm[:n * nchans].reshape(n, nchans).copy())
