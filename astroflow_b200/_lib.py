@@ -1,0 +1,111 @@
+"""ctypes binding of libastroflow_dd.so (declared in include/astroflow_dd.h).
+
+The library is built in-tree by astroflow_b200/build.py.  Loading fails loudly
+when it is missing: there is no CPU fallback for the dedispersion path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libastroflow_dd.so")
+
+DD_OK = 0
+DD_ERR_INVALID = 1
+DD_ERR_RUNTIME = 2
+DD_ERR_CUDA = 3
+DD_ERR_NOMEM = 4
+DD_ERR_TIMEOUT = 5
+DD_ERR_UNSUPPORTED = 6
+
+ALGO_SUBBAND, ALGO_BRUTE = 0, 1
+ZDM_CALLSITE, ZDM_RANGE = 0, 1
+TABLE_REFERENCE, TABLE_FP64 = 0, 1
+FREQ_HEADER, FREQ_FIL = 0, 1
+
+# Every symbol include/astroflow_dd.h declares.
+EXPORTS = ("dd_plan_create", "dd_plan_destroy", "dd_plan_get_info", "dd_plan_get_tables",
+           "dd_plan_set_delay_table", "dd_run", "dd_run_ex", "dd_run_host", "dd_last_error",
+           "dd_abi_version")
+
+
+class Header(ctypes.Structure):
+    _fields_ = [("mjd", ctypes.c_double), ("tsamp", ctypes.c_double), ("fch1", ctypes.c_double),
+                ("foff", ctypes.c_double), ("nbits", ctypes.c_int32), ("nchans", ctypes.c_int32),
+                ("ndata", ctypes.c_int64)]
+
+
+class IqrmConfig(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int32), ("radius_frac", ctypes.c_float),
+                ("nsigma", ctypes.c_float), ("geofactor", ctypes.c_double),
+                ("win_sec", ctypes.c_double), ("hop_sec", ctypes.c_double),
+                ("include_tail", ctypes.c_int32)]
+
+
+class RfiConfig(ctypes.Structure):
+    _fields_ = [("use_mask", ctypes.c_int32), ("use_zero_dm", ctypes.c_int32),
+                ("use_iqrm", ctypes.c_int32), ("iqrm", IqrmConfig)]
+
+
+class PlanParams(ctypes.Structure):
+    _fields_ = [("dm_low", ctypes.c_float), ("dm_high", ctypes.c_float),
+                ("dm_step", ctypes.c_float), ("freq_start", ctypes.c_float),
+                ("freq_end", ctypes.c_float), ("time_downsample", ctypes.c_int32),
+                ("t_sample", ctypes.c_float), ("algorithm", ctypes.c_int32),
+                ("subband_width", ctypes.c_int32), ("ndm0", ctypes.c_int32),
+                ("zero_dm_mode", ctypes.c_int32), ("table_mode", ctypes.c_int32),
+                ("freq_mode", ctypes.c_int32), ("freq_table", ctypes.c_void_p)]
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in (
+        "chan_start", "chan_end", "dm_steps", "nsamp_in", "nsamp_binned", "out_cols",
+        "out_elem_bytes", "nsb", "ndm_nom", "max_delay", "max_residual", "nslices",
+        "n_iqrm_windows", "workspace_bytes", "delay_rows", "delay_cols",
+        "table_mismatch_fp64")] + [("adds_per_run", ctypes.c_double)]
+
+
+_lib = None
+
+
+def load():
+    """Load the library (once).  Raises RuntimeError if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m astroflow_b200.build` "
+            "(there is no CPU fallback for the dedispersion path)")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    L.dd_plan_create.argtypes = [ctypes.POINTER(Header), ctypes.POINTER(PlanParams),
+                                 ctypes.POINTER(RfiConfig), P, ctypes.c_int32, ctypes.c_int32,
+                                 ctypes.POINTER(ctypes.c_void_p)]
+    L.dd_plan_destroy.argtypes = [P]
+    L.dd_plan_get_info.argtypes = [P, ctypes.POINTER(PlanInfo)]
+    L.dd_plan_get_tables.argtypes = [P, P, P]
+    L.dd_plan_set_delay_table.argtypes = [P, P]
+    L.dd_run.argtypes = [P, P, P, P]
+    L.dd_run_ex.argtypes = [P, P, P, P, P, P, P]
+    L.dd_run_host.argtypes = [P, P, P, P]
+    L.dd_last_error.restype = ctypes.c_char_p
+    L.dd_abi_version.restype = ctypes.c_int
+    for name in EXPORTS:
+        if name not in ("dd_last_error", "dd_abi_version"):
+            getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    """Map a status code to the exception the reference raises for it."""
+    if rc == DD_OK:
+        return
+    msg = load().dd_last_error().decode(errors="replace")
+    if rc == DD_ERR_INVALID:
+        raise ValueError(msg)
+    if rc == DD_ERR_NOMEM:
+        raise MemoryError(msg)
+    raise RuntimeError(msg)

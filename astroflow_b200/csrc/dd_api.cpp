@@ -1,0 +1,733 @@
+// C ABI of the B200 dedispersion library: plan construction (argument checks,
+// frequency table, channel range, DM grid, delay tables, workspace) and the run
+// orchestration.  Host arithmetic that decides table entries is compiled with
+// -ffp-contract=off and without fast-math, so every float expression below is
+// evaluated in IEEE single precision exactly as written.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "dd_internal.h"
+
+namespace dd {
+
+int tile_samples();
+
+namespace {
+thread_local std::string g_last_error;
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) DD_CUDA_TRY(cudaSetDevice(dev));
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+Error invalid(const char* fmt, double a = 0, double b = 0, double c = 0, double d = 0) {
+  char buf[512];
+  std::snprintf(buf, sizeof(buf), fmt, a, b, c, d);
+  return Error{DD_ERR_INVALID, buf};
+}
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+// ---- frequency table and band (dedispered.cu:1003-1031, cpucal.hpp:85-116)
+void build_freq(dd_plan& P) {
+  const int n = P.hdr.nchans;
+  P.freq.resize(n);
+  if (P.p.freq_mode == DD_FREQ_FIL) {
+    if (P.p.freq_table) {
+      P.freq.assign(P.p.freq_table, P.p.freq_table + n);
+    } else {
+      // src/data/filterbank.cpp:445-449, in double.
+      const double f1 = P.hdr.fch1, fo = P.hdr.foff;
+      for (int i = 0; i < n; ++i) P.freq[i] = f1 + static_cast<double>(i) * fo;
+    }
+  } else {
+    // dedispered.cu:1004-1005: header.fch1 + i*header.foff in float.
+    const float f1 = static_cast<float>(P.hdr.fch1), fo = static_cast<float>(P.hdr.foff);
+    for (int i = 0; i < n; ++i) {
+      volatile float prod = static_cast<float>(static_cast<size_t>(i)) * fo;
+      volatile float f = f1 + prod;
+      P.freq[i] = static_cast<double>(f);
+    }
+  }
+  for (int i = 1; i < n; ++i)
+    if (!(P.freq[i] > P.freq[i - 1]))
+      throw Error{DD_ERR_INVALID, "channel frequencies must be ascending (flip foff < 0 data first)"};
+}
+
+void build_band(dd_plan& P) {
+  const int n = P.hdr.nchans;
+  const float fmin = static_cast<float>(P.freq.front());
+  const float fmax = static_cast<float>(P.freq.back());
+  if (P.p.freq_start < fmin || P.p.freq_end > fmax)
+    throw invalid(P.p.algorithm == DD_ALGO_BRUTE
+                      ? "Frequency range [%.3f-%.3f MHz] out of filterbank range [%.3f-%.3f MHz]"
+                      : "Frequency range [%.3f-%.3f MHz] out of spectrum range [%.3f-%.3f MHz]",
+                  P.p.freq_start, P.p.freq_end, fmin, fmax);
+  const float n1 = static_cast<float>(static_cast<size_t>(n - 1));
+  volatile float span = fmax - fmin;
+  volatile float qa = (P.p.freq_start - fmin) / span;
+  volatile float qb = (P.p.freq_end - fmin) / span;
+  size_t cs = static_cast<size_t>(qa * n1);
+  size_t ce = static_cast<size_t>(qb * n1);
+  ce = std::min<size_t>(static_cast<size_t>(n - 1), ce);
+  if (cs >= static_cast<size_t>(n) || ce >= static_cast<size_t>(n))
+    throw invalid("Invalid channel range [%.0f-%.0f] for %.0f channels", double(cs), double(ce), n);
+  P.cs = static_cast<int64_t>(cs);
+  P.ce = static_cast<int64_t>(ce);
+  volatile float q = (P.p.dm_high - P.p.dm_low) / P.p.dm_step;
+  P.dm_steps = static_cast<int64_t>(static_cast<size_t>(q)) + 1;
+  P.ref_freq = static_cast<float>(P.freq[ce]);  // REF_FREQ_END
+}
+
+// ---- brute-force delay table (cpucal.hpp:119-132) in IEEE float
+void build_brute_table(dd_plan& P) {
+  const int64_t nc = P.nc;
+  P.h_delay.assign(static_cast<size_t>(P.dm_steps * nc), 0);
+  const float ref = P.ref_freq;
+  volatile float ref2 = ref * ref;
+  const float inv_ref2 = 1.0f / ref2;
+  const double tsamp = P.tsamp;
+  int64_t mism = 0;
+  for (int64_t s = 0; s < P.dm_steps; ++s) {
+    volatile float idx = static_cast<float>(static_cast<size_t>(s));
+    volatile float prod = idx * P.p.dm_step;
+    volatile float dm = P.p.dm_low + prod;
+    for (int64_t c = 0; c < nc; ++c) {
+      const float fr = static_cast<float>(P.freq[P.cs + c]);
+      volatile float f2 = fr * fr;
+      volatile float a = 1.0f / f2;
+      volatile float diff = a - inv_ref2;
+      volatile float kd = 4148.808f * dm;
+      volatile float delay = kd * diff;
+      const int v32 = static_cast<int>(std::round(static_cast<double>(delay) / tsamp));
+      const double dm64 = static_cast<double>(P.p.dm_low) + static_cast<double>(s) * P.p.dm_step;
+      const double f = P.freq[P.cs + c], r = P.freq[P.ce];
+      const double e = 4148.808 * dm64 * (1.0 / (f * f) - 1.0 / (r * r)) / tsamp;
+      const int v64 = static_cast<int>(std::floor(e + 0.5));
+      mism += (v32 != v64);
+      P.h_delay[s * nc + c] = P.p.table_mode == DD_TABLE_FP64 ? v64 : v32;
+    }
+  }
+  P.table_mismatch_fp64 = mism;
+}
+
+// ---- IQRM window plan (iqrm.cu:348-397) and lags (iqrm.cu:188-200)
+void build_iqrm(dd_plan& P) {
+  const dd_iqrm_config& q = P.rfi.iqrm;
+  const double win_sec = std::max(0.0, q.win_sec), hop_sec = std::max(0.0, q.hop_sec);
+  // header.tsamp * time_downsample in float (dedispered.cu:1088), or
+  // fil.tsamp * time_downsample in double (dedispered.cu:580).
+  double tsamp;
+  if (P.p.freq_mode == DD_FREQ_FIL) {
+    tsamp = P.tsamp * P.p.time_downsample;
+  } else {
+    volatile float ts = static_cast<float>(P.tsamp) * static_cast<float>(P.p.time_downsample);
+    tsamp = static_cast<double>(ts);
+  }
+  const uint32_t ns = static_cast<uint32_t>(P.nbin);
+  const uint32_t W = win_sec > 0.0 ? static_cast<uint32_t>(std::floor(win_sec / tsamp)) : 0u;
+  const uint32_t H = hop_sec > 0.0 ? static_cast<uint32_t>(std::floor(hop_sec / tsamp)) : W;
+  P.win_t0.clear();
+  P.win_t1.clear();
+  if (W == 0 || W >= ns) {
+    P.win_t0.push_back(0);
+    P.win_t1.push_back(ns);
+  } else {
+    uint32_t t0 = 0;
+    while (t0 + W <= ns) {
+      P.win_t0.push_back(t0);
+      P.win_t1.push_back(t0 + W);
+      t0 += (H ? H : W);
+    }
+    if (q.include_tail && t0 < ns && ns > t0 + 4) {
+      P.win_t0.push_back(t0);
+      P.win_t1.push_back(ns);
+    }
+  }
+  const int64_t csub = P.ce - P.cs;  // IQRM's chan_end is exclusive (iqrm.cu:219)
+  const float rf = std::max(0.0f, q.radius_frac);
+  volatile float rprod = rf * static_cast<float>(csub);
+  int radius = std::max(1, static_cast<int>(std::floor(static_cast<float>(rprod))));
+  const double g = q.geofactor > 1.0 ? q.geofactor : 1.5;
+  P.lags.clear();
+  int lag = 1;
+  while (lag <= radius) {
+    // |lag| >= csub would index outside the statistic vector (the reference
+    // reads past its end there); such lags are left out.
+    if (lag < csub) {
+      P.lags.push_back(+lag);
+      P.lags.push_back(-lag);
+    }
+    int nxt = static_cast<int>(g * lag);
+    lag = std::max(nxt, lag + 1);
+  }
+  // Segments: maximal runs of samples covered by the same set of windows.
+  std::vector<uint32_t> cuts{0u, ns};
+  for (size_t w = 0; w < P.win_t0.size(); ++w) {
+    cuts.push_back(std::min(P.win_t0[w], ns));
+    cuts.push_back(std::min(P.win_t1[w], ns));
+  }
+  std::sort(cuts.begin(), cuts.end());
+  cuts.erase(std::unique(cuts.begin(), cuts.end()), cuts.end());
+  P.segs.clear();
+  for (size_t k = 0; k + 1 < cuts.size(); ++k) P.segs.push_back(IqrmSeg{cuts[k], cuts[k + 1]});
+  if (P.segs.empty()) P.segs.push_back(IqrmSeg{0u, ns});
+}
+
+bool callsite_zdm_active(const dd_plan& P) {
+  return P.rfi.use_zero_dm && P.p.zero_dm_mode == DD_ZDM_CALLSITE && P.cs > 0;
+}
+
+void upload(DevBuf& b, const void* h, size_t bytes) {
+  b.alloc(bytes);
+  if (bytes) DD_CUDA_TRY(cudaMemcpy(b.p, h, bytes, cudaMemcpyHostToDevice));
+}
+
+void create_subband(dd_plan& P) {
+  P.sbw = P.p.subband_width > 0 ? P.p.subband_width : 32;
+  P.ndm0 = P.p.ndm0 > 0 ? P.p.ndm0 : 32;
+  const int ds = P.p.time_downsample;
+  P.nbin = (P.nin + ds - 1) / ds;
+  P.dch = P.ce - P.cs + 1;
+  P.nsb = (P.dch + P.sbw - 1) / P.sbw;
+  P.ndm_nom = (P.dm_steps + P.ndm0 - 1) / P.ndm0;
+  P.h_delay.assign(static_cast<size_t>(P.ndm_nom * P.dch), 0);
+  P.h_res.assign(static_cast<size_t>(P.dm_steps * P.nsb), 0);
+  DevBuf d_freq;
+  upload(d_freq, P.freq.data(), sizeof(double) * P.freq.size());
+  P.d_delay.alloc(sizeof(int32_t) * P.h_delay.size());
+  P.d_res.alloc(sizeof(int32_t) * P.h_res.size());
+  launch_subband_tables(d_freq.as<double>(), P.cs, P.ce, P.p.dm_low, P.p.dm_step, P.dm_steps,
+                        P.sbw, P.ndm0, P.ref_freq, P.tsamp, ds,
+                        P.d_delay.as<int32_t>(), P.d_res.as<int32_t>(), 0);
+  DD_CUDA_TRY(cudaMemcpy(P.h_delay.data(), P.d_delay.p, sizeof(int32_t) * P.h_delay.size(),
+                         cudaMemcpyDeviceToHost));
+  DD_CUDA_TRY(cudaMemcpy(P.h_res.data(), P.d_res.p, sizeof(int32_t) * P.h_res.size(),
+                         cudaMemcpyDeviceToHost));
+  // FP64 comparison table for the coarse delays (and replacement in FP64 mode).
+  int64_t mism = 0;
+  const double tsamp = P.tsamp, r = P.freq[P.ce];
+  for (int64_t j = 0; j < P.ndm_nom; ++j) {
+    const double dm = static_cast<double>(P.p.dm_low) + static_cast<double>(j) * P.ndm0 * P.p.dm_step;
+    for (int64_t c = 0; c < P.dch; ++c) {
+      const double f = P.freq[P.cs + c];
+      const int v = static_cast<int>(std::floor(4148.808 * dm * (1.0 / (f * f) - 1.0 / (r * r)) / tsamp + 0.5)) / ds;
+      mism += (v != P.h_delay[j * P.dch + c]);
+      if (P.p.table_mode == DD_TABLE_FP64) P.h_delay[j * P.dch + c] = v;
+    }
+  }
+  if (P.p.table_mode == DD_TABLE_FP64) {
+    for (int64_t m = 0; m < P.dm_steps; ++m) {
+      const int64_t j = m / P.ndm0;
+      const double dd = (static_cast<double>(m) - static_cast<double>(j * P.ndm0)) * P.p.dm_step;
+      for (int64_t sb = 0; sb < P.nsb; ++sb) {
+        const int64_t ch0 = P.cs + sb * P.sbw;
+        const int64_t ch1 = std::min<int64_t>(ch0 + P.sbw, P.ce + 1);
+        const double f = P.freq[(ch0 + ch1 - 1) / 2];
+        P.h_res[m * P.nsb + sb] = static_cast<int>(std::floor(4148.808 * dd * (1.0 / (f * f) - 1.0 / (r * r)) / (tsamp * ds) + 0.5));
+      }
+    }
+    DD_CUDA_TRY(cudaMemcpy(P.d_delay.p, P.h_delay.data(), sizeof(int32_t) * P.h_delay.size(), cudaMemcpyHostToDevice));
+    DD_CUDA_TRY(cudaMemcpy(P.d_res.p, P.h_res.data(), sizeof(int32_t) * P.h_res.size(), cudaMemcpyHostToDevice));
+  }
+  P.table_mismatch_fp64 = mism;
+  int mind = 0, minr = 0;
+  P.max_delay = 0;
+  P.max_res = 0;
+  for (int v : P.h_delay) { P.max_delay = std::max(P.max_delay, v); mind = std::min(mind, v); }
+  for (int v : P.h_res) { P.max_res = std::max(P.max_res, v); minr = std::min(minr, v); }
+  if (mind < 0 || minr < 0)
+    throw invalid("negative dispersion delays (DM below zero or band order) are not supported");
+  P.inter16 = (P.nbits == 8 && P.sbw <= 257) ? 1 : 0;
+  const int64_t kT = tile_samples();
+  // Time tile of the stage-1 -> stage-2 pipeline: long enough that the stage-1
+  // halo (max_res extra samples per tile) stays small, short enough that one
+  // tile of subband sums stays below ~1 GiB.
+  const int64_t per_col = P.ndm_nom * P.nsb * (P.inter16 ? 2 : 4);
+  int64_t L = std::max<int64_t>(kT, round_up(std::max<int64_t>(16 * P.max_res, 8 * kT), kT));
+  while (L > kT && L * per_col > (int64_t(1) << 30)) L -= kT;
+  L = std::min<int64_t>(L, round_up(P.nbin, kT));
+  P.tile = L;
+  P.tile_pitch = round_up(round_up(L + P.max_res, kT) + 64, 64);
+  const int64_t ntiles = (P.nbin + L - 1) / L;
+  P.xpitch = round_up(ntiles * L + round_up(L + P.max_res, kT) + P.max_delay + 64, 64);
+  P.d_x.alloc(static_cast<size_t>(P.dch * P.xpitch) * P.elem);
+  DD_CUDA_TRY(cudaMemset(P.d_x.p, 0, P.d_x.bytes));
+  P.d_inter.alloc(static_cast<size_t>(P.ndm_nom * P.nsb * P.tile_pitch) * (P.inter16 ? 2 : 4));
+  DD_CUDA_TRY(cudaMemset(P.d_inter.p, 0, P.d_inter.bytes));
+  if (ds > 1 || callsite_zdm_active(P))
+    P.d_binned.alloc(static_cast<size_t>(P.nbin * P.hdr.nchans) * P.elem);
+  P.adds = static_cast<double>(P.ndm_nom) * P.dch * P.nbin +
+           static_cast<double>(P.dm_steps) * P.nsb * P.nbin;
+}
+
+void create_brute(dd_plan& P) {
+  const int ds = P.p.time_downsample;
+  if (P.cs >= P.ce) throw invalid("Invalid chan parameters");
+  if (ds < 1) throw invalid("time_downsample must be >= 1");
+  if (P.p.dm_low > P.p.dm_high || P.p.dm_low < 0 || P.p.dm_step <= 0)
+    throw invalid("Invalid DM parameters");
+  if (P.p.t_sample > P.nin * P.tsamp)
+    throw invalid("t_sample exceeds total observation time");
+  P.nbin = P.nin;
+  P.nc = P.ce - P.cs;
+  build_brute_table(P);
+  P.sps = static_cast<int64_t>(std::round(static_cast<double>(P.p.t_sample) / P.tsamp));
+  if (P.sps <= 0) throw invalid("t_sample shorter than one sample");
+  P.nslices = (P.nin + P.sps - 1) / P.sps;
+  P.slice_cols.clear();
+  P.out_cols = 0;
+  for (int64_t s = 0; s < P.nslices; ++s) {
+    const int64_t start = s * P.sps, end = std::min(start + P.sps, P.nin);
+    const int64_t cols = (end - start + ds - 1) / ds;
+    P.slice_cols.push_back(cols);
+    P.out_cols += cols;
+  }
+  P.cols0 = P.slice_cols.front();
+  P.phases_merge = (P.sps % ds) == 0;
+  P.max_delay = 0;
+  int mind = 0;
+  for (int v : P.h_delay) { P.max_delay = std::max(P.max_delay, v); mind = std::min(mind, v); }
+  if (mind < 0) throw invalid("negative dispersion delays are not supported");
+  const int64_t kT = tile_samples();
+  P.phase_len = round_up((P.nin + ds - 1) / ds + P.max_delay / ds + round_up(P.cols0, kT) + kT + 64, 64);
+  P.d_x.alloc(static_cast<size_t>(P.nc * ds * P.phase_len) * P.elem);
+  DD_CUDA_TRY(cudaMemset(P.d_x.p, 0, P.d_x.bytes));
+  P.d_delay.alloc(sizeof(int32_t) * P.h_delay.size());
+  DD_CUDA_TRY(cudaMemcpy(P.d_delay.p, P.h_delay.data(), sizeof(int32_t) * P.h_delay.size(),
+                         cudaMemcpyHostToDevice));
+  P.adds = static_cast<double>(P.dm_steps) * P.nc * P.out_cols;
+}
+
+void create_rfi(dd_plan& P) {
+  const int64_t n = P.hdr.nchans;
+  std::vector<uint8_t> keep(static_cast<size_t>(n), 1);
+  bool any_bad = false;
+  for (int32_t c : P.bad)
+    if (c >= 0 && c < n) { keep[c] = 0; any_bad = true; }
+  if (P.rfi.use_mask && any_bad) upload(P.d_bad_keep, keep.data(), keep.size());
+  if (P.rfi.use_iqrm) {
+    build_iqrm(P);
+    const int nwin = static_cast<int>(P.win_t0.size());
+    std::vector<uint32_t> win(2 * nwin);
+    for (int w = 0; w < nwin; ++w) { win[2 * w] = P.win_t0[w]; win[2 * w + 1] = P.win_t1[w]; }
+    upload(P.d_win, win.data(), sizeof(uint32_t) * win.size());
+    std::vector<uint32_t> st0(P.segs.size());
+    for (size_t k = 0; k < P.segs.size(); ++k) st0[k] = P.segs[k].t0;
+    upload(P.d_seg_t0, st0.data(), sizeof(uint32_t) * st0.size());
+    if (!P.lags.empty()) upload(P.d_lags, P.lags.data(), sizeof(int32_t) * P.lags.size());
+    const int64_t csub = std::max<int64_t>(P.ce - P.cs, 1);
+    P.d_stats.alloc(sizeof(unsigned long long) * 2 * csub * nwin);
+    P.d_iqrm_scratch.alloc(iqrm_scratch_bytes(nwin, csub, static_cast<int>(P.lags.size())));
+    P.d_masks.alloc(static_cast<size_t>(nwin) * n);
+    P.d_segmask.alloc(P.segs.size() * n);
+  }
+  if (callsite_zdm_active(P) && P.cs * P.ce > P.nbin * n)
+    throw invalid("zero-DM at the reference call site would read past the chunk (%.0f x %.0f elements)",
+                  double(P.ce), double(P.cs));
+  if (P.rfi.use_zero_dm) {
+    if (P.p.zero_dm_mode == DD_ZDM_RANGE) P.d_zdm.alloc(sizeof(uint32_t) * P.nbin);
+    else if (callsite_zdm_active(P)) P.d_zdm.alloc(sizeof(float) * (P.ce + 1));
+  }
+}
+
+void run_rfi_and_prep(dd_plan& P, const void* input, uint8_t* masks_out, uint32_t* bounds_out,
+                      void* prepped, cudaStream_t st) {
+  const int64_t n = P.hdr.nchans;
+  const void* src = input;
+  const int ds = P.p.time_downsample;
+  if (ds > 1) {
+    launch_time_binning(input, P.d_binned.p, P.nbits, P.nin, n, ds, st);
+    src = P.d_binned.p;
+  }
+  const bool callsite = callsite_zdm_active(P);
+  if (callsite && src == input) {
+    DD_CUDA_TRY(cudaMemcpyAsync(P.d_binned.p, input, static_cast<size_t>(P.nbin * n) * P.elem,
+                                cudaMemcpyDeviceToDevice, st));
+    src = P.d_binned.p;
+  }
+  const uint8_t* segmask = nullptr;
+  const int nseg = static_cast<int>(P.segs.size());
+  if (P.rfi.use_iqrm) {
+    const int nwin = static_cast<int>(P.win_t0.size());
+    const int64_t csub = P.ce - P.cs;
+    if (csub > 0 && !P.lags.empty()) {
+      launch_iqrm_stats(src, P.nbits, P.nbin, n, P.cs, csub, P.d_win.as<uint32_t>(), nwin,
+                        P.d_stats.as<unsigned long long>(), st);
+      launch_iqrm_decide(P.d_stats.as<unsigned long long>(), nwin, P.d_win.as<uint32_t>(), n,
+                         P.cs, csub, P.rfi.iqrm.mode, std::max(0.0f, P.rfi.iqrm.nsigma),
+                         P.d_lags.as<int32_t>(), static_cast<int>(P.lags.size()), P.iqrm_variant,
+                         P.d_iqrm_scratch.p, P.d_masks.as<uint8_t>(), st);
+    } else {
+      DD_CUDA_TRY(cudaMemsetAsync(P.d_masks.p, 0, P.d_masks.bytes, st));
+    }
+    launch_segment_masks(P.d_masks.as<uint8_t>(), nwin, P.d_win.as<uint32_t>(),
+                         P.d_seg_t0.as<uint32_t>(), nseg, n, P.d_segmask.as<uint8_t>(), st);
+    segmask = P.d_segmask.as<uint8_t>();
+    if (masks_out)
+      DD_CUDA_TRY(cudaMemcpyAsync(masks_out, P.d_masks.p, static_cast<size_t>(nwin) * n,
+                                  cudaMemcpyDeviceToDevice, st));
+    if (bounds_out)
+      DD_CUDA_TRY(cudaMemcpyAsync(bounds_out, P.d_win.p, sizeof(uint32_t) * 2 * nwin,
+                                  cudaMemcpyDeviceToDevice, st));
+  }
+  PrepArgs a{};
+  a.nbits = P.nbits;
+  a.nsamp = P.nbin;
+  a.nchans = n;
+  a.keep = P.d_bad_keep.as<uint8_t>();
+  a.nseg = nseg;
+  a.seg_t0 = P.d_seg_t0.as<uint32_t>();
+  if (callsite) {
+    // Reference order on the flat buffer: IQRM mask, zero-DM as called, mask file.
+    if (segmask) launch_apply_masks_inplace(const_cast<void*>(src), P.nbits, P.nbin, n, segmask,
+                                            P.d_seg_t0.as<uint32_t>(), nseg, st);
+    launch_zero_dm_callsite(const_cast<void*>(src), P.nbits, static_cast<size_t>(P.cs),
+                            static_cast<size_t>(P.ce), static_cast<size_t>(P.nbin),
+                            P.d_zdm.as<float>(), st);
+    a.segmask = nullptr;
+  } else {
+    a.segmask = segmask;
+    if (P.rfi.use_zero_dm && P.p.zero_dm_mode == DD_ZDM_RANGE) {
+      launch_zdm_offsets(src, P.nbits, P.nbin, n, P.cs, P.ce, segmask, P.d_seg_t0.as<uint32_t>(),
+                         nseg, P.d_zdm.as<uint32_t>(), st);
+      a.zdm_off = P.d_zdm.as<uint32_t>();
+      a.zdm_cs = P.cs;
+      a.zdm_ce = P.ce;
+    }
+  }
+  a.x = src;
+  a.out = P.d_x.p;
+  a.c0 = P.cs;
+  a.c1 = P.ce + 1;
+  a.ds = 1;
+  a.pitch = P.xpitch;
+  a.full_out = prepped;
+  launch_prep(a, st);
+}
+
+void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out,
+                 uint32_t* bounds_out, void* prepped, cudaStream_t st) {
+  run_rfi_and_prep(P, input, masks_out, bounds_out, prepped, st);
+  for (int64_t t0 = 0; t0 < P.nbin; t0 += P.tile) {
+    Stage1Args s1{};
+    s1.x = P.d_x.p;
+    s1.xpitch = P.xpitch;
+    s1.nbits = P.nbits;
+    s1.delay1 = P.d_delay.as<int32_t>();
+    s1.dch = P.dch;
+    s1.nsb = P.nsb;
+    s1.ndm_nom = P.ndm_nom;
+    s1.sbw = P.sbw;
+    s1.t0 = t0;
+    s1.ncols = P.tile + P.max_res;
+    s1.inter = P.d_inter.p;
+    s1.tile_pitch = P.tile_pitch;
+    s1.inter16 = P.inter16;
+    launch_stage1(s1, st);
+    Stage2Args s2{};
+    s2.inter = P.d_inter.p;
+    s2.tile_pitch = P.tile_pitch;
+    s2.inter16 = P.inter16;
+    s2.res = P.d_res.as<int32_t>();
+    s2.nsb = P.nsb;
+    s2.dm_steps = P.dm_steps;
+    s2.ndm0 = P.ndm0;
+    s2.ncols = std::min<int64_t>(P.tile, P.nbin - t0);
+    s2.out = output;
+    s2.out_pitch = P.nbin;
+    s2.col0 = t0;
+    s2.out64 = 0;
+    s2.sbw = P.sbw;
+    s2.src_max = P.sbw * 255;
+    launch_stage2(s2, st);
+  }
+}
+
+void run_brute(dd_plan& P, const void* input, void* output, void* prepped, cudaStream_t st) {
+  PrepArgs a{};
+  a.x = input;
+  a.nbits = P.nbits;
+  a.nsamp = P.nin;
+  a.nchans = P.hdr.nchans;
+  a.out = P.d_x.p;
+  a.c0 = P.cs;
+  a.c1 = P.ce;
+  a.ds = P.p.time_downsample;
+  a.pitch = P.phase_len;
+  a.full_out = prepped;
+  launch_prep(a, st);
+  BruteArgs b{};
+  b.x = P.d_x.p;
+  b.phase_len = P.phase_len;
+  b.ds = P.p.time_downsample;
+  b.nbits = P.nbits;
+  b.delay = P.d_delay.as<int32_t>();
+  b.nc = P.nc;
+  b.dm_steps = P.dm_steps;
+  b.out = output;
+  b.out_pitch = P.out_cols;
+  b.out64 = P.nbits == 32;
+  if (P.phases_merge) {
+    b.start = 0;
+    b.ncols = P.out_cols;
+    b.col0 = 0;
+    launch_brute(b, st);
+  } else {
+    for (int64_t s = 0; s < P.nslices; ++s) {
+      b.start = s * P.sps;
+      b.ncols = P.slice_cols[s];
+      b.col0 = s * P.cols0;
+      launch_brute(b, st);
+    }
+  }
+}
+
+int64_t workspace_of(const dd_plan& P) {
+  const DevBuf* bufs[] = {&P.d_delay, &P.d_res, &P.d_lags, &P.d_bad_keep, &P.d_win, &P.d_seg_t0,
+                          &P.d_binned, &P.d_x, &P.d_inter, &P.d_stats, &P.d_iqrm_scratch,
+                          &P.d_masks, &P.d_segmask, &P.d_zdm};
+  int64_t t = 0;
+  for (auto* b : bufs) t += static_cast<int64_t>(b->bytes);
+  return t;
+}
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    g_last_error.clear();
+    f();
+    return DD_OK;
+  } catch (const Error& e) {
+    g_last_error = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return DD_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return DD_ERR_RUNTIME;
+  }
+}
+
+}  // namespace
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+void DevBuf::alloc(size_t n) {
+  release();
+  if (n == 0) return;
+  cudaError_t e = cudaMalloc(&p, n);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    cudaGetLastError();
+    throw Error{e == cudaErrorMemoryAllocation ? DD_ERR_NOMEM : DD_ERR_CUDA,
+                std::string("device allocation of ") + std::to_string(n) + " bytes failed: " +
+                    cudaGetErrorString(e)};
+  }
+  bytes = n;
+}
+
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+}  // namespace dd
+
+using namespace dd;
+
+extern "C" {
+
+int dd_abi_version(void) { return DD_ABI_VERSION; }
+
+const char* dd_last_error(void) { return g_last_error.c_str(); }
+
+int dd_plan_create(const dd_header* header, const dd_plan_params* params,
+                   const dd_rfi_config* rfi, const int32_t* bad_channels, int32_t n_bad,
+                   int32_t device, dd_plan** plan) {
+  if (!plan) { set_error("plan pointer is NULL"); return DD_ERR_INVALID; }
+  *plan = nullptr;
+  dd_plan* P = nullptr;
+  int rc = guarded([&] {
+    if (!header || !params) throw Error{DD_ERR_INVALID, "header and params are required"};
+    if (header->nbits != 8 && header->nbits != 16 && header->nbits != 32)
+      throw Error{DD_ERR_INVALID, "nbits must be 8, 16 or 32"};
+    if (header->nchans < 2 || header->ndata < 1 || !(header->tsamp > 0))
+      throw Error{DD_ERR_INVALID, "header needs nchans >= 2, ndata >= 1 and tsamp > 0"};
+    if (params->time_downsample < 1) throw Error{DD_ERR_INVALID, "time_downsample must be >= 1"};
+    if (!(params->dm_step > 0) || params->dm_high < params->dm_low)
+      throw Error{DD_ERR_INVALID, "Invalid DM parameters"};
+    int ndev = 0;
+    DD_CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (ndev == 0) throw Error{DD_ERR_RUNTIME, "No CUDA devices found"};
+    if (device < 0 || device >= ndev) throw Error{DD_ERR_INVALID, "invalid target device"};
+    DeviceGuard g(device);
+    P = new dd_plan();
+    P->hdr = *header;
+    P->p = *params;
+    if (rfi) P->rfi = *rfi;
+    if (P->p.algorithm == DD_ALGO_BRUTE) {
+      // The CPU path the brute-force mode follows has no RFI stages.
+      P->rfi.use_iqrm = P->rfi.use_mask = P->rfi.use_zero_dm = 0;
+    }
+    if (bad_channels && n_bad > 0) P->bad.assign(bad_channels, bad_channels + n_bad);
+    P->device = device;
+    P->nbits = header->nbits;
+    P->elem = header->nbits / 8;
+    P->nin = header->ndata;
+    // The reference's GPU path casts sample counts to unsigned int in its RFI
+    // kernels (rfimarker.cu, iqrm.cu).
+    if (P->nin >= (int64_t(1) << 32)) throw Error{DD_ERR_INVALID, "ndata too large"};
+    // Floating-point forms of the reference's IQRM arithmetic (bit 8: std from a
+    // fused multiply-add; bit 4: threshold through the reciprocal of 1.349).
+    P->iqrm_variant = 8 | 4;
+    if (const char* v = std::getenv("ASTROFLOW_DD_IQRM_VARIANT")) P->iqrm_variant = std::atoi(v);
+    // The _dedisperse_spec path's Header carries tsamp as float.
+    P->tsamp = P->p.freq_mode == DD_FREQ_FIL ? header->tsamp
+                                              : static_cast<double>(static_cast<float>(header->tsamp));
+    build_freq(*P);
+    build_band(*P);
+    if (P->p.algorithm == DD_ALGO_BRUTE) {
+      create_brute(*P);
+    } else if (P->p.algorithm == DD_ALGO_SUBBAND) {
+      if (P->nbits == 32) throw Error{DD_ERR_UNSUPPORTED, "32-bit samples are supported by the brute-force algorithm only"};
+      create_subband(*P);
+      create_rfi(*P);
+    } else {
+      throw Error{DD_ERR_INVALID, "unknown algorithm"};
+    }
+    DD_CUDA_TRY(cudaDeviceSynchronize());
+  });
+  if (rc != DD_OK) {
+    delete P;
+    return rc;
+  }
+  *plan = P;
+  return DD_OK;
+}
+
+int dd_plan_destroy(dd_plan* plan) {
+  if (!plan) return DD_OK;
+  return guarded([&] {
+    DeviceGuard g(plan->device);
+    delete plan;
+  });
+}
+
+int dd_plan_get_info(const dd_plan* P, dd_plan_info* info) {
+  if (!P || !info) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  return guarded([&] {
+    dd_plan_info o{};
+    o.chan_start = P->cs;
+    o.chan_end = P->ce;
+    o.dm_steps = P->dm_steps;
+    o.nsamp_in = P->nin;
+    o.nsamp_binned = P->nbin;
+    o.out_cols = P->p.algorithm == DD_ALGO_BRUTE ? P->out_cols : P->nbin;
+    o.out_elem_bytes = P->nbits == 32 ? 8 : 4;
+    o.nsb = P->nsb;
+    o.ndm_nom = P->ndm_nom;
+    o.max_delay = P->max_delay;
+    o.max_residual = P->max_res;
+    o.nslices = P->nslices;
+    o.n_iqrm_windows = P->rfi.use_iqrm ? static_cast<int64_t>(P->win_t0.size()) : 0;
+    o.workspace_bytes = workspace_of(*P);
+    o.delay_rows = P->p.algorithm == DD_ALGO_BRUTE ? P->dm_steps : P->ndm_nom;
+    o.delay_cols = P->p.algorithm == DD_ALGO_BRUTE ? P->nc : P->dch;
+    o.table_mismatch_fp64 = P->table_mismatch_fp64;
+    o.adds_per_run = P->adds;
+    *info = o;
+  });
+}
+
+int dd_plan_get_tables(const dd_plan* P, int32_t* delay, int32_t* residual) {
+  if (!P) { set_error("NULL plan"); return DD_ERR_INVALID; }
+  return guarded([&] {
+    if (delay) std::memcpy(delay, P->h_delay.data(), sizeof(int32_t) * P->h_delay.size());
+    if (residual && !P->h_res.empty())
+      std::memcpy(residual, P->h_res.data(), sizeof(int32_t) * P->h_res.size());
+  });
+}
+
+int dd_plan_set_delay_table(dd_plan* P, const int32_t* delay) {
+  if (!P || !delay) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  return guarded([&] {
+    if (P->p.algorithm != DD_ALGO_BRUTE)
+      throw Error{DD_ERR_UNSUPPORTED, "delay table injection is for the brute-force algorithm"};
+    DeviceGuard g(P->device);
+    int mx = 0;
+    for (size_t i = 0; i < P->h_delay.size(); ++i) {
+      if (delay[i] < 0) throw Error{DD_ERR_INVALID, "negative delay in table"};
+      mx = std::max(mx, delay[i]);
+    }
+    const int ds = P->p.time_downsample;
+    const int64_t need = (P->nin + ds - 1) / ds + mx / ds + 2;
+    if (need + tile_samples() > P->phase_len) throw Error{DD_ERR_INVALID, "delay larger than the plan's padding"};
+    std::memcpy(P->h_delay.data(), delay, sizeof(int32_t) * P->h_delay.size());
+    P->max_delay = mx;
+    DD_CUDA_TRY(cudaMemcpy(P->d_delay.p, delay, sizeof(int32_t) * P->h_delay.size(), cudaMemcpyHostToDevice));
+  });
+}
+
+int dd_run_ex(dd_plan* P, const void* input, void* output, uint8_t* iqrm_masks,
+              uint32_t* iqrm_bounds, void* prepped, void* stream) {
+  if (!P || !input || !output) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  return guarded([&] {
+    DeviceGuard g(P->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (P->p.algorithm == DD_ALGO_BRUTE) run_brute(*P, input, output, prepped, st);
+    else run_subband(*P, input, output, iqrm_masks, iqrm_bounds, prepped, st);
+    DD_CUDA_TRY(cudaGetLastError());
+  });
+}
+
+int dd_run(dd_plan* P, const void* input, void* output, void* stream) {
+  return dd_run_ex(P, input, output, nullptr, nullptr, nullptr, stream);
+}
+
+int dd_run_host(dd_plan* P, const void* h_input, void* h_output, void* stream) {
+  if (!P || !h_input || !h_output) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  return guarded([&] {
+    DeviceGuard g(P->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t in_bytes = static_cast<size_t>(P->nin * P->hdr.nchans) * P->elem;
+    const size_t out_bytes = static_cast<size_t>(P->dm_steps) *
+                             (P->p.algorithm == DD_ALGO_BRUTE ? P->out_cols : P->nbin) *
+                             (P->nbits == 32 ? 8 : 4);
+    void* d_in = nullptr;
+    void* d_out = nullptr;
+    DD_CUDA_TRY(cudaMallocAsync(&d_in, in_bytes, st));
+    cudaError_t e = cudaMallocAsync(&d_out, out_bytes, st);
+    if (e != cudaSuccess) {
+      cudaFreeAsync(d_in, st);
+      throw Error{DD_ERR_NOMEM, std::string("output allocation failed: ") + cudaGetErrorString(e)};
+    }
+    DD_CUDA_TRY(cudaMemcpyAsync(d_in, h_input, in_bytes, cudaMemcpyHostToDevice, st));
+    if (P->p.algorithm == DD_ALGO_BRUTE) run_brute(*P, d_in, d_out, nullptr, st);
+    else run_subband(*P, d_in, d_out, nullptr, nullptr, nullptr, st);
+    DD_CUDA_TRY(cudaMemcpyAsync(h_output, d_out, out_bytes, cudaMemcpyDeviceToHost, st));
+    DD_CUDA_TRY(cudaFreeAsync(d_in, st));
+    DD_CUDA_TRY(cudaFreeAsync(d_out, st));
+    DD_CUDA_TRY(cudaStreamSynchronize(st));
+  });
+}
+
+}  // extern "C"

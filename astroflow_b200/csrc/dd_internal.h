@@ -1,0 +1,205 @@
+// Internal declarations of the B200 dedispersion library (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/astroflow_dd.h"
+
+namespace dd {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+struct Error {
+  int code;
+  std::string msg;
+};
+#define DD_CUDA_TRY(call)                                                          \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess)                                                         \
+      throw ::dd::Error{DD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+
+// ---------------------------------------------------------------- device buffer
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void alloc(size_t n);
+  void release();
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Geometry of one IQRM segment: the samples [t0, t1) are covered by the same
+// set of IQRM windows, whose masks are OR-ed into seg_mask[segment][nchans].
+struct IqrmSeg {
+  uint32_t t0, t1;
+};
+
+}  // namespace dd
+
+struct dd_plan {
+  dd_header hdr{};
+  dd_plan_params p{};
+  dd_rfi_config rfi{};
+  int device = 0;
+  int nbits = 8;
+  int elem = 1;  // bytes per input sample
+
+  std::vector<double> freq;  // channel frequencies (ascending)
+  int64_t cs = 0, ce = 0;    // band: [cs, ce] subband, [cs, ce) brute force
+  int64_t dm_steps = 0;
+  int64_t nin = 0;           // input samples
+  int64_t nbin = 0;          // binned samples (subband) / input samples (brute)
+  float ref_freq = 0.f;
+  double tsamp = 0;          // sampling time as the reference path uses it
+
+  // subband geometry
+  int64_t dch = 0, nsb = 0, ndm_nom = 0;
+  int sbw = 32, ndm0 = 32;
+  int max_delay = 0, max_res = 0;
+  int inter16 = 0;           // stage-1 sums stored as uint16 (8-bit input, narrow subbands)
+  int64_t tile = 0;          // time tile of the stage-1 -> stage-2 pipeline
+  int64_t tile_pitch = 0;    // row pitch of the inter tile (elements)
+  int64_t xpitch = 0;        // row pitch of the channel-major prepared input (elements)
+
+  // brute-force geometry (CPU path semantics)
+  int64_t nc = 0;            // channels summed, [cs, ce)
+  int64_t sps = 0;           // samples per slice
+  int64_t nslices = 0;
+  int64_t cols0 = 0;         // columns of a full slice
+  std::vector<int64_t> slice_cols;
+  int64_t out_cols = 0;
+  int64_t phase_len = 0;     // padded length of one phase row of the brute-force layout
+  bool phases_merge = true;  // slices share one phase pattern (sps % ds == 0)
+
+  // tables (host copies)
+  std::vector<int32_t> h_delay;  // [ndm_nom][dch] (subband) or [dm_steps][nc] (brute)
+  std::vector<int32_t> h_res;    // [dm_steps][nsb]
+  int64_t table_mismatch_fp64 = 0;
+
+  // IQRM
+  std::vector<uint32_t> win_t0, win_t1;
+  std::vector<int32_t> lags;
+  std::vector<dd::IqrmSeg> segs;
+  int iqrm_variant = 0;
+  std::vector<int32_t> bad;
+
+  // device state
+  dd::DevBuf d_delay, d_res, d_lags, d_bad_keep, d_win, d_seg_t0;
+  dd::DevBuf d_binned;   // binned / working copy of the input [nbin][nchans]
+  dd::DevBuf d_x;        // prepared channel-major input
+  dd::DevBuf d_inter;    // stage-1 tile
+  dd::DevBuf d_stats;    // IQRM sums [nwin][2][csub] uint64
+  dd::DevBuf d_iqrm_scratch;
+  dd::DevBuf d_masks;    // IQRM window masks [nwin][nchans]
+  dd::DevBuf d_segmask;  // [nseg][nchans]
+  dd::DevBuf d_zdm;      // per-sample zero-DM offsets [nbin]
+  double adds = 0;
+};
+
+namespace dd {
+
+// ---- fast-math translation unit (dd_fastmath.cu) ----
+void launch_subband_tables(const double* d_freq, int64_t cs, int64_t ce, float dm_low,
+                           float dm_step, int64_t dm_steps, int sbw, int ndm0, float ref_freq,
+                           double tsamp, int ds, int32_t* d_delay1, int32_t* d_res,
+                           cudaStream_t st);
+// mean_ws: device workspace of chan_end floats.
+void launch_zero_dm_callsite(void* data, int nbits, size_t chan_start, size_t chan_end,
+                             size_t down_ndata, float* mean_ws, cudaStream_t st);
+
+// ---- RFI and layout (dd_rfi.cu) ----
+void launch_time_binning(const void* in, void* out, int nbits, int64_t ndata, int64_t nchans,
+                         int ds, cudaStream_t st);
+// d_win: [nwin][2] (t0, t1); d_sums: [nwin][2][csub] (sum, sum of squares).
+void launch_iqrm_stats(const void* x, int nbits, int64_t nsamp, int64_t nchans, int64_t cs,
+                       int64_t csub, const uint32_t* d_win, int nwin,
+                       unsigned long long* d_sums, cudaStream_t st);
+size_t iqrm_scratch_bytes(int nwin, int64_t csub, int nlags);
+void launch_iqrm_decide(const unsigned long long* d_sums, int nwin, const uint32_t* d_win,
+                        int64_t nchans, int64_t cs, int64_t csub, int mode, float nsigma,
+                        const int32_t* d_lags, int nlags, int variant, void* scratch,
+                        uint8_t* d_masks, cudaStream_t st);
+void launch_segment_masks(const uint8_t* d_masks, int nwin, const uint32_t* d_win,
+                          const uint32_t* d_seg_t0, int nseg, int64_t nchans,
+                          uint8_t* d_segmask, cudaStream_t st);
+void launch_apply_masks_inplace(void* x, int nbits, int64_t nsamp, int64_t nchans,
+                                const uint8_t* d_segmask, const uint32_t* d_seg_t0, int nseg,
+                                cudaStream_t st);
+void launch_zdm_offsets(const void* x, int nbits, int64_t nsamp, int64_t nchans, int64_t cs,
+                        int64_t ce_excl, const uint8_t* d_segmask, const uint32_t* d_seg_t0,
+                        int nseg, uint32_t* d_off, cudaStream_t st);
+struct PrepArgs {
+  const void* x;           // [nsamp][nchans] input (binned)
+  int nbits;
+  int64_t nsamp, nchans;
+  const uint8_t* segmask;  // nullptr: no IQRM masking in this pass
+  const uint32_t* seg_t0;
+  int nseg;
+  const uint32_t* zdm_off; // nullptr: no zero-DM subtraction in this pass
+  int64_t zdm_cs, zdm_ce;  // channel range the zero-DM offset applies to
+  const uint8_t* keep;     // nullptr: no static mask
+  // channel-major output: out[(c - c0) * rows_per_chan + phase][q] with
+  // q = t / ds, phase = t % ds (ds = 1 for the subband layout)
+  void* out;
+  int64_t c0, c1;          // channels [c0, c1)
+  int ds;
+  int64_t pitch;           // elements per output row
+  void* full_out;          // optional [nsamp][nchans] copy after all stages
+};
+void launch_prep(const PrepArgs& a, cudaStream_t st);
+
+// ---- dedispersion sums (dd_dedisp.cu) ----
+struct Stage1Args {
+  const void* x;           // channel-major input, row pitch xpitch (elements)
+  int64_t xpitch;
+  int nbits;
+  const int32_t* delay1;   // [ndm_nom][dch]
+  int64_t dch, nsb, ndm_nom;
+  int sbw;
+  int64_t t0;              // absolute start sample of the tile
+  int64_t ncols;           // columns of inter to compute
+  void* inter;             // [ndm_nom][nsb][tile_pitch]
+  int64_t tile_pitch;
+  int inter16;
+};
+void launch_stage1(const Stage1Args& a, cudaStream_t st);
+struct Stage2Args {
+  const void* inter;
+  int64_t tile_pitch;
+  int inter16;
+  const int32_t* res;      // [dm_steps][nsb]
+  int64_t nsb, dm_steps;
+  int ndm0;
+  int64_t ncols;           // output columns of this tile
+  void* out;               // row m at out + m*out_pitch + col0
+  int64_t out_pitch, col0;
+  int out64;
+  int sbw;
+  int src_max;             // largest value one inter element can hold
+};
+void launch_stage2(const Stage2Args& a, cudaStream_t st);
+struct BruteArgs {
+  const void* x;           // phase layout [nc][ds][phase_len]
+  int64_t phase_len;
+  int ds;
+  int nbits;
+  const int32_t* delay;    // [dm_steps][nc]
+  int64_t nc, dm_steps;
+  int64_t start;           // first input sample of the slice
+  int64_t ncols;           // columns of this slice
+  void* out;
+  int64_t out_pitch, col0;
+  int out64;
+};
+void launch_brute(const BruteArgs& a, cudaStream_t st);
+
+}  // namespace dd

@@ -1,0 +1,440 @@
+// RFI stages and input layout for the B200 dedispersion path.
+//
+//  * time binning with sqrt compression (src/core/dedispered.cu:337-376);
+//  * IQRM channel masks (src/core/iqrm.cu:21-185, 203-345), computed entirely on
+//    the device: per-channel sums are exact 64-bit integers (the reference's
+//    double sums of integer samples are exact, so the statistics agree), and
+//    the per-lag sort, percentiles, threshold and votes run in one block per
+//    window instead of the reference's two host round trips per lag;
+//  * window-mask application (src/rfi/rfimarker.cu:309-390), zero-DM over a
+//    channel range with an exact integer mean, and the static channel mask
+//    (rfimarker.cu:469-488), fused into the pass that writes the channel-major
+//    layout the dedispersion kernels read.
+// Host-side arithmetic of the reference (its percentile and threshold code runs
+// on the CPU) is reproduced with explicitly rounded intrinsics so that no
+// multiply-add contraction changes it.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstdint>
+
+#include "dd_internal.h"
+
+namespace dd {
+namespace {
+
+template <typename T> struct Lim;
+template <> struct Lim<uint8_t> { static constexpr uint64_t vmax = 255u; };
+template <> struct Lim<uint16_t> { static constexpr uint64_t vmax = 65535u; };
+template <> struct Lim<uint32_t> { static constexpr uint64_t vmax = 4294967295u; };
+
+// ---------------------------------------------------------------- binning
+template <typename T>
+__global__ void k_time_binning(const T* __restrict__ in, T* __restrict__ out, int64_t nchans,
+                               int64_t ndata, int ds, int64_t nout) {
+  int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= nchans * nout) return;
+  int64_t c = idx % nchans;
+  int64_t k = idx / nchans;
+  int64_t t0 = k * ds;
+  int64_t t1 = t0 + ds < ndata ? t0 + ds : ndata;
+  uint64_t sum = 0;
+  for (int64_t t = t0; t < t1; ++t) sum += static_cast<uint64_t>(in[c + t * nchans]);
+  const uint64_t vmax = Lim<T>::vmax;
+  uint64_t cnt = static_cast<uint64_t>(t1 - t0);
+  double s = sqrt(static_cast<double>(sum));
+  double smax = sqrt(static_cast<double>(vmax * (cnt ? cnt : 1)));
+  double v = __dmul_rn(__ddiv_rn(s, smax > 0.0 ? smax : 1.0), static_cast<double>(vmax));
+  out[c + k * nchans] = static_cast<T>(v < static_cast<double>(vmax) ? v : static_cast<double>(vmax));
+}
+
+// ---------------------------------------------------------------- IQRM sums
+// Block: 256 consecutive channels of [cs, cs+csub); grid.y: time chunks.
+template <typename T>
+__global__ void k_iqrm_stats(const T* __restrict__ x, int64_t nsamp, int64_t nchans, int64_t cs,
+                             int64_t csub, const uint32_t* __restrict__ win, int nwin,
+                             int64_t chunk, unsigned long long* __restrict__ sums) {
+  int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= csub) return;
+  const int64_t c = cs + i;
+  const int64_t lo = static_cast<int64_t>(blockIdx.y) * chunk;
+  const int64_t hi = lo + chunk < nsamp ? lo + chunk : nsamp;
+  for (int w = 0; w < nwin; ++w) {
+    int64_t a = win[2 * w] > lo ? win[2 * w] : lo;
+    int64_t b = win[2 * w + 1] < hi ? win[2 * w + 1] : hi;
+    if (a >= b) continue;
+    unsigned long long s = 0, s2 = 0;
+    for (int64_t t = a; t < b; ++t) {
+      unsigned long long v = x[t * nchans + c];
+      s += v;
+      s2 += v * v;
+    }
+    atomicAdd(&sums[(static_cast<int64_t>(w) * 2) * csub + i], s);
+    atomicAdd(&sums[(static_cast<int64_t>(w) * 2 + 1) * csub + i], s2);
+  }
+}
+
+__device__ __forceinline__ int iqrm_target(int lag, int i, int csub) {
+  if (lag < 0) return i < csub + lag ? i - lag : csub - 1;
+  return i < lag ? 0 : i - lag;
+}
+
+// Percentile of iqrm.cu:299-306 (host code there): pos = q*(n-1) in double,
+// linear interpolation with the float difference promoted to double.
+__device__ __forceinline__ float pct_sorted(const float* v, int n, float q) {
+  if (n == 1) return v[0];
+  double pos = __dmul_rn(static_cast<double>(q), static_cast<double>(n - 1));
+  int lo = static_cast<int>(floor(pos));
+  int hi = static_cast<int>(ceil(pos));
+  double w = __dsub_rn(pos, static_cast<double>(lo));
+  float dlt = __fsub_rn(v[hi], v[lo]);
+  return static_cast<float>(__dadd_rn(static_cast<double>(v[lo]), __dmul_rn(static_cast<double>(dlt), w)));
+}
+
+// One block per window.  Scratch per window: x, d (float), recv, cast (int),
+// flags (nlags x csub bytes).  Dynamic shared memory: the sort buffer.
+__global__ void k_iqrm_decide(const unsigned long long* __restrict__ sums,
+                              const uint32_t* __restrict__ win, int64_t nchans, int64_t cs,
+                              int csub, int mode, float nsigma, const int32_t* __restrict__ lags,
+                              int nlags, int variant, float* __restrict__ xs,
+                              float* __restrict__ ds_, int* __restrict__ recv,
+                              int* __restrict__ cast_, uint8_t* __restrict__ flags,
+                              int sort_n, uint8_t* __restrict__ masks) {
+  extern __shared__ float srt[];
+  __shared__ float s_med, s_thr;
+  __shared__ int s_skip;
+  const int w = blockIdx.x;
+  const unsigned W = win[2 * w + 1] - win[2 * w];
+  float* x = xs + static_cast<int64_t>(w) * csub;
+  float* d = ds_ + static_cast<int64_t>(w) * csub;
+  int* rc = recv + static_cast<int64_t>(w) * csub;
+  int* cc = cast_ + static_cast<int64_t>(w) * csub;
+  uint8_t* fl = flags + static_cast<int64_t>(w) * nlags * csub;
+  uint8_t* mask = masks + static_cast<int64_t>(w) * nchans;
+  const unsigned long long* s1 = sums + (static_cast<int64_t>(w) * 2) * csub;
+  const unsigned long long* s2 = s1 + csub;
+  for (int c = threadIdx.x; c < nchans; c += blockDim.x) mask[c] = 0;
+  if (W == 0 || csub == 0) return;
+  // Statistic per channel, make_stat_from_sums (iqrm.cu:72-91).
+  for (int i = threadIdx.x; i < csub; i += blockDim.x) {
+    double mean = __ddiv_rn(static_cast<double>(s1[i]), static_cast<double>(W));
+    if (mode == 0) {
+      x[i] = static_cast<float>(mean);
+    } else {
+      double e2 = __ddiv_rn(static_cast<double>(s2[i]), static_cast<double>(W));
+      double var = (variant & 8) ? __fma_rn(-mean, mean, e2) : __dsub_rn(e2, __dmul_rn(mean, mean));
+      if (var < 0.0) var = 0.0;
+      x[i] = static_cast<float>(sqrt(var));
+    }
+    rc[i] = 0;
+    cc[i] = 0;
+  }
+  __syncthreads();
+  for (int l = 0; l < nlags; ++l) {
+    const int lag = lags[l];
+    // Lagged difference with edge clipping, make_diff_with_clipping (iqrm.cu:94-117).
+    for (int k = threadIdx.x; k < sort_n; k += blockDim.x) {
+      float v = FLT_MAX;
+      if (k < csub) {
+        if (lag < 0) {
+          int cut = csub + lag;
+          v = k < cut ? __fsub_rn(x[k], x[k - lag]) : __fsub_rn(x[cut], x[csub - 1]);
+        } else {
+          v = k < lag ? __fsub_rn(x[lag], x[0]) : __fsub_rn(x[k], x[k - lag]);
+        }
+        d[k] = v;
+        fl[static_cast<int64_t>(l) * csub + k] = 0;
+      }
+      srt[k] = k < csub ? v : __int_as_float(0x7f800000);  // +inf pads past the end
+    }
+    __syncthreads();
+    // Bitonic sort of sort_n (power of two) floats, ascending.
+    for (int size = 2; size <= sort_n; size <<= 1) {
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int k = threadIdx.x; k < sort_n; k += blockDim.x) {
+          int p = k ^ stride;
+          if (p > k) {
+            float a = srt[k], b = srt[p];
+            bool up = (k & size) == 0;
+            if ((a > b) == up) { srt[k] = b; srt[p] = a; }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    if (threadIdx.x == 0) {
+      float q1 = pct_sorted(srt, csub, 0.25f);
+      float med = pct_sorted(srt, csub, 0.50f);
+      float q3 = pct_sorted(srt, csub, 0.75f);
+      float s;
+      if (variant & 4) s = fabsf(__fmul_rn(__fsub_rn(q3, q1), __frcp_rn(1.349f)));
+      else s = fabsf(__fdiv_rn(__fsub_rn(q3, q1), 1.349f));
+      bool skip = !(s > 0.f) || !isfinite(s);
+      s_skip = skip;
+      s_med = med;
+      s_thr = __fmul_rn(nsigma, s);
+    }
+    __syncthreads();
+    if (!s_skip) {
+      // flag_and_count_kernel (iqrm.cu:120-151).
+      const float med = s_med, thr = s_thr;
+      for (int i = threadIdx.x; i < csub; i += blockDim.x) {
+        float val = __fsub_rn(d[i], med);
+        if (val > thr) {
+          fl[static_cast<int64_t>(l) * csub + i] = 1;
+          atomicAdd(&rc[i], 1);
+          atomicAdd(&cc[iqrm_target(lag, i, csub)], 1);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // merge_lags_to_mask_kernel (iqrm.cu:154-185).
+  for (int i = threadIdx.x; i < csub; i += blockDim.x) {
+    int ri = rc[i];
+    uint8_t m = 0;
+    if (ri > 0) {
+      for (int l = 0; l < nlags; ++l) {
+        if (!fl[static_cast<int64_t>(l) * csub + i]) continue;
+        if (cc[iqrm_target(lags[l], i, csub)] < ri) { m = 1; break; }
+      }
+    }
+    mask[cs + i] = m;
+  }
+}
+
+// OR of the masks of all windows covering each segment of samples.
+__global__ void k_segment_masks(const uint8_t* __restrict__ masks, int nwin,
+                                const uint32_t* __restrict__ win, const uint32_t* __restrict__ seg_t0,
+                                int nseg, int64_t nchans, uint8_t* __restrict__ segmask) {
+  const int s = blockIdx.y;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= nchans || s >= nseg) return;
+  const uint32_t a = seg_t0[s];
+  uint8_t m = 0;
+  for (int w = 0; w < nwin; ++w)
+    if (win[2 * w] <= a && a < win[2 * w + 1]) m |= masks[static_cast<int64_t>(w) * nchans + c];
+  segmask[static_cast<int64_t>(s) * nchans + c] = m;
+}
+
+__device__ __forceinline__ int find_seg(const uint32_t* seg_t0, int nseg, int64_t t) {
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (static_cast<int64_t>(seg_t0[mid]) <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename T>
+__global__ void k_apply_masks(T* __restrict__ x, int64_t nsamp, int64_t nchans,
+                              const uint8_t* __restrict__ segmask, const uint32_t* __restrict__ seg_t0,
+                              int nseg) {
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= nchans) return;
+  for (int64_t t = blockIdx.y; t < nsamp; t += gridDim.y) {
+    const int s = find_seg(seg_t0, nseg, t);
+    if (segmask[static_cast<int64_t>(s) * nchans + c]) x[t * nchans + c] = 0;
+  }
+}
+
+// Zero-DM offset per sample: one warp per sample row, warp-shuffle reduction of
+// the sum and count of the non-zero (post-IQRM) values of [cs, ce).
+template <typename T>
+__global__ void k_zdm_offsets(const T* __restrict__ x, int64_t nsamp, int64_t nchans, int64_t cs,
+                              int64_t ce, const uint8_t* __restrict__ segmask,
+                              const uint32_t* __restrict__ seg_t0, int nseg,
+                              uint32_t* __restrict__ off) {
+  const int lane = threadIdx.x & 31;
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (t >= nsamp) return;
+  const uint8_t* sm = nullptr;
+  if (segmask) sm = segmask + static_cast<int64_t>(find_seg(seg_t0, nseg, t)) * nchans;
+  unsigned long long s = 0;
+  unsigned int n = 0;
+  const T* row = x + t * nchans;
+  for (int64_t c = cs + lane; c < ce; c += 32) {
+    uint64_t v = row[c];
+    if (sm && sm[c]) v = 0;
+    if (v) { s += v; n += 1; }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+    n += __shfl_xor_sync(0xffffffffu, n, o);
+  }
+  if (lane == 0) off[t] = n ? static_cast<uint32_t>((s + n - 1) / n) : 0u;
+}
+
+// Fused RFI application and transpose to the channel-major layout.
+// Tile: 64 samples x 64 channels, 256 threads.
+template <typename T>
+__global__ void k_prep(PrepArgs a) {
+  __shared__ T tile[64][65];
+  const T* x = static_cast<const T*>(a.x);
+  const int64_t tb = static_cast<int64_t>(blockIdx.x) * 64;
+  const int64_t cb = a.c0 + static_cast<int64_t>(blockIdx.y) * 64;
+  const int tx = threadIdx.x & 63;   // channel within tile (read phase)
+  const int ty = threadIdx.x >> 6;   // 0..3
+  const int64_t c = cb + tx;
+  for (int r = ty; r < 64; r += 4) {
+    const int64_t t = tb + r;
+    T v = 0;
+    if (t < a.nsamp && c < a.c1) {
+      v = x[t * a.nchans + c];
+      if (a.segmask) {
+        const int s = find_seg(a.seg_t0, a.nseg, t);
+        if (a.segmask[static_cast<int64_t>(s) * a.nchans + c]) v = 0;
+      }
+      if (a.zdm_off && c >= a.zdm_cs && c < a.zdm_ce) {
+        const uint32_t m = a.zdm_off[t];
+        v = static_cast<T>(static_cast<uint32_t>(v) > m ? static_cast<uint32_t>(v) - m : 0u);
+      }
+      if (a.keep && !a.keep[c]) v = 0;
+    }
+    tile[r][tx] = v;
+  }
+  __syncthreads();
+  if (a.out) {
+    T* out = static_cast<T*>(a.out);
+    // write phase: thread -> (channel row, sample)
+    for (int r = ty; r < 64; r += 4) {
+      const int64_t cc = cb + r;
+      const int64_t t = tb + tx;
+      if (cc < a.c1 && t < a.nsamp) {
+        const int64_t row = (cc - a.c0) * a.ds + (t % a.ds);
+        out[row * a.pitch + t / a.ds] = tile[tx][r];
+      }
+    }
+  }
+}
+
+// Full-layout copy of the prepared input (parity checks only): all channels.
+template <typename T>
+__global__ void k_prep_full(PrepArgs a) {
+  const T* x = static_cast<const T*>(a.x);
+  T* out = static_cast<T*>(a.full_out);
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= a.nchans) return;
+  for (int64_t t = blockIdx.y; t < a.nsamp; t += gridDim.y) {
+  T v = x[t * a.nchans + c];
+  if (a.segmask) {
+    const int s = find_seg(a.seg_t0, a.nseg, t);
+    if (a.segmask[static_cast<int64_t>(s) * a.nchans + c]) v = 0;
+  }
+  if (a.zdm_off && c >= a.zdm_cs && c < a.zdm_ce) {
+    const uint32_t m = a.zdm_off[t];
+    v = static_cast<T>(static_cast<uint32_t>(v) > m ? static_cast<uint32_t>(v) - m : 0u);
+  }
+  if (a.keep && !a.keep[c]) v = 0;
+  out[t * a.nchans + c] = v;
+  }
+}
+
+}  // namespace
+
+void launch_time_binning(const void* in, void* out, int nbits, int64_t ndata, int64_t nchans,
+                         int ds, cudaStream_t st) {
+  const int64_t nout = (ndata + ds - 1) / ds;
+  const int64_t total = nout * nchans;
+  const unsigned blocks = static_cast<unsigned>((total + 255) / 256);
+  switch (nbits) {
+    case 8: k_time_binning<uint8_t><<<blocks, 256, 0, st>>>(static_cast<const uint8_t*>(in), static_cast<uint8_t*>(out), nchans, ndata, ds, nout); break;
+    case 16: k_time_binning<uint16_t><<<blocks, 256, 0, st>>>(static_cast<const uint16_t*>(in), static_cast<uint16_t*>(out), nchans, ndata, ds, nout); break;
+    default: k_time_binning<uint32_t><<<blocks, 256, 0, st>>>(static_cast<const uint32_t*>(in), static_cast<uint32_t*>(out), nchans, ndata, ds, nout); break;
+  }
+  DD_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_iqrm_stats(const void* x, int nbits, int64_t nsamp, int64_t nchans, int64_t cs,
+                       int64_t csub, const uint32_t* d_win, int nwin, unsigned long long* d_sums,
+                       cudaStream_t st) {
+  DD_CUDA_TRY(cudaMemsetAsync(d_sums, 0, sizeof(unsigned long long) * 2 * csub * nwin, st));
+  const int64_t chunk = 1024;
+  dim3 grid(static_cast<unsigned>((csub + 255) / 256), static_cast<unsigned>((nsamp + chunk - 1) / chunk));
+  switch (nbits) {
+    case 8: k_iqrm_stats<uint8_t><<<grid, 256, 0, st>>>(static_cast<const uint8_t*>(x), nsamp, nchans, cs, csub, d_win, nwin, chunk, d_sums); break;
+    case 16: k_iqrm_stats<uint16_t><<<grid, 256, 0, st>>>(static_cast<const uint16_t*>(x), nsamp, nchans, cs, csub, d_win, nwin, chunk, d_sums); break;
+    default: k_iqrm_stats<uint32_t><<<grid, 256, 0, st>>>(static_cast<const uint32_t*>(x), nsamp, nchans, cs, csub, d_win, nwin, chunk, d_sums); break;
+  }
+  DD_CUDA_TRY(cudaGetLastError());
+}
+
+size_t iqrm_scratch_bytes(int nwin, int64_t csub, int nlags) {
+  return static_cast<size_t>(nwin) * csub * (4 + 4 + 4 + 4 + nlags) + 256;
+}
+
+void launch_iqrm_decide(const unsigned long long* d_sums, int nwin, const uint32_t* d_win,
+                        int64_t nchans, int64_t cs, int64_t csub, int mode, float nsigma,
+                        const int32_t* d_lags, int nlags, int variant, void* scratch,
+                        uint8_t* d_masks, cudaStream_t st) {
+  char* p = static_cast<char*>(scratch);
+  float* xs = reinterpret_cast<float*>(p); p += sizeof(float) * nwin * csub;
+  float* ds_ = reinterpret_cast<float*>(p); p += sizeof(float) * nwin * csub;
+  int* recv = reinterpret_cast<int*>(p); p += sizeof(int) * nwin * csub;
+  int* cast_ = reinterpret_cast<int*>(p); p += sizeof(int) * nwin * csub;
+  uint8_t* flags = reinterpret_cast<uint8_t*>(p);
+  int sort_n = 1;
+  while (sort_n < csub) sort_n <<= 1;
+  const size_t smem = sizeof(float) * sort_n;
+  if (smem > 48 * 1024)
+    DD_CUDA_TRY(cudaFuncSetAttribute(k_iqrm_decide, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  k_iqrm_decide<<<nwin, 1024, smem, st>>>(d_sums, d_win, nchans, cs, static_cast<int>(csub), mode,
+                                          nsigma, d_lags, nlags, variant, xs, ds_, recv, cast_,
+                                          flags, sort_n, d_masks);
+  DD_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_segment_masks(const uint8_t* d_masks, int nwin, const uint32_t* d_win,
+                          const uint32_t* d_seg_t0, int nseg, int64_t nchans, uint8_t* d_segmask,
+                          cudaStream_t st) {
+  dim3 grid(static_cast<unsigned>((nchans + 255) / 256), static_cast<unsigned>(nseg));
+  k_segment_masks<<<grid, 256, 0, st>>>(d_masks, nwin, d_win, d_seg_t0, nseg, nchans, d_segmask);
+  DD_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_apply_masks_inplace(void* x, int nbits, int64_t nsamp, int64_t nchans,
+                                const uint8_t* d_segmask, const uint32_t* d_seg_t0, int nseg,
+                                cudaStream_t st) {
+  dim3 grid(static_cast<unsigned>((nchans + 255) / 256), static_cast<unsigned>(nsamp < 8192 ? nsamp : 8192));
+  switch (nbits) {
+    case 8: k_apply_masks<uint8_t><<<grid, 256, 0, st>>>(static_cast<uint8_t*>(x), nsamp, nchans, d_segmask, d_seg_t0, nseg); break;
+    case 16: k_apply_masks<uint16_t><<<grid, 256, 0, st>>>(static_cast<uint16_t*>(x), nsamp, nchans, d_segmask, d_seg_t0, nseg); break;
+    default: k_apply_masks<uint32_t><<<grid, 256, 0, st>>>(static_cast<uint32_t*>(x), nsamp, nchans, d_segmask, d_seg_t0, nseg); break;
+  }
+  DD_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_zdm_offsets(const void* x, int nbits, int64_t nsamp, int64_t nchans, int64_t cs,
+                        int64_t ce_excl, const uint8_t* d_segmask, const uint32_t* d_seg_t0,
+                        int nseg, uint32_t* d_off, cudaStream_t st) {
+  const unsigned blocks = static_cast<unsigned>((nsamp + 7) / 8);
+  switch (nbits) {
+    case 8: k_zdm_offsets<uint8_t><<<blocks, 256, 0, st>>>(static_cast<const uint8_t*>(x), nsamp, nchans, cs, ce_excl, d_segmask, d_seg_t0, nseg, d_off); break;
+    case 16: k_zdm_offsets<uint16_t><<<blocks, 256, 0, st>>>(static_cast<const uint16_t*>(x), nsamp, nchans, cs, ce_excl, d_segmask, d_seg_t0, nseg, d_off); break;
+    default: k_zdm_offsets<uint32_t><<<blocks, 256, 0, st>>>(static_cast<const uint32_t*>(x), nsamp, nchans, cs, ce_excl, d_segmask, d_seg_t0, nseg, d_off); break;
+  }
+  DD_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_prep(const PrepArgs& a, cudaStream_t st) {
+  if (a.out) {
+    dim3 grid(static_cast<unsigned>((a.nsamp + 63) / 64), static_cast<unsigned>((a.c1 - a.c0 + 63) / 64));
+    switch (a.nbits) {
+      case 8: k_prep<uint8_t><<<grid, 256, 0, st>>>(a); break;
+      case 16: k_prep<uint16_t><<<grid, 256, 0, st>>>(a); break;
+      default: k_prep<uint32_t><<<grid, 256, 0, st>>>(a); break;
+    }
+    DD_CUDA_TRY(cudaGetLastError());
+  }
+  if (a.full_out) {
+    dim3 grid(static_cast<unsigned>((a.nchans + 255) / 256), static_cast<unsigned>(a.nsamp < 8192 ? a.nsamp : 8192));
+    switch (a.nbits) {
+      case 8: k_prep_full<uint8_t><<<grid, 256, 0, st>>>(a); break;
+      case 16: k_prep_full<uint16_t><<<grid, 256, 0, st>>>(a); break;
+      default: k_prep_full<uint32_t><<<grid, 256, 0, st>>>(a); break;
+    }
+    DD_CUDA_TRY(cudaGetLastError());
+  }
+}
+
+}  // namespace dd

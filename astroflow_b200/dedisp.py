@@ -1,0 +1,175 @@
+"""Plan-based Python API over the C ABI (include/astroflow_dd.h).
+
+A Plan holds the delay tables and the device workspace for one chunk geometry
+(header, DM plan, band, RFI settings) and dedisperses any number of chunks of
+that geometry.  Device buffers are torch tensors; torch is used for memory and
+streams only, every sample is computed by the library's CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+
+_ALGOS = {"subband": _lib.ALGO_SUBBAND, "brute": _lib.ALGO_BRUTE}
+_ZDM = {"callsite": _lib.ZDM_CALLSITE, "range": _lib.ZDM_RANGE}
+_TABLES = {"reference": _lib.TABLE_REFERENCE, "fp64": _lib.TABLE_FP64}
+_FREQ = {"header": _lib.FREQ_HEADER, "fil": _lib.FREQ_FIL}
+_NP = {8: np.uint8, 16: np.uint16, 32: np.uint32}
+
+
+@dataclass
+class IqrmParams:
+    """IQRM settings (the reference's iqrmconfig, include/rfi.h:12-39)."""
+    mode: int = 0
+    radius_frac: float = 0.10
+    nsigma: float = 3.0
+    geofactor: float = 1.5
+    win_sec: float = 5.0
+    hop_sec: float = 2.5
+    include_tail: bool = True
+
+
+@dataclass
+class RfiParams:
+    """RFI stage switches (the reference's rficonfig, include/rfi.h:41-57)."""
+    use_mask: bool = False
+    use_zero_dm: bool = False
+    use_iqrm: bool = False
+    iqrm: IqrmParams = field(default_factory=IqrmParams)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _tdtype(bits: int):
+    torch = _torch()
+    return {8: torch.uint8, 16: torch.uint16, 32: torch.uint32, 64: torch.uint64}[bits]
+
+
+class Plan:
+    """One dedispersion geometry on one GPU.
+
+    header: mapping/object with tsamp, fch1, foff, nbits, nchans, ndata (ascending
+    frequency order, foff > 0).  algorithm "subband" follows the reference GPU
+    path (src/core/dedispered.cu:988-1304), "brute" its CPU path
+    (include/cpucal.hpp:75-201).
+    """
+
+    def __init__(self, header, dm_low: float, dm_high: float, freq_start: float,
+                 freq_end: float, dm_step: float = 1.0, time_downsample: int = 1,
+                 t_sample: float = 0.5, algorithm: str = "subband", subband_width: int = 32,
+                 ndm0: int = 32, zero_dm_mode: str = "callsite", table_mode: str = "reference",
+                 freq_mode: str = "header", freq_table: Optional[np.ndarray] = None,
+                 rfi: Optional[RfiParams] = None, bad_channels: Optional[Sequence[int]] = None,
+                 device: int = 0):
+        L = _lib.load()
+        g = (lambda k: header[k]) if isinstance(header, dict) else (lambda k: getattr(header, k))
+        self.nbits = int(g("nbits"))
+        self.nchans = int(g("nchans"))
+        self.device = int(device)
+        h = _lib.Header(float(g("mjd")) if _has(header, "mjd") else 0.0, float(g("tsamp")),
+                        float(g("fch1")), float(g("foff")), self.nbits, self.nchans,
+                        int(g("ndata")))
+        self._freq_table = None
+        if freq_table is not None:
+            self._freq_table = np.ascontiguousarray(freq_table, np.float64)
+        p = _lib.PlanParams(dm_low, dm_high, dm_step, freq_start, freq_end, int(time_downsample),
+                            t_sample, _ALGOS[algorithm], int(subband_width), int(ndm0),
+                            _ZDM[zero_dm_mode], _TABLES[table_mode], _FREQ[freq_mode],
+                            None if self._freq_table is None else self._freq_table.ctypes.data)
+        r = rfi or RfiParams()
+        q = r.iqrm
+        rc_ = _lib.RfiConfig(int(r.use_mask), int(r.use_zero_dm), int(r.use_iqrm),
+                             _lib.IqrmConfig(int(q.mode), q.radius_frac, q.nsigma, q.geofactor,
+                                             q.win_sec, q.hop_sec, int(bool(q.include_tail))))
+        bad = np.ascontiguousarray(list(bad_channels or []), np.int32)
+        self._h = ctypes.c_void_p()
+        _lib.check(L.dd_plan_create(ctypes.byref(h), ctypes.byref(p), ctypes.byref(rc_),
+                                    bad.ctypes.data if bad.size else None, int(bad.size),
+                                    self.device, ctypes.byref(self._h)))
+        info = _lib.PlanInfo()
+        _lib.check(L.dd_plan_get_info(self._h, ctypes.byref(info)))
+        self.info = {n: getattr(info, n) for n, _ in _lib.PlanInfo._fields_}
+        self.algorithm = algorithm
+        self.out_shape = (int(self.info["dm_steps"]), int(self.info["out_cols"]))
+        self.out_bits = 64 if self.nbits == 32 else 32
+        self.in_shape = (int(self.info["nsamp_in"]), self.nchans)
+
+    # ------------------------------------------------------------------ tables
+    def tables(self):
+        """(delay, residual) int32 arrays; residual is None for brute force."""
+        i = self.info
+        d = np.zeros((int(i["delay_rows"]), int(i["delay_cols"])), np.int32)
+        r = None
+        if self.algorithm == "subband":
+            r = np.zeros((int(i["dm_steps"]), int(i["nsb"])), np.int32)
+        _lib.check(_lib.load().dd_plan_get_tables(self._h, d.ctypes.data,
+                                                  None if r is None else r.ctypes.data))
+        return d, r
+
+    def set_delay_table(self, delay: np.ndarray) -> None:
+        delay = np.ascontiguousarray(delay, np.int32)
+        if delay.shape != (int(self.info["delay_rows"]), int(self.info["delay_cols"])):
+            raise ValueError(f"delay table must have shape {self.info['delay_rows'], self.info['delay_cols']}")
+        _lib.check(_lib.load().dd_plan_set_delay_table(self._h, delay.ctypes.data))
+
+    # ------------------------------------------------------------------ running
+    def empty_output(self):
+        torch = _torch()
+        return torch.empty(self.out_shape, dtype=_tdtype(self.out_bits),
+                           device=f"cuda:{self.device}")
+
+    def run(self, x, out=None, stream=None, iqrm_masks=None, iqrm_bounds=None, prepped=None):
+        """Dedisperse a device tensor x ([nsamp, nchans] or flat, uint8/16/32) into
+        out ([dm_steps, out_cols] uint32, or uint64 for 32-bit input)."""
+        torch = _torch()
+        if not x.is_cuda or not x.is_contiguous():
+            raise ValueError("input must be a contiguous CUDA tensor")
+        if x.element_size() * 8 != self.nbits:
+            raise ValueError(f"input dtype must be uint{self.nbits}")
+        if x.numel() < self.in_shape[0] * self.in_shape[1]:
+            raise ValueError("input holds fewer than ndata * nchans samples")
+        if out is None:
+            out = self.empty_output()
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        ptr = lambda t: None if t is None else t.data_ptr()
+        _lib.check(_lib.load().dd_run_ex(self._h, x.data_ptr(), out.data_ptr(), ptr(iqrm_masks),
+                                         ptr(iqrm_bounds), ptr(prepped),
+                                         ctypes.c_void_p(stream.cuda_stream)))
+        return out
+
+    def run_host(self, x: np.ndarray, out: Optional[np.ndarray] = None, stream=None):
+        """Dedisperse a host array through dd_run_host (copies inside the call)."""
+        x = np.ascontiguousarray(x)
+        if x.dtype != _NP[self.nbits]:
+            raise ValueError(f"input dtype must be uint{self.nbits}")
+        if x.size < self.in_shape[0] * self.in_shape[1]:
+            raise ValueError("input holds fewer than ndata * nchans samples")
+        if out is None:
+            out = np.empty(self.out_shape, np.uint64 if self.out_bits == 64 else np.uint32)
+        h = None if stream is None else ctypes.c_void_p(stream.cuda_stream)
+        _lib.check(_lib.load().dd_run_host(self._h, x.ctypes.data, out.ctypes.data, h))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.load().dd_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _has(obj, k):
+    return (k in obj) if isinstance(obj, dict) else hasattr(obj, k)

@@ -1,0 +1,149 @@
+"""Seeded synthetic filterbank chunks with the shapes of astroflow's workloads.
+
+Data are time-major [nsamp, nchans] in ascending frequency order (the order the
+reference's readers produce after flipping foff < 0 files, src/data/filterbank.cpp:793-842):
+Gaussian noise rounded and clipped to the sample type, dispersed Gaussian
+pulses with delays 4148.808*DM*(f^-2 - f_hi^-2) s rounded at injection
+(python/astroflow/dataset/simulator.py:22, 122-124), optional sinusoidal RFI
+channels and broadband zero-DM impulses.  Small chunks are generated with
+numpy; large ones on a CUDA device with torch (same statistics, seeded).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+KDM = 4148.808
+
+
+@dataclass
+class ChunkSpec:
+    nchans: int = 1024
+    nsamp: int = 1 << 17
+    nbits: int = 8
+    f_hi: float = 1500.0          # MHz, top of the band
+    bandwidth: float = 500.0      # MHz
+    tsamp: float = 49.152e-6      # s
+    seed: int = 0
+    mean: Optional[float] = None  # default 128 (8-bit) / 32768 (16-bit)
+    sigma: Optional[float] = None # default 20 / 2000
+    pulses: Sequence[Tuple[float, float, float, float]] = ()  # (dm, t0 s, width s, amplitude)
+    rfi_frac: float = 0.0         # fraction of channels with a sinusoid
+    rfi_amp: float = 60.0
+    rfi_period: Tuple[int, int] = (2, 200)
+    impulses: int = 0             # broadband zero-DM impulses
+    imp_amp: float = 50.0
+    imp_width: Tuple[int, int] = (1, 4)
+
+    @property
+    def foff(self) -> float:
+        return self.bandwidth / self.nchans
+
+    @property
+    def fch1(self) -> float:
+        """Lowest channel frequency (ascending order)."""
+        return self.f_hi - (self.nchans - 1) * self.foff
+
+    def header(self) -> dict:
+        return dict(mjd=0.0, tsamp=self.tsamp, fch1=self.fch1, foff=self.foff, nbits=self.nbits,
+                    nchans=self.nchans, ndata=self.nsamp, filename="synthetic")
+
+    def freqs(self) -> np.ndarray:
+        return self.fch1 + np.arange(self.nchans) * self.foff
+
+
+def _defaults(spec: ChunkSpec):
+    if spec.nbits == 8:
+        return (128.0 if spec.mean is None else spec.mean, 20.0 if spec.sigma is None else spec.sigma, 255)
+    return (32768.0 if spec.mean is None else spec.mean, 2000.0 if spec.sigma is None else spec.sigma, 65535)
+
+
+def _extras(spec: ChunkSpec, rng: np.random.Generator):
+    """Additive signal: ("add", rows, cols, values) pulses, ("sin", channel, (period,
+    phase)) RFI channels and ("imp", start, width) broadband impulses."""
+    f = spec.freqs()
+    adds: list = []
+    for dm, t0, width, amp in spec.pulses:
+        delay = KDM * dm * (f ** -2 - spec.f_hi ** -2)
+        w = max(width / spec.tsamp, 0.5)
+        half = int(math.ceil(4 * w))
+        offs = np.arange(-half, half + 1)
+        prof = amp * np.exp(-0.5 * (offs / w) ** 2)
+        for c in range(spec.nchans):
+            centre = int(np.rint((t0 + delay[c]) / spec.tsamp))
+            rows = centre + offs
+            ok = (rows >= 0) & (rows < spec.nsamp)
+            if ok.any():
+                adds.append(("add", rows[ok], np.full(int(ok.sum()), c), prof[ok]))
+    if spec.rfi_frac > 0:
+        nr = max(1, int(round(spec.rfi_frac * spec.nchans)))
+        chans = rng.choice(spec.nchans, size=nr, replace=False)
+        periods = rng.integers(spec.rfi_period[0], spec.rfi_period[1] + 1, size=nr)
+        phases = rng.uniform(0, 2 * np.pi, size=nr)
+        for c, p, ph in zip(chans, periods, phases):
+            adds.append(("sin", int(c), (float(p), float(ph))))
+    for _ in range(spec.impulses):
+        t = int(rng.integers(0, spec.nsamp))
+        wd = int(rng.integers(spec.imp_width[0], spec.imp_width[1] + 1))
+        adds.append(("imp", t, wd))
+    return adds
+
+
+def make_chunk(spec: ChunkSpec) -> Tuple[np.ndarray, dict]:
+    """Host (numpy) chunk [nsamp, nchans] of uint8/uint16 and its header."""
+    rng = np.random.default_rng(spec.seed)
+    mean, sigma, vmax = _defaults(spec)
+    x = rng.normal(mean, sigma, size=(spec.nsamp, spec.nchans)).astype(np.float32)
+    for item in _extras(spec, rng):
+        if item[0] == "sin":
+            _, c, (p, ph) = item
+            t = np.arange(spec.nsamp, dtype=np.float32)
+            x[:, c] += spec.rfi_amp * np.sin(2 * np.pi * t / p + ph)
+        elif item[0] == "imp":
+            _, t, wd = item
+            x[t:t + wd, :] += spec.imp_amp
+        else:
+            _, rows, cols, vals = item
+            np.add.at(x, (rows, cols), vals)
+    dt = np.uint8 if spec.nbits == 8 else np.uint16
+    return np.clip(np.rint(x), 0, vmax).astype(dt), spec.header()
+
+
+def make_chunk_device(spec: ChunkSpec, device: int = 0):
+    """Device (torch) chunk with the same construction, generated on the GPU."""
+    import torch
+
+    mean, sigma, vmax = _defaults(spec)
+    rng = np.random.default_rng(spec.seed)
+    g = torch.Generator(device=f"cuda:{device}")
+    g.manual_seed(spec.seed)
+    dt = torch.uint8 if spec.nbits == 8 else torch.uint16
+    out = torch.empty((spec.nsamp, spec.nchans), dtype=dt, device=f"cuda:{device}")
+    rows_per = max(1, (1 << 27) // spec.nchans)
+    extras = _extras(spec, rng)
+    for r0 in range(0, spec.nsamp, rows_per):
+        r1 = min(spec.nsamp, r0 + rows_per)
+        blk = torch.randn((r1 - r0, spec.nchans), generator=g, device=out.device) * sigma + mean
+        for item in extras:
+            if item[0] == "sin":
+                _, c, (p, ph) = item
+                t = torch.arange(r0, r1, device=out.device, dtype=torch.float32)
+                blk[:, c] += spec.rfi_amp * torch.sin(2 * math.pi * t / p + ph)
+            elif item[0] == "imp":
+                _, t, wd = item
+                a, b = max(t, r0), min(t + wd, r1)
+                if a < b:
+                    blk[a - r0:b - r0, :] += spec.imp_amp
+            else:
+                _, rows, cols, vals = item
+                sel = (rows >= r0) & (rows < r1)
+                if sel.any():
+                    rr = torch.as_tensor(rows[sel] - r0, device=out.device)
+                    cc = torch.as_tensor(cols[sel], device=out.device)
+                    vv = torch.as_tensor(vals[sel], device=out.device, dtype=torch.float32)
+                    blk.index_put_((rr, cc), vv, accumulate=True)
+        out[r0:r1] = torch.clamp(torch.round(blk), 0, vmax).to(torch.int32).to(dt)
+    return out, spec.header()

@@ -1,0 +1,208 @@
+/* astroflow_dd.h — C ABI of the B200 dedispersion library (libastroflow_dd.so).
+ *
+ * This is the drop-in boundary for astroflow's dedispersion hot path: every
+ * entry point takes plain pointers, sizes and PODs, returns a status code and
+ * never exits the process.  It replaces, for the Python pipeline, the compute
+ * that the reference binds through pybind11 in src/bindpy:
+ *
+ *   _astroflow_core._dedisperse_spec      -> dd_plan_create + dd_run[_host]
+ *       (src/bindpy/bindings.cpp:43-57, src/bindpy/pyapi.cpp:284-309,
+ *        src/core/dedispered.cu:988-1304 gpucal::dedisperse_spec<T>)
+ *   _astroflow_core._dedispered_fil       -> dd_plan_create(freq_mode = DD_FREQ_FIL,
+ *        algorithm = DD_ALGO_SUBBAND for target 1 / DD_ALGO_BRUTE for target 0)
+ *       (src/bindpy/bindings.cpp:25-29, src/bindpy/pyapi.cpp:6-51,
+ *        src/core/dedispered.cu:483-986, include/cpucal.hpp:75-201)
+ *
+ * and the stage functions the reference keeps in src/core and src/rfi
+ * (include/iqrmcuda.h, include/rfimarker.h), whose results are exposed for
+ * parity checks through dd_run_ex.
+ *
+ * Pointers passed to dd_run / dd_run_ex are device pointers on the plan's
+ * device; dd_run_host takes host pointers (pinned or pageable) and stages the
+ * copies on the given stream.  `stream` is a cudaStream_t (NULL = the legacy
+ * default stream).  All functions are thread-compatible: one plan must not be
+ * used by two threads at once; different plans are independent.
+ */
+#ifndef ASTROFLOW_DD_H
+#define ASTROFLOW_DD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DD_ABI_VERSION 1
+
+/* Status codes.  DD_ERR_INVALID corresponds to the reference's
+ * std::invalid_argument (Python ValueError), e.g. a frequency range outside
+ * the band (dedispered.cu:1009-1027); the others to std::runtime_error
+ * (Python RuntimeError).  The reference exits the process on CUDA errors
+ * (dedispered.cu:76-84); this library returns DD_ERR_CUDA instead. */
+enum dd_status {
+  DD_OK = 0,
+  DD_ERR_INVALID = 1,
+  DD_ERR_RUNTIME = 2,
+  DD_ERR_CUDA = 3,
+  DD_ERR_NOMEM = 4,
+  DD_ERR_TIMEOUT = 5,
+  DD_ERR_UNSUPPORTED = 6
+};
+
+/* Filterbank header: the fields of the reference's Header (include/data.h:24-50)
+ * and Filterbank (include/filterbank.h:66-88).  The _dedisperse_spec path's
+ * Header holds float fields; callers pass those floats widened to double (an
+ * exact conversion) and the library rounds them back to float wherever the
+ * reference computes in float (freq_mode DD_FREQ_HEADER).  The filename path
+ * (DD_FREQ_FIL) uses them as the double values the SIGPROC reader produces. */
+typedef struct dd_header {
+  double mjd;
+  double tsamp;    /* seconds */
+  double fch1;     /* MHz, lowest channel (data are in ascending frequency order) */
+  double foff;     /* MHz, > 0 */
+  int32_t nbits;   /* 8, 16 or 32 */
+  int32_t nchans;
+  int64_t ndata;   /* time samples */
+} dd_header;
+
+/* IQRM parameters, the reference's iqrmconfig (include/rfi.h:12-39). */
+typedef struct dd_iqrm_config {
+  int32_t mode;        /* 0 = per-channel mean, 1 = per-channel standard deviation */
+  float radius_frac;
+  float nsigma;
+  double geofactor;
+  double win_sec;      /* 0 = one window over the whole chunk */
+  double hop_sec;
+  int32_t include_tail;
+} dd_iqrm_config;
+
+/* RFI stage switches, the reference's rficonfig (include/rfi.h:41-57). */
+typedef struct dd_rfi_config {
+  int32_t use_mask;     /* zero the channels listed in the mask file */
+  int32_t use_zero_dm;  /* zero-DM filter */
+  int32_t use_iqrm;     /* IQRM channel masking */
+  dd_iqrm_config iqrm;
+} dd_rfi_config;
+
+enum dd_algorithm {
+  DD_ALGO_SUBBAND = 0, /* two-stage subband sums of the reference GPU path (dedispered.cu:416-476) */
+  DD_ALGO_BRUTE = 1    /* direct sums with the CPU path's semantics (cpucal.hpp:75-201) */
+};
+
+enum dd_zero_dm_mode {
+  /* The filter as the reference calls it (dedispered.cu:1107): the 4-argument
+   * call resolves to zero_dm_filter(T*, num_channels, num_samples, alpha), so it
+   * is a no-op when chan_start == 0 and otherwise filters the first
+   * chan_start*chan_end elements as [chan_end][chan_start] with
+   * alpha = down_ndata (rfimarker.cu:130-169). */
+  DD_ZDM_CALLSITE = 0,
+  /* The range filter the call site intends (rfimarker.cu:257-305): per sample,
+   * subtract the mean of the non-zero values of [chan_start, chan_end) from
+   * those channels and clip at zero, with the mean taken exactly
+   * (v -> max(0, v - ceil(sum/count))). */
+  DD_ZDM_RANGE = 1
+};
+
+enum dd_table_mode {
+  /* Delay tables with the reference path's own arithmetic: for the subband
+   * algorithm the single-precision device expressions of dedispered.cu:318-335
+   * and 385-413 evaluated on the GPU with the same fast-math flags; for the
+   * brute-force algorithm the float expression of cpucal.hpp:124-131 in IEEE
+   * arithmetic. */
+  DD_TABLE_REFERENCE = 0,
+  /* round(4148.808*DM*(f^-2 - fref^-2)/tsamp) evaluated in FP64 on the host. */
+  DD_TABLE_FP64 = 1
+};
+
+enum dd_freq_mode {
+  DD_FREQ_HEADER = 0, /* freq[i] = fch1 + i*foff in float (dedispered.cu:1004-1005) */
+  DD_FREQ_FIL = 1     /* freq[i] = fch1 + i*foff in double (filterbank.cpp:445-449) */
+};
+
+typedef struct dd_plan_params {
+  float dm_low;
+  float dm_high;
+  float dm_step;
+  float freq_start;          /* MHz, >= lowest channel frequency */
+  float freq_end;            /* MHz, <= highest channel frequency */
+  int32_t time_downsample;   /* >= 1 */
+  float t_sample;            /* seconds per slice of the brute-force path (cpucal.hpp:141) */
+  int32_t algorithm;         /* dd_algorithm */
+  int32_t subband_width;     /* channels per subband (AF_SUBBAND_SIZE_CH, default 32) */
+  int32_t ndm0;              /* fine DMs per nominal DM (AF_SUBBAND_NDM0, default 32) */
+  int32_t zero_dm_mode;      /* dd_zero_dm_mode */
+  int32_t table_mode;        /* dd_table_mode */
+  int32_t freq_mode;         /* dd_freq_mode */
+  const double* freq_table;  /* optional [nchans] channel frequencies (DD_FREQ_FIL; a
+                                SIGPROC file's own table, filterbank.cpp:376-383), or NULL */
+} dd_plan_params;
+
+typedef struct dd_plan_info {
+  int64_t chan_start;        /* first channel of the band */
+  int64_t chan_end;          /* last channel (inclusive for subband, exclusive for brute force) */
+  int64_t dm_steps;          /* DM trials = output rows */
+  int64_t nsamp_in;          /* input time samples */
+  int64_t nsamp_binned;      /* samples after time binning (subband) */
+  int64_t out_cols;          /* output columns per DM row */
+  int64_t out_elem_bytes;    /* 4 (uint32) or 8 (uint64 for 32-bit input) */
+  int64_t nsb;               /* subbands (subband algorithm) */
+  int64_t ndm_nom;           /* nominal DMs (subband algorithm) */
+  int64_t max_delay;         /* largest stage-1 or brute-force delay, samples */
+  int64_t max_residual;      /* largest stage-2 shift, samples */
+  int64_t nslices;           /* brute force: slices of t_sample */
+  int64_t n_iqrm_windows;    /* IQRM windows (0 when IQRM is off) */
+  int64_t workspace_bytes;   /* device workspace the plan holds */
+  int64_t delay_rows;        /* rows of the delay table (ndm_nom or dm_steps) */
+  int64_t delay_cols;        /* columns of the delay table (channels) */
+  int64_t table_mismatch_fp64; /* delay entries where the table differs from the FP64 table */
+  double adds_per_run;       /* algorithmic integer additions per dd_run */
+} dd_plan_info;
+
+typedef struct dd_plan dd_plan;
+
+/* Build a plan: validates the arguments with the reference's rules (band
+ * edges, channel range, DM count, dedispered.cu:1003-1031 / cpucal.hpp:85-116),
+ * builds the delay tables, and reserves the device workspace on `device`
+ * (the reference's target_id, dedispered.cu:997-1001).  bad_channels is the
+ * list the reference reads from its mask file (rfimarker.cu:441-467); it may
+ * be NULL when n_bad == 0. */
+int dd_plan_create(const dd_header* header, const dd_plan_params* params,
+                   const dd_rfi_config* rfi, const int32_t* bad_channels, int32_t n_bad,
+                   int32_t device, dd_plan** plan);
+int dd_plan_destroy(dd_plan* plan);
+int dd_plan_get_info(const dd_plan* plan, dd_plan_info* info);
+
+/* Copy the plan's delay tables to host memory: delay is [delay_rows][delay_cols]
+ * int32; residual is [dm_steps][nsb] int32 (subband only, may be NULL). */
+int dd_plan_get_tables(const dd_plan* plan, int32_t* delay, int32_t* residual);
+
+/* Replace the brute-force delay table ([dm_steps][delay_cols] int32, host). */
+int dd_plan_set_delay_table(dd_plan* plan, const int32_t* delay);
+
+/* Dedisperse one chunk.  input: [nsamp_in][nchans] samples of header.nbits
+ * (device).  output: [dm_steps][out_cols] uint32 (uint64 for 32-bit input),
+ * device.  Brute force writes the slices of t_sample back to back: slice s
+ * occupies columns [s*cols0, s*cols0 + cols_s) of every row. */
+int dd_run(dd_plan* plan, const void* input, void* output, void* stream);
+
+/* dd_run with the intermediate results exposed for parity checks (device
+ * pointers, each may be NULL): iqrm_masks [n_iqrm_windows][nchans] uint8 and
+ * iqrm_bounds [n_iqrm_windows][2] uint32 (t0, t1) as in iqrm_omp::WindowMask
+ * (include/iqrm.hpp:162-166); prepped [nsamp_binned][nchans] samples after
+ * binning and all RFI stages, the input the dedispersion sums read. */
+int dd_run_ex(dd_plan* plan, const void* input, void* output, uint8_t* iqrm_masks,
+              uint32_t* iqrm_bounds, void* prepped, void* stream);
+
+/* dd_run from host memory: copies input in, runs, copies the output back and
+ * synchronises the stream.  Host buffers may be pageable or pinned. */
+int dd_run_host(dd_plan* plan, const void* h_input, void* h_output, void* stream);
+
+/* Last error message of the calling thread ("" if none). */
+const char* dd_last_error(void);
+int dd_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ASTROFLOW_DD_H */
