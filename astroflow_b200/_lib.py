@@ -26,8 +26,8 @@ FREQ_HEADER, FREQ_FIL = 0, 1
 
 # Every symbol include/astroflow_dd.h declares.
 EXPORTS = ("dd_plan_create", "dd_plan_destroy", "dd_plan_get_info", "dd_plan_get_tables",
-           "dd_plan_set_delay_table", "dd_run", "dd_run_ex", "dd_run_host", "dd_last_error",
-           "dd_abi_version")
+           "dd_plan_set_delay_table", "dd_run", "dd_run_ex", "dd_run_host", "dd_run_profiled",
+           "dd_measure_int_add_rate", "dd_last_error", "dd_abi_version")
 
 
 class Header(ctypes.Structure):
@@ -63,7 +63,14 @@ class PlanInfo(ctypes.Structure):
         "chan_start", "chan_end", "dm_steps", "nsamp_in", "nsamp_binned", "out_cols",
         "out_elem_bytes", "nsb", "ndm_nom", "max_delay", "max_residual", "nslices",
         "n_iqrm_windows", "workspace_bytes", "delay_rows", "delay_cols",
-        "table_mismatch_fp64")] + [("adds_per_run", ctypes.c_double)]
+        "table_mismatch_fp64", "tile_samples")] + [("adds_per_run", ctypes.c_double)]
+
+
+class RunStats(ctypes.Structure):
+    _fields_ = [("total_ms", ctypes.c_float), ("prep_ms", ctypes.c_float),
+                ("stage1_ms", ctypes.c_float), ("stage2_ms", ctypes.c_float),
+                ("launches", ctypes.c_int32), ("stage1_launches", ctypes.c_int32),
+                ("stage2_launches", ctypes.c_int32)]
 
 
 _lib = None
@@ -90,6 +97,8 @@ def load():
     L.dd_run.argtypes = [P, P, P, P]
     L.dd_run_ex.argtypes = [P, P, P, P, P, P, P]
     L.dd_run_host.argtypes = [P, P, P, P]
+    L.dd_run_profiled.argtypes = [P, P, P, P, ctypes.POINTER(RunStats)]
+    L.dd_measure_int_add_rate.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
     L.dd_last_error.restype = ctypes.c_char_p
     L.dd_abi_version.restype = ctypes.c_int
     for name in EXPORTS:

@@ -34,6 +34,8 @@ UNITS = [
     ("dd_fastmath.cu", FASTMATH),
     ("dd_rfi.cu", []),
     ("dd_dedisp.cu", []),
+    ("dd_probe.cu", []),
+    ("dd_sumsmem.cu", []),
 ]
 HOST = ["dd_api.cpp"]
 HEADERS = ["dd_internal.h", os.path.join("..", "..", "include", "astroflow_dd.h")]

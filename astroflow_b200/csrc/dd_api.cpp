@@ -190,6 +190,68 @@ void build_iqrm(dd_plan& P) {
   if (P.segs.empty()) P.segs.push_back(IqrmSeg{0u, ns});
 }
 
+// Event recorder for dd_run_profiled: a plan-owned pool of events, recorded in
+// pairs around the stages on the run's stream.
+struct Prof {
+  dd_plan& P;
+  cudaStream_t st;
+  size_t used = 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prep, s1, s2, total;
+  cudaEvent_t take() {
+    if (used == P.events.size()) {
+      cudaEvent_t e;
+      DD_CUDA_TRY(cudaEventCreate(&e));
+      P.events.push_back(e);
+    }
+    return P.events[used++];
+  }
+  cudaEvent_t mark() {
+    cudaEvent_t e = take();
+    DD_CUDA_TRY(cudaEventRecord(e, st));
+    return e;
+  }
+  static float sum(const std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& v) {
+    float t = 0.f;
+    for (auto& pr : v) {
+      float ms = 0.f;
+      DD_CUDA_TRY(cudaEventElapsedTime(&ms, pr.first, pr.second));
+      t += ms;
+    }
+    return t;
+  }
+};
+
+// Largest spread (max - min) of a table's offsets over groups of `rows` consecutive
+// rows, per column; rows are grouped within blocks of `group` rows (0: no blocks).
+int table_spread(const std::vector<int32_t>& tab, int64_t nrows, int64_t ncols, int rows,
+                 int64_t group) {
+  int spread = 0;
+  const int64_t blk = group > 0 ? group : nrows;
+  for (int64_t b0 = 0; b0 < nrows; b0 += blk) {
+    const int64_t b1 = std::min(nrows, b0 + blk);
+    for (int64_t r0 = b0; r0 < b1; r0 += rows) {
+      const int64_t r1 = std::min(b1, r0 + rows);
+      for (int64_t c = 0; c < ncols; ++c) {
+        int lo = tab[r0 * ncols + c], hi = lo;
+        for (int64_t r = r0 + 1; r < r1; ++r) {
+          lo = std::min(lo, tab[r * ncols + c]);
+          hi = std::max(hi, tab[r * ncols + c]);
+        }
+        spread = std::max(spread, hi - lo);
+      }
+    }
+  }
+  return spread;
+}
+
+// Bytes of one staged window: the tile plus the rows' spread, 16-byte alignment
+// slack and the funnel shift's extra word; 0 when the four windows of a block
+// would not fit comfortably in shared memory.
+int window_bytes(int spread, int tile, int elem) {
+  const int64_t w = round_up(static_cast<int64_t>(spread + tile) * elem + 40, 16);
+  return sum_smem_bytes(static_cast<int>(w)) <= 200 * 1024 ? static_cast<int>(w) : 0;
+}
+
 bool callsite_zdm_active(const dd_plan& P) {
   return P.rfi.use_zero_dm && P.p.zero_dm_mode == DD_ZDM_CALLSITE && P.cs > 0;
 }
@@ -255,6 +317,14 @@ void create_subband(dd_plan& P) {
   if (mind < 0 || minr < 0)
     throw invalid("negative dispersion delays (DM below zero or band order) are not supported");
   P.inter16 = (P.nbits == 8 && P.sbw <= 257) ? 1 : 0;
+  if (P.nbits <= 16) {
+    const int T1 = sum_variant_tile(P.elem, P.nbits == 8 && !P.inter16);
+    P.win1 = window_bytes(table_spread(P.h_delay, P.ndm_nom, P.dch, kSumRows, 0), T1, P.elem);
+  }
+  if (P.inter16) {
+    const int T2 = sum_variant_tile(2, false);
+    P.win2 = window_bytes(table_spread(P.h_res, P.dm_steps, P.nsb, kSumRows, P.ndm0), T2, 2);
+  }
   const int64_t kT = tile_samples();
   // Time tile of the stage-1 -> stage-2 pipeline: long enough that the stage-1
   // halo (max_res extra samples per tile) stays small, short enough that one
@@ -266,7 +336,7 @@ void create_subband(dd_plan& P) {
   P.tile = L;
   P.tile_pitch = round_up(round_up(L + P.max_res, kT) + 64, 64);
   const int64_t ntiles = (P.nbin + L - 1) / L;
-  P.xpitch = round_up(ntiles * L + round_up(L + P.max_res, kT) + P.max_delay + 64, 64);
+  P.xpitch = round_up(ntiles * L + round_up(L + P.max_res, 8192) + P.max_delay + 8192, 64);
   P.d_x.alloc(static_cast<size_t>(P.dch * P.xpitch) * P.elem);
   DD_CUDA_TRY(cudaMemset(P.d_x.p, 0, P.d_x.bytes));
   P.d_inter.alloc(static_cast<size_t>(P.ndm_nom * P.nsb * P.tile_pitch) * (P.inter16 ? 2 : 4));
@@ -275,6 +345,16 @@ void create_subband(dd_plan& P) {
     P.d_binned.alloc(static_cast<size_t>(P.nbin * P.hdr.nchans) * P.elem);
   P.adds = static_cast<double>(P.ndm_nom) * P.dch * P.nbin +
            static_cast<double>(P.dm_steps) * P.nsb * P.nbin;
+}
+
+// The staged-window sums serve 8- and 16-bit samples without downsampling (one
+// source row per channel); other cases use the direct kernels.
+void set_brute_window(dd_plan& P) {
+  P.winb = 0;
+  if (P.p.time_downsample == 1 && P.nbits <= 16) {
+    const int T = sum_variant_tile(P.elem, P.nbits == 8);
+    P.winb = window_bytes(table_spread(P.h_delay, P.dm_steps, P.nc, kSumRows, 0), T, P.elem);
+  }
 }
 
 void create_brute(dd_plan& P) {
@@ -312,6 +392,7 @@ void create_brute(dd_plan& P) {
   P.d_delay.alloc(sizeof(int32_t) * P.h_delay.size());
   DD_CUDA_TRY(cudaMemcpy(P.d_delay.p, P.h_delay.data(), sizeof(int32_t) * P.h_delay.size(),
                          cudaMemcpyHostToDevice));
+  set_brute_window(P);
   P.adds = static_cast<double>(P.dm_steps) * P.nc * P.out_cols;
 }
 
@@ -423,8 +504,10 @@ void run_rfi_and_prep(dd_plan& P, const void* input, uint8_t* masks_out, uint32_
 }
 
 void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out,
-                 uint32_t* bounds_out, void* prepped, cudaStream_t st) {
+                 uint32_t* bounds_out, void* prepped, cudaStream_t st, Prof* pf = nullptr) {
+  cudaEvent_t a = pf ? pf->mark() : nullptr;
   run_rfi_and_prep(P, input, masks_out, bounds_out, prepped, st);
+  if (pf) pf->prep.emplace_back(a, pf->mark());
   for (int64_t t0 = 0; t0 < P.nbin; t0 += P.tile) {
     Stage1Args s1{};
     s1.x = P.d_x.p;
@@ -440,7 +523,36 @@ void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out
     s1.inter = P.d_inter.p;
     s1.tile_pitch = P.tile_pitch;
     s1.inter16 = P.inter16;
-    launch_stage1(s1, st);
+    cudaEvent_t b1 = pf ? pf->mark() : nullptr;
+    if (P.win1) {
+      SumLaunch L{};
+      L.mode = SumLaunch::kStage1;
+      L.src = static_cast<const char*>(P.d_x.p);
+      L.src_pitch = P.xpitch * P.elem;
+      L.off = P.d_delay.as<int32_t>();
+      L.off_pitch = P.dch;
+      L.base = t0;
+      L.nsrc_total = P.dch;
+      L.nrows_total = P.ndm_nom;
+      L.group = P.sbw;
+      L.rows_per_block = kSumRows;
+      L.nsb_out = P.nsb;
+      L.out = static_cast<char*>(P.d_inter.p);
+      L.out_pitch = P.tile_pitch * (P.inter16 ? 2 : 4);
+      L.out_col0 = 0;
+      L.out_elem = P.inter16 ? 2 : 4;
+      L.ncols = P.tile + P.max_res;
+      L.win_bytes = P.win1;
+      L.src_bytes = P.elem;
+      L.flush = (P.nbits == 8 && !P.inter16) ? 1 : 0;
+      L.lane_per = 1;
+      L.grid_y = static_cast<unsigned>((P.ndm_nom + kSumRows - 1) / kSumRows);
+      L.grid_z = static_cast<unsigned>(P.nsb);
+      launch_sum(L, st);
+    } else {
+      launch_stage1(s1, st);
+    }
+    if (pf) pf->s1.emplace_back(b1, pf->mark());
     Stage2Args s2{};
     s2.inter = P.d_inter.p;
     s2.tile_pitch = P.tile_pitch;
@@ -456,11 +568,41 @@ void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out
     s2.out64 = 0;
     s2.sbw = P.sbw;
     s2.src_max = P.sbw * 255;
-    launch_stage2(s2, st);
+    cudaEvent_t b2 = pf ? pf->mark() : nullptr;
+    if (P.win2) {
+      SumLaunch L{};
+      L.mode = SumLaunch::kStage2;
+      L.src = static_cast<const char*>(P.d_inter.p);
+      L.src_pitch = P.tile_pitch * 2;
+      L.off = P.d_res.as<int32_t>();
+      L.off_pitch = P.nsb;
+      L.base = 0;
+      L.nsrc_total = P.nsb;
+      L.nrows_total = P.dm_steps;
+      L.group = P.ndm0;
+      L.rows_per_block = kSumRows;
+      L.out = static_cast<char*>(output);
+      L.out_pitch = P.nbin * 4;
+      L.out_col0 = t0;
+      L.out_elem = 4;
+      L.ncols = s2.ncols;
+      L.win_bytes = P.win2;
+      L.src_bytes = 2;
+      L.flush = 0;
+      L.lane_per = 65535 / (255 * P.sbw);
+      L.grid_y = static_cast<unsigned>(P.ndm_nom * ((P.ndm0 + kSumRows - 1) / kSumRows));
+      L.grid_z = 1;
+      launch_sum(L, st);
+    } else {
+      launch_stage2(s2, st);
+    }
+    if (pf) pf->s2.emplace_back(b2, pf->mark());
   }
 }
 
-void run_brute(dd_plan& P, const void* input, void* output, void* prepped, cudaStream_t st) {
+void run_brute(dd_plan& P, const void* input, void* output, void* prepped, cudaStream_t st,
+               Prof* pf = nullptr) {
+  cudaEvent_t e0 = pf ? pf->mark() : nullptr;
   PrepArgs a{};
   a.x = input;
   a.nbits = P.nbits;
@@ -473,6 +615,8 @@ void run_brute(dd_plan& P, const void* input, void* output, void* prepped, cudaS
   a.pitch = P.phase_len;
   a.full_out = prepped;
   launch_prep(a, st);
+  if (pf) pf->prep.emplace_back(e0, pf->mark());
+  cudaEvent_t e1 = pf ? pf->mark() : nullptr;
   BruteArgs b{};
   b.x = P.d_x.p;
   b.phase_len = P.phase_len;
@@ -484,7 +628,30 @@ void run_brute(dd_plan& P, const void* input, void* output, void* prepped, cudaS
   b.out = output;
   b.out_pitch = P.out_cols;
   b.out64 = P.nbits == 32;
-  if (P.phases_merge) {
+  if (P.winb) {
+    SumLaunch L{};
+    L.mode = SumLaunch::kBrute;
+    L.src = static_cast<const char*>(P.d_x.p);
+    L.src_pitch = P.phase_len * P.elem;
+    L.off = P.d_delay.as<int32_t>();
+    L.off_pitch = P.nc;
+    L.base = 0;
+    L.nsrc_total = P.nc;
+    L.nrows_total = P.dm_steps;
+    L.rows_per_block = kSumRows;
+    L.out = static_cast<char*>(output);
+    L.out_pitch = P.out_cols * 4;
+    L.out_col0 = 0;
+    L.out_elem = 4;
+    L.ncols = P.out_cols;
+    L.win_bytes = P.winb;
+    L.src_bytes = P.elem;
+    L.flush = P.nbits == 8 ? 1 : 0;
+    L.lane_per = 1;
+    L.grid_y = static_cast<unsigned>((P.dm_steps + kSumRows - 1) / kSumRows);
+    L.grid_z = 1;
+    launch_sum(L, st);
+  } else if (P.phases_merge) {
     b.start = 0;
     b.ncols = P.out_cols;
     b.col0 = 0;
@@ -497,7 +664,9 @@ void run_brute(dd_plan& P, const void* input, void* output, void* prepped, cudaS
       launch_brute(b, st);
     }
   }
+  if (pf) pf->s2.emplace_back(e1, pf->mark());
 }
+
 
 int64_t workspace_of(const dd_plan& P) {
   const DevBuf* bufs[] = {&P.d_delay, &P.d_res, &P.d_lags, &P.d_bad_keep, &P.d_win, &P.d_seg_t0,
@@ -529,6 +698,11 @@ int guarded(F&& f) {
 }  // namespace
 
 void set_error(const std::string& msg) { g_last_error = msg; }
+
+long long& launch_count() {
+  thread_local long long n = 0;
+  return n;
+}
 
 void DevBuf::alloc(size_t n) {
   release();
@@ -653,6 +827,7 @@ int dd_plan_get_info(const dd_plan* P, dd_plan_info* info) {
     o.delay_rows = P->p.algorithm == DD_ALGO_BRUTE ? P->dm_steps : P->ndm_nom;
     o.delay_cols = P->p.algorithm == DD_ALGO_BRUTE ? P->nc : P->dch;
     o.table_mismatch_fp64 = P->table_mismatch_fp64;
+    o.tile_samples = P->tile;
     o.adds_per_run = P->adds;
     *info = o;
   });
@@ -679,10 +854,11 @@ int dd_plan_set_delay_table(dd_plan* P, const int32_t* delay) {
       mx = std::max(mx, delay[i]);
     }
     const int ds = P->p.time_downsample;
-    const int64_t need = (P->nin + ds - 1) / ds + mx / ds + 2;
+    const int64_t need = (P->nin + ds - 1) / ds + mx / ds + 96;
     if (need + tile_samples() > P->phase_len) throw Error{DD_ERR_INVALID, "delay larger than the plan's padding"};
     std::memcpy(P->h_delay.data(), delay, sizeof(int32_t) * P->h_delay.size());
     P->max_delay = mx;
+    set_brute_window(*P);
     DD_CUDA_TRY(cudaMemcpy(P->d_delay.p, delay, sizeof(int32_t) * P->h_delay.size(), cudaMemcpyHostToDevice));
   });
 }
@@ -701,6 +877,41 @@ int dd_run_ex(dd_plan* P, const void* input, void* output, uint8_t* iqrm_masks,
 
 int dd_run(dd_plan* P, const void* input, void* output, void* stream) {
   return dd_run_ex(P, input, output, nullptr, nullptr, nullptr, stream);
+}
+
+int dd_run_profiled(dd_plan* P, const void* input, void* output, void* stream,
+                    dd_run_stats* stats) {
+  if (!P || !input || !output || !stats) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  return guarded([&] {
+    DeviceGuard g(P->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Prof pf{*P, st};
+    const long long l0 = launch_count();
+    cudaEvent_t t0 = pf.mark();
+    if (P->p.algorithm == DD_ALGO_BRUTE) run_brute(*P, input, output, nullptr, st, &pf);
+    else run_subband(*P, input, output, nullptr, nullptr, nullptr, st, &pf);
+    cudaEvent_t t1 = pf.mark();
+    DD_CUDA_TRY(cudaEventSynchronize(t1));
+    dd_run_stats o{};
+    DD_CUDA_TRY(cudaEventElapsedTime(&o.total_ms, t0, t1));
+    o.prep_ms = Prof::sum(pf.prep);
+    o.stage1_ms = Prof::sum(pf.s1);
+    o.stage2_ms = Prof::sum(pf.s2);
+    o.launches = static_cast<int32_t>(launch_count() - l0);
+    o.stage1_launches = static_cast<int32_t>(pf.s1.size());
+    o.stage2_launches = P->p.algorithm == DD_ALGO_BRUTE
+                            ? static_cast<int32_t>((P->winb || P->phases_merge) ? 1 : P->nslices)
+                            : static_cast<int32_t>(pf.s2.size());
+    *stats = o;
+  });
+}
+
+int dd_measure_int_add_rate(int32_t device, double* adds_per_second) {
+  if (!adds_per_second) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  return guarded([&] {
+    DeviceGuard g(device);
+    *adds_per_second = measure_int_add_rate(device);
+  });
 }
 
 int dd_run_host(dd_plan* P, const void* h_input, void* h_output, void* stream) {

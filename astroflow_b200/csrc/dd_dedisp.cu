@@ -378,7 +378,7 @@ void launch_stage1(const Stage1Args& a, cudaStream_t st) {
   if (a.nbits == 8) k_stage1_u8<<<grid, kThreads, 0, st>>>(a);
   else if (a.nbits == 16) k_stage1_wide<uint16_t><<<grid, kThreads, 0, st>>>(a);
   else k_stage1_wide<uint32_t><<<grid, kThreads, 0, st>>>(a);
-  DD_CUDA_TRY(cudaGetLastError());
+  DD_LAUNCHED();
 }
 
 void launch_stage2(const Stage2Args& a, cudaStream_t st) {
@@ -386,7 +386,7 @@ void launch_stage2(const Stage2Args& a, cudaStream_t st) {
   const int64_t per_nom = (a.ndm0 + kRows - 1) / kRows;
   dim3 grid(static_cast<unsigned>((a.ncols + kTile - 1) / kTile), static_cast<unsigned>(nnom * per_nom));
   k_stage2<<<grid, kThreads, 0, st>>>(a);
-  DD_CUDA_TRY(cudaGetLastError());
+  DD_LAUNCHED();
 }
 
 void launch_brute(const BruteArgs& a, cudaStream_t st) {
@@ -395,7 +395,7 @@ void launch_brute(const BruteArgs& a, cudaStream_t st) {
   if (a.nbits == 8) k_brute<uint8_t><<<grid, kThreads, 0, st>>>(a);
   else if (a.nbits == 16) k_brute<uint16_t><<<grid, kThreads, 0, st>>>(a);
   else k_brute_u32<<<grid, kThreads, 0, st>>>(a);
-  DD_CUDA_TRY(cudaGetLastError());
+  DD_LAUNCHED();
 }
 
 int tile_samples() { return kTile; }

@@ -134,7 +134,8 @@ void zero_dm_callsite_t(T* data, size_t chan_start, size_t chan_end, size_t down
   k_zdm_mean<T><<<num_samples, 256, 0, st>>>(data, num_channels, num_samples, mean);
   dim3 grid(num_samples, (num_channels + 255) / 256);
   k_zdm_subtract<T><<<grid, 256, 0, st>>>(data, num_channels, num_samples, mean, alpha);
-  DD_CUDA_TRY(cudaGetLastError());
+  DD_COUNT_LAUNCH();
+  DD_LAUNCHED();
 }
 
 }  // namespace
@@ -155,7 +156,7 @@ void launch_subband_tables(const double* d_freq, int64_t cs, int64_t ce, float d
   k_delay1<<<gs, bs, 0, st>>>(d_delay1, dm_low, dm_high_coarse, dm_step_coarse,
                               static_cast<size_t>(cs), static_cast<size_t>(ce), d_freq, ref_freq,
                               tsamp, ndm_nom, ds);
-  DD_CUDA_TRY(cudaGetLastError());
+  DD_LAUNCHED();
   // Subband centre frequencies, dedispered.cu:1151-1157.
   std::vector<double> h_sbfreq(nsb);
   std::vector<double> h_freq(static_cast<size_t>(ce + 1));
@@ -175,7 +176,7 @@ void launch_subband_tables(const double* d_freq, int64_t cs, int64_t ce, float d
   k_residual2<<<static_cast<unsigned>((total + 255) / 256), 256, 0, st>>>(
       d_res, d_sbfreq, static_cast<size_t>(dm_steps), nsb, static_cast<size_t>(ndm0), dm_low,
       dm_step, ref_freq, tsamp, ds);
-  DD_CUDA_TRY(cudaGetLastError());
+  DD_LAUNCHED();
   DD_CUDA_TRY(cudaFreeAsync(d_sbfreq, st));
   DD_CUDA_TRY(cudaStreamSynchronize(st));
 }

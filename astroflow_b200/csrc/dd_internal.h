@@ -24,6 +24,16 @@ struct Error {
       throw ::dd::Error{DD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
   } while (0)
 
+// Kernel launches made by this library on the calling thread (monotonic).
+long long& launch_count();
+#define DD_COUNT_LAUNCH() (++::dd::launch_count())
+// After a kernel launch: count it and surface launch errors.
+#define DD_LAUNCHED()                           \
+  do {                                          \
+    DD_COUNT_LAUNCH();                          \
+    DD_CUDA_TRY(cudaGetLastError());            \
+  } while (0)
+
 // ---------------------------------------------------------------- device buffer
 struct DevBuf {
   void* p = nullptr;
@@ -69,6 +79,7 @@ struct dd_plan {
   int64_t tile = 0;          // time tile of the stage-1 -> stage-2 pipeline
   int64_t tile_pitch = 0;    // row pitch of the inter tile (elements)
   int64_t xpitch = 0;        // row pitch of the channel-major prepared input (elements)
+  int win1 = 0, win2 = 0;    // staged window bytes of the shared-memory sums (0: not used)
 
   // brute-force geometry (CPU path semantics)
   int64_t nc = 0;            // channels summed, [cs, ce)
@@ -79,6 +90,7 @@ struct dd_plan {
   int64_t out_cols = 0;
   int64_t phase_len = 0;     // padded length of one phase row of the brute-force layout
   bool phases_merge = true;  // slices share one phase pattern (sps % ds == 0)
+  int winb = 0;              // staged window bytes of the brute-force sums (0: not used)
 
   // tables (host copies)
   std::vector<int32_t> h_delay;  // [ndm_nom][dch] (subband) or [dm_steps][nc] (brute)
@@ -103,6 +115,10 @@ struct dd_plan {
   dd::DevBuf d_segmask;  // [nseg][nchans]
   dd::DevBuf d_zdm;      // per-sample zero-DM offsets [nbin]
   double adds = 0;
+  std::vector<cudaEvent_t> events;  // timing events of dd_run_profiled
+  ~dd_plan() {
+    for (cudaEvent_t e : events) cudaEventDestroy(e);
+  }
 };
 
 namespace dd {
@@ -201,5 +217,42 @@ struct BruteArgs {
   int out64;
 };
 void launch_brute(const BruteArgs& a, cudaStream_t st);
+
+// ---- shared-memory staged sums (dd_sumsmem.cu) ----
+constexpr int kSumRows = 8;  // output rows per block
+struct SumLaunch {
+  enum Mode { kStage1 = 0, kStage2 = 1, kBrute = 2 };
+  int mode;
+  const char* src;         // byte address of source row 0
+  int64_t src_pitch;       // bytes between source rows
+  const int32_t* off;      // per-row, per-source offsets (elements)
+  int64_t off_pitch;       // entries between consecutive rows of `off`
+  int64_t base;            // element index added to every offset
+  int64_t nsrc_total;      // stage 1: channels of the band; stage 2: subbands; brute: channels
+  int64_t nrows_total;     // stage 1: nominal DMs; stage 2 and brute: DM trials
+  int group;               // stage 1: subband width; stage 2: fine DMs per nominal DM
+  int rows_per_block;      // kSumRows
+  int64_t nsb_out;         // stage 1: subbands (inter rows are (j, sb))
+  char* out;               // byte address of output row 0, column 0
+  int64_t out_pitch;       // bytes between output rows (stage 1: between (j, sb) rows)
+  int64_t out_col0;        // first output column of the launch (elements)
+  int out_elem;            // bytes per output element
+  int64_t ncols;           // columns of the launch
+  int win_bytes;           // bytes of one staged source window
+  int src_bytes;           // 1 or 2
+  int flush;               // 8-bit sources: widen lanes every 256 sources
+  int lane_per;            // 16-bit sources: sources per 16-bit lane before widening
+  unsigned grid_y, grid_z;
+};
+void launch_sum(const SumLaunch& L, cudaStream_t st);
+int sum_tile_samples(int src_bytes, int nw);
+size_t sum_smem_bytes(int win_bytes);
+// Tile (samples per block) of the kernel launch_sum picks for these sources.
+inline int sum_variant_tile(int src_bytes, bool flush) {
+  return sum_tile_samples(src_bytes, (src_bytes == 2 || flush) ? 2 : 4);
+}
+
+// ---- probes (dd_probe.cu) ----
+double measure_int_add_rate(int device);
 
 }  // namespace dd

@@ -342,7 +342,7 @@ void launch_time_binning(const void* in, void* out, int nbits, int64_t ndata, in
     case 16: k_time_binning<uint16_t><<<blocks, 256, 0, st>>>(static_cast<const uint16_t*>(in), static_cast<uint16_t*>(out), nchans, ndata, ds, nout); break;
     default: k_time_binning<uint32_t><<<blocks, 256, 0, st>>>(static_cast<const uint32_t*>(in), static_cast<uint32_t*>(out), nchans, ndata, ds, nout); break;
   }
-  DD_CUDA_TRY(cudaGetLastError());
+  DD_LAUNCHED();
 }
 
 void launch_iqrm_stats(const void* x, int nbits, int64_t nsamp, int64_t nchans, int64_t cs,
@@ -356,7 +356,7 @@ void launch_iqrm_stats(const void* x, int nbits, int64_t nsamp, int64_t nchans, 
     case 16: k_iqrm_stats<uint16_t><<<grid, 256, 0, st>>>(static_cast<const uint16_t*>(x), nsamp, nchans, cs, csub, d_win, nwin, chunk, d_sums); break;
     default: k_iqrm_stats<uint32_t><<<grid, 256, 0, st>>>(static_cast<const uint32_t*>(x), nsamp, nchans, cs, csub, d_win, nwin, chunk, d_sums); break;
   }
-  DD_CUDA_TRY(cudaGetLastError());
+  DD_LAUNCHED();
 }
 
 size_t iqrm_scratch_bytes(int nwin, int64_t csub, int nlags) {
@@ -381,7 +381,7 @@ void launch_iqrm_decide(const unsigned long long* d_sums, int nwin, const uint32
   k_iqrm_decide<<<nwin, 1024, smem, st>>>(d_sums, d_win, nchans, cs, static_cast<int>(csub), mode,
                                           nsigma, d_lags, nlags, variant, xs, ds_, recv, cast_,
                                           flags, sort_n, d_masks);
-  DD_CUDA_TRY(cudaGetLastError());
+  DD_LAUNCHED();
 }
 
 void launch_segment_masks(const uint8_t* d_masks, int nwin, const uint32_t* d_win,
@@ -389,7 +389,7 @@ void launch_segment_masks(const uint8_t* d_masks, int nwin, const uint32_t* d_wi
                           cudaStream_t st) {
   dim3 grid(static_cast<unsigned>((nchans + 255) / 256), static_cast<unsigned>(nseg));
   k_segment_masks<<<grid, 256, 0, st>>>(d_masks, nwin, d_win, d_seg_t0, nseg, nchans, d_segmask);
-  DD_CUDA_TRY(cudaGetLastError());
+  DD_LAUNCHED();
 }
 
 void launch_apply_masks_inplace(void* x, int nbits, int64_t nsamp, int64_t nchans,
@@ -401,7 +401,7 @@ void launch_apply_masks_inplace(void* x, int nbits, int64_t nsamp, int64_t nchan
     case 16: k_apply_masks<uint16_t><<<grid, 256, 0, st>>>(static_cast<uint16_t*>(x), nsamp, nchans, d_segmask, d_seg_t0, nseg); break;
     default: k_apply_masks<uint32_t><<<grid, 256, 0, st>>>(static_cast<uint32_t*>(x), nsamp, nchans, d_segmask, d_seg_t0, nseg); break;
   }
-  DD_CUDA_TRY(cudaGetLastError());
+  DD_LAUNCHED();
 }
 
 void launch_zdm_offsets(const void* x, int nbits, int64_t nsamp, int64_t nchans, int64_t cs,
@@ -413,7 +413,7 @@ void launch_zdm_offsets(const void* x, int nbits, int64_t nsamp, int64_t nchans,
     case 16: k_zdm_offsets<uint16_t><<<blocks, 256, 0, st>>>(static_cast<const uint16_t*>(x), nsamp, nchans, cs, ce_excl, d_segmask, d_seg_t0, nseg, d_off); break;
     default: k_zdm_offsets<uint32_t><<<blocks, 256, 0, st>>>(static_cast<const uint32_t*>(x), nsamp, nchans, cs, ce_excl, d_segmask, d_seg_t0, nseg, d_off); break;
   }
-  DD_CUDA_TRY(cudaGetLastError());
+  DD_LAUNCHED();
 }
 
 void launch_prep(const PrepArgs& a, cudaStream_t st) {
@@ -424,7 +424,7 @@ void launch_prep(const PrepArgs& a, cudaStream_t st) {
       case 16: k_prep<uint16_t><<<grid, 256, 0, st>>>(a); break;
       default: k_prep<uint32_t><<<grid, 256, 0, st>>>(a); break;
     }
-    DD_CUDA_TRY(cudaGetLastError());
+    DD_LAUNCHED();
   }
   if (a.full_out) {
     dim3 grid(static_cast<unsigned>((a.nchans + 255) / 256), static_cast<unsigned>(a.nsamp < 8192 ? a.nsamp : 8192));
@@ -433,7 +433,7 @@ void launch_prep(const PrepArgs& a, cudaStream_t st) {
       case 16: k_prep_full<uint16_t><<<grid, 256, 0, st>>>(a); break;
       default: k_prep_full<uint32_t><<<grid, 256, 0, st>>>(a); break;
     }
-    DD_CUDA_TRY(cudaGetLastError());
+    DD_LAUNCHED();
   }
 }
 

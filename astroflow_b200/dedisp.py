@@ -146,6 +146,19 @@ class Plan:
                                          ctypes.c_void_p(stream.cuda_stream)))
         return out
 
+    def run_profiled(self, x, out=None, stream=None) -> dict:
+        """Run once and return the device-time breakdown (ms) and launch counts."""
+        torch = _torch()
+        if out is None:
+            out = self.empty_output()
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        st = _lib.RunStats()
+        _lib.check(_lib.load().dd_run_profiled(self._h, x.data_ptr(), out.data_ptr(),
+                                               ctypes.c_void_p(stream.cuda_stream),
+                                               ctypes.byref(st)))
+        return {n: getattr(st, n) for n, _ in _lib.RunStats._fields_}
+
     def run_host(self, x: np.ndarray, out: Optional[np.ndarray] = None, stream=None):
         """Dedisperse a host array through dd_run_host (copies inside the call)."""
         x = np.ascontiguousarray(x)
@@ -169,6 +182,13 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+def measure_int_add_rate(device: int = 0) -> float:
+    """Sustained 32-bit integer additions per second on `device` (library probe)."""
+    v = ctypes.c_double()
+    _lib.check(_lib.load().dd_measure_int_add_rate(int(device), ctypes.byref(v)))
+    return v.value
 
 
 def _has(obj, k):

@@ -1,0 +1,438 @@
+#!/usr/bin/env python
+"""Benchmark of astroflow's dedispersion hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME]
+
+One step = one pass of the path (binning, RFI stages, dedispersion) over one
+chunk already resident in HBM.  Default workload (the configuration the
+headline metric is quoted on): 4096 channels of 8-bit samples, 2^20 samples of
+49.152 us, DM 0-3000 in steps of 0.5 (6001 trials), subband width 64, IQRM
+(std, radius 5, 3 sigma, one window) and the zero-DM filter on, with sinusoidal
+RFI channels, broadband impulses and three dispersed pulses injected.
+
+Prints one JSON line (rank 0).  `value` is DM-trial*samples per second over all
+ranks (weak scaling: every rank dedisperses its own chunk; the path has no
+exchange between GPUs).  `e2e` is the same metric through the C ABI with host
+buffers (dd_run_host: host->device copy, run, device->host copy per step).
+`--impl reference` times the reference's own CPU implementation of the path
+(include/cpucal.hpp, built from source into oracle/_ref) on this host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DM-trial·samples/s"
+UNIT = "DM-trial·samples/s"
+
+WORKLOADS = {
+    # 4096 ch u8, 2^20 samples, DM 0:0.5:3000, subband width 64, IQRM + zero-DM
+    "wideband-4096ch-u8-2^20-6001dm-subband64-rfi": dict(
+        nchans=4096, nsamp=1 << 20, nbits=8, dm=(0.0, 3000.0, 0.5), algorithm="subband",
+        subband_width=64, ds=1, rfi=dict(use_zero_dm=True, use_iqrm=True, use_mask=False,
+                                         iqrm=dict(mode=1, radius_frac=0.00134, nsigma=3.0,
+                                                   geofactor=1.5, win_sec=0.0, hop_sec=0.5,
+                                                   include_tail=True)),
+        chunk=dict(rfi_frac=0.05, rfi_amp=60.0, impulses=20, imp_amp=50.0,
+                   pulses=[(120.0, 4.0, 1e-3, 12.0), (780.0, 12.0, 1e-3, 12.0),
+                           (2400.0, 20.0, 1e-3, 12.0)])),
+    # the same configuration on 2^17 samples (ncu captures: a few GB on the device)
+    "wideband-4096ch-u8-2^17-6001dm-subband64-rfi": dict(
+        nchans=4096, nsamp=1 << 17, nbits=8, dm=(0.0, 3000.0, 0.5), algorithm="subband",
+        subband_width=64, ds=1, rfi=dict(use_zero_dm=True, use_iqrm=True, use_mask=False,
+                                         iqrm=dict(mode=1, radius_frac=0.00134, nsigma=3.0,
+                                                   geofactor=1.5, win_sec=0.0, hop_sec=0.5,
+                                                   include_tail=True)),
+        chunk=dict(rfi_frac=0.05, rfi_amp=60.0, impulses=20, imp_amp=50.0,
+                   pulses=[(120.0, 0.5, 1e-3, 12.0), (780.0, 1.5, 1e-3, 12.0),
+                           (2400.0, 2.5, 1e-3, 12.0)])),
+    # 1024 ch u8, 2^17 samples, DM 0:1:1000, brute force (the CPU path's semantics)
+    "plain-1024ch-u8-2^17-1001dm-brute": dict(
+        nchans=1024, nsamp=1 << 17, nbits=8, dm=(0.0, 1000.0, 1.0), algorithm="brute",
+        subband_width=32, ds=1, rfi=None,
+        chunk=dict(pulses=[(565.0, 2.0, 1e-3, 12.0)])),
+}
+DEFAULT_WORKLOAD = "wideband-4096ch-u8-2^20-6001dm-subband64-rfi"
+
+
+# ---------------------------------------------------------------- distributed plumbing
+class Dist:
+    def __init__(self, gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def stop(self) -> dict:
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        smax = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------- reference CPU
+def reference_cpu_rate(x_host: np.ndarray, hdr: dict, wl: dict, target_s: float):
+    """Time the reference's cpucal::dedispered_fil_omp (built from source into
+    oracle/_ref) on a bounded sample: all DM trials of the workload over the first
+    n samples of the chunk, n chosen so one call takes about target_s seconds.
+    Returns (DM-trial*samples/s, threads, sample description, seconds)."""
+    from oracle import oracle as O
+
+    lib = O.ref_cpu()
+    threads = int(lib.ref_cpu_threads())
+    nchans = hdr["nchans"]
+    lo, hi, step = wl["dm"]
+    freq = O.freq_table_fil(hdr["fch1"], hdr["foff"], nchans)
+    fs, fe = float(np.float32(freq[0])), float(np.float32(freq[-1]))
+    ndm = O.dm_steps(lo, hi, step)
+
+    def run(n):
+        xs = np.ascontiguousarray(x_host[:n])
+        t = time.perf_counter()
+        O.ref_bruteforce_cpu(xs, nchans, hdr["fch1"], hdr["foff"], hdr["tsamp"], lo, hi, fs, fe,
+                             step, 1, n * hdr["tsamp"] * 0.999)
+        return time.perf_counter() - t
+
+    n = 256
+    dt = run(n)
+    while dt < 0.5 and n < x_host.shape[0]:
+        n = min(x_host.shape[0], n * 4)
+        dt = run(n)
+    n = int(min(x_host.shape[0], max(256, n * target_s / max(dt, 1e-3))))
+    dt = run(n)
+    rate = ndm * n / dt
+    sample = (f"reference cpucal::dedispered_fil_omp (brute force, the reference's CPU path) on "
+              f"the first {n} samples x {nchans} channels, all {ndm} DM trials, "
+              f"{threads} OpenMP threads")
+    return rate, threads, sample, dt
+
+
+# ---------------------------------------------------------------- helpers
+def roofline_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+def make_plan(wl, hdr, device):
+    from astroflow_b200.dedisp import IqrmParams, Plan, RfiParams
+
+    lo, hi, step = wl["dm"]
+    freq_lo = float(np.float32(np.float32(hdr["fch1"])))
+    nch = hdr["nchans"]
+    f32 = np.float32
+    top = float(f32(f32(hdr["fch1"]) + f32(nch - 1) * f32(hdr["foff"])))
+    rfi = None
+    if wl["rfi"]:
+        r = wl["rfi"]
+        rfi = RfiParams(use_mask=r["use_mask"], use_zero_dm=r["use_zero_dm"],
+                        use_iqrm=r["use_iqrm"], iqrm=IqrmParams(**r["iqrm"]))
+    if wl["algorithm"] == "brute":
+        return Plan(hdr, lo, hi, freq_lo, top, step, wl["ds"], hdr["nsamp_total_s"],
+                    algorithm="brute", freq_mode="fil", device=device)
+    return Plan(hdr, lo, hi, freq_lo, top, step, wl["ds"], algorithm="subband",
+                subband_width=wl["subband_width"], rfi=rfi, device=device)
+
+
+def e2e_run(plan, x, out, units, dist, dev, stream, steps):
+    """The workload's metric through dd_run_host with pinned host buffers (host->device
+    copy, run, device->host copy inside the timed region).  Returns (e2e dict, whether
+    the host path's first rows equal the device-resident run's)."""
+    import torch
+
+    h_in = torch.empty(tuple(x.shape), dtype=x.dtype, pin_memory=True)
+    h_in.copy_(x)
+    h_out = torch.empty(plan.out_shape, dtype=out.dtype, pin_memory=True)
+    h_in_np = h_in.view(torch.uint8).numpy() if x.dtype == torch.uint8 else h_in.view(torch.int16).numpy().view(np.uint16)
+    h_out_np = h_out.view(torch.int32).numpy().view(np.uint32)
+    plan.run_host(h_in_np, h_out_np, stream)  # warm-up (allocator pool, caches)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(steps):
+        plan.run_host(h_in_np, h_out_np, stream)
+    e3.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = dist.max(e2.elapsed_time(e3) / steps)
+    e2e = {"value": dist.world * units / (e2e_ms * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": int(h_in.numel() * h_in.element_size()),
+           "d2h_bytes_per_step": int(h_out.numel() * h_out.element_size()),
+           "ms_per_step": e2e_ms}
+    # bit-level spot check of the host path against the device run
+    same = bool(torch.equal(h_out[:4].to(dev).view(torch.int32), out[:4].view(torch.int32)))
+    return e2e, same
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    wl = WORKLOADS[args.workload]
+
+    import torch
+
+    from astroflow_b200.synth import ChunkSpec, make_chunk_device
+
+    dist = Dist(args.gpus)
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    spec = ChunkSpec(nchans=wl["nchans"], nsamp=wl["nsamp"], nbits=wl["nbits"], seed=1234 + dist.rank,
+                     **wl["chunk"])
+    hdr = spec.header()
+    f32 = np.float32
+    # the Header the reference's _dedisperse_spec path receives holds float fields
+    hdr.update(tsamp=float(f32(hdr["tsamp"])), fch1=float(f32(hdr["fch1"])),
+               foff=float(f32(hdr["foff"])), nsamp_total_s=float(f32(hdr["ndata"] * hdr["tsamp"] * 0.999)))
+    config = {"workload": args.workload, "nchans": wl["nchans"], "nsamp": wl["nsamp"],
+              "nbits": wl["nbits"], "dm_low": wl["dm"][0], "dm_high": wl["dm"][1],
+              "dm_step": wl["dm"][2], "algorithm": wl["algorithm"],
+              "subband_width": wl["subband_width"] if wl["algorithm"] == "subband" else None,
+              "rfi": "iqrm(std, radius 5 lags, 3 sigma) + zero-DM (reference call-site semantics)"
+                     if wl["rfi"] else "off",
+              "l2": "inputs larger than L2 (chunk >> 126 MB), no flush between steps",
+              "parallelism": f"replicas x{dist.world} (independent chunks, no exchange)"}
+
+    if args.impl == "reference":
+        if dist.rank != 0:
+            dist.close()
+            return
+        x, _ = make_chunk_device(spec, dev)
+        nsamp_sample = min(wl["nsamp"], 1 << 14)
+        x_host = x[:nsamp_sample].cpu().numpy()
+        del x
+        from oracle import oracle as O
+
+        if not O.ref_cpu_available():
+            print(json.dumps({"impl": "reference", "unavailable": "reference CPU build "
+                              "oracle/_ref/libref_cpu.so is missing (build with make -C oracle ref)"}))
+            return
+        for _ in range(args.warmup):
+            reference_cpu_rate(x_host, hdr, wl, target_s=2.0)
+        rates, secs = [], []
+        for _ in range(args.steps):
+            r, threads, sample, dt = reference_cpu_rate(x_host, hdr, wl, target_s=6.0)
+            rates.append(r)
+            secs.append(dt)
+        value = float(np.median(rates))
+        ms = 1e3 * wl["nsamp"] * O.dm_steps(*wl["dm"]) / value
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+                "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                                 "kind": "reference", "sample": sample},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0},
+                "note": "each step times one bounded sample; ms_per_step extrapolates the rate "
+                        "to the full workload"}
+        print(json.dumps(line))
+        return
+
+    # ------------------------------------------------------------ our arm
+    from astroflow_b200.dedisp import measure_int_add_rate
+
+    x, _ = make_chunk_device(spec, dev)
+    plan = make_plan(wl, hdr, dev)
+    out = plan.empty_output()
+    stream = torch.cuda.current_stream(dev)
+    units = plan.out_shape[0] * plan.out_shape[1]
+    for _ in range(args.warmup):
+        plan.run(x, out)
+    torch.cuda.synchronize(dev)
+
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.3)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    e0.record(stream)
+    for _ in range(args.steps):
+        stats.append(plan.run_profiled(x, out, stream))
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms = dist.max(ms)
+    value = dist.world * units / (ms * 1e-3)
+
+    # per-stage breakdown from the timed steps (device time, CUDA events on the run's stream)
+    st = {k: float(np.mean([s[k] for s in stats])) for k in ("total_ms", "prep_ms", "stage1_ms", "stage2_ms")}
+    launches = int(sum(s["launches"] for s in stats))
+    s1n, s2n = stats[0]["stage1_launches"], stats[0]["stage2_launches"]
+    info = plan.info
+    hbm_peak, peak_kind = roofline_peaks()
+    add_peak = measure_int_add_rate(dev)
+    bytes_per_unit = (wl["nsamp"] * wl["nchans"] * wl["nbits"] / 8 + units * 4) / units
+    if wl["algorithm"] == "subband":
+        tile = min(int(info["nsamp_binned"]), int(info["tile_samples"]))
+        if st["stage1_ms"] >= st["stage2_ms"]:
+            kname, kms, kn = "stage1", st["stage1_ms"], s1n
+            adds_launch = info["ndm_nom"] * (info["chan_end"] - info["chan_start"] + 1) * tile
+        else:
+            kname, kms, kn = "stage2", st["stage2_ms"], s2n
+            adds_launch = info["dm_steps"] * info["nsb"] * tile
+        units_launch = info["dm_steps"] * tile
+    else:
+        kname, kms, kn = "brute", st["stage2_ms"], s2n
+        units_launch = units / max(kn, 1)
+        adds_launch = info["adds_per_run"] / max(kn, 1)
+    avg_launch_s = kms / max(kn, 1) * 1e-3
+    achieved = units_launch * bytes_per_unit / avg_launch_s / 1e9
+    adds_rate = adds_launch / avg_launch_s
+    step_adds = info["adds_per_run"] / (st["total_ms"] * 1e-3)
+    roof_time = max(units * bytes_per_unit / (hbm_peak * 1e9), info["adds_per_run"] / add_peak)
+    roofline = {
+        "bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+        "frac": achieved / hbm_peak, "peak_kind": peak_kind,
+        "traffic": ncu_traffic(kname),
+        "bytes_per_unit": bytes_per_unit, "units_per_launch": units_launch,
+        "avg_launch_ms": avg_launch_s * 1e3,
+        "int_add": {"achieved": adds_rate, "peak": add_peak, "unit": "adds/s",
+                    "frac": adds_rate / add_peak, "peak_kind": "measured live (IADD3 probe)"},
+        "binding": "int_add" if info["adds_per_run"] / add_peak > units * bytes_per_unit / (hbm_peak * 1e9) else "hbm",
+        "step_frac": roof_time / (st["total_ms"] * 1e-3),
+        "step_adds_per_s": step_adds,
+        "stages_ms": st,
+    }
+
+    # e2e: same metric through the C ABI with host buffers (pinned), copies in the timed region
+    e2e, same = None, None
+    if args.e2e_steps > 0:
+        e2e, same = e2e_run(plan, x, out, units, dist, dev, stream, args.e2e_steps)
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        if O.ref_cpu_available():
+            x_host = x[: min(wl["nsamp"], 1 << 14)].cpu().numpy()
+            rate, threads, sample, dt = reference_cpu_rate(x_host, hdr, wl, target_s=12.0)
+            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": sample, "seconds": dt}
+    dist.barrier()
+    if dist.rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": f"u{wl['nbits']}", "data": "synthetic (seeded, generated on the GPU)",
+                "config": config, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": clk,
+                "host_path_matches_device": same}
+        print(json.dumps(line))
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -156,6 +156,7 @@ typedef struct dd_plan_info {
   int64_t delay_rows;        /* rows of the delay table (ndm_nom or dm_steps) */
   int64_t delay_cols;        /* columns of the delay table (channels) */
   int64_t table_mismatch_fp64; /* delay entries where the table differs from the FP64 table */
+  int64_t tile_samples;      /* time samples per stage-1/stage-2 launch (subband) */
   double adds_per_run;       /* algorithmic integer additions per dd_run */
 } dd_plan_info;
 
@@ -197,6 +198,28 @@ int dd_run_ex(dd_plan* plan, const void* input, void* output, uint8_t* iqrm_mask
 /* dd_run from host memory: copies input in, runs, copies the output back and
  * synchronises the stream.  Host buffers may be pageable or pinned. */
 int dd_run_host(dd_plan* plan, const void* h_input, void* h_output, void* stream);
+
+/* Device-time breakdown of one run, measured with CUDA events on the run's
+ * stream (the role of the reference's AF_DEBUG stage timers,
+ * dedispered.cu:41-73, without their device-wide synchronisations). */
+typedef struct dd_run_stats {
+  float total_ms;          /* the whole run */
+  float prep_ms;           /* binning, RFI stages and layout */
+  float stage1_ms;         /* subband stage 1, all time tiles */
+  float stage2_ms;         /* subband stage 2 or brute-force sums, all time tiles */
+  int32_t launches;        /* kernels this library launched */
+  int32_t stage1_launches;
+  int32_t stage2_launches;
+} dd_run_stats;
+
+/* dd_run that also fills `stats`; synchronises the stream before returning. */
+int dd_run_profiled(dd_plan* plan, const void* input, void* output, void* stream,
+                    dd_run_stats* stats);
+
+/* Measures this GPU's sustained 32-bit integer addition rate (additions per
+ * second, a three-input add counted as two) with a register-resident kernel;
+ * the denominator of the add-bound roofline of the dedispersion sums. */
+int dd_measure_int_add_rate(int32_t device, double* adds_per_second);
 
 /* Last error message of the calling thread ("" if none). */
 const char* dd_last_error(void);
