@@ -330,9 +330,16 @@ void create_subband(dd_plan& P) {
   // halo (max_res extra samples per tile) stays small, short enough that one
   // tile of subband sums stays below ~1 GiB.
   const int64_t per_col = P.ndm_nom * P.nsb * (P.inter16 ? 2 : 4);
-  int64_t L = std::max<int64_t>(kT, round_up(std::max<int64_t>(16 * P.max_res, 8 * kT), kT));
-  while (L > kT && L * per_col > (int64_t(1) << 30)) L -= kT;
-  L = std::min<int64_t>(L, round_up(P.nbin, kT));
+  // Tile length L plus the stage-2 halo (max_res) should fill whole stage-1 block
+  // tiles T1: L = n*T1 - R with R the halo rounded to the base tile.  n grows
+  // while one tile of subband sums stays within 1 GiB and the tile is not
+  // longer than the chunk.
+  const int64_t T1 = P.win1 ? sum_variant_tile(P.elem, P.nbits == 8 && !P.inter16) : kT;
+  const int64_t R = round_up(std::max<int64_t>(P.max_res, 1), kT);
+  int64_t n = 1;
+  while (n * T1 - R < kT) ++n;
+  while (((n + 1) * T1 - R) * per_col <= (int64_t(1) << 30) && (n * T1 - R) < P.nbin) ++n;
+  int64_t L = std::max<int64_t>(kT, n * T1 - R);
   P.tile = L;
   P.tile_pitch = round_up(round_up(L + P.max_res, kT) + 64, 64);
   const int64_t ntiles = (P.nbin + L - 1) / L;

@@ -103,60 +103,53 @@ __device__ __forceinline__ Geo make_geo(const SumLaunch& L, int T) {
   return g;
 }
 
-// Stage the windows of sources i, i+1 into buf (windows of win_bytes each).
-// orow receives, per source and row, the byte offset of the row's sample 0 in
-// the staged window.
+// Stage the windows of sources i, i+1 into words [wbase_s, wbase_s + win_words) of
+// the shared array (one window per source), and publish, for every row, the
+// word index and byte shift of its sample 0 inside the window.
 template <int SB, int RB>
-__device__ __forceinline__ void stage_pair(const Geo& g, int i, char* buf, int win_bytes,
-                                           int tile_bytes, int (&orow)[2][RB]) {
+__device__ __forceinline__ void stage_pair(const Geo& g, int i, uint32_t* sw, int win_words,
+                                           int tile_bytes, int* rowq, int* rowsh) {
 #pragma unroll
   for (int s = 0; s < 2; ++s) {
     const int src = i + s;
     if (src >= g.nsrc) {
-#pragma unroll
-      for (int r = 0; r < RB; ++r) orow[s][r] = 0;
+      if (threadIdx.x < RB) { rowq[s * RB + threadIdx.x] = 0; rowsh[s * RB + threadIdx.x] = 0; }
       continue;
     }
     int lo = 0x7fffffff, hi = -0x7fffffff;
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
-      const int o = r < g.nrows ? __ldg(g.off + r * g.off_pitch + src) : 0;
-      orow[s][r] = o;
-      if (r < g.nrows) { lo = min(lo, o); hi = max(hi, o); }
+      if (r < g.nrows) {
+        const int o = __ldg(g.off + r * g.off_pitch + src);
+        lo = min(lo, o);
+        hi = max(hi, o);
+      }
     }
-    // Rows past nrows are summed too (their results are never stored): give them
-    // the window's first offset so every shared-memory read stays inside it.
-#pragma unroll
-    for (int r = 0; r < RB; ++r)
-      if (r >= g.nrows) orow[s][r] = lo;
     const int64_t first = (g.base + lo) * SB;
     const int64_t a0 = first & ~int64_t(15);
     const int64_t last = (g.base + hi) * SB + tile_bytes + 8;  // + the funnel's second word
     const int nbytes = static_cast<int>((last - a0 + 15) & ~int64_t(15));
     const char* gsrc = g.src + static_cast<int64_t>(src) * g.src_pitch + a0;
-    char* dst = buf + s * win_bytes;
-    for (int b = threadIdx.x * 16; b < nbytes; b += kThreads * 16) cp_async16(dst + b, gsrc + b);
-    const int delta = static_cast<int>(first - a0) - lo * SB;
-#pragma unroll
-    for (int r = 0; r < RB; ++r) orow[s][r] = orow[s][r] * SB + delta;
+    uint32_t* dst = sw + s * win_words;
+    for (int b = threadIdx.x * 16; b < nbytes; b += kThreads * 16)
+      cp_async16(reinterpret_cast<char*>(dst) + b, gsrc + b);
+    if (threadIdx.x < RB) {
+      // Rows past nrows are summed too (their results are never stored); they
+      // take the window's first offset so their reads stay inside the window.
+      const int r = threadIdx.x;
+      const int o = r < g.nrows ? __ldg(g.off + r * g.off_pitch + src) : lo;
+      const int ob = static_cast<int>(first - a0) + (o - lo) * SB;  // byte offset of sample 0
+      rowq[s * RB + r] = s * win_words + (ob >> 2);
+      rowsh[s * RB + r] = (ob & 3) * 8;
+    }
   }
-}
-
-__device__ __forceinline__ uint32_t lds32(const char* p) { return *reinterpret_cast<const uint32_t*>(p); }
-
-// The 32-bit sample word at byte offset ob + 4*w of a staged window.
-__device__ __forceinline__ uint32_t fetch(const char* win, int ob, int w) {
-  const int b = ob + w * 4;
-  const uint32_t sh = static_cast<uint32_t>(b & 3) * 8u;
-  const char* q = win + (b & ~3);
-  const uint32_t lo = lds32(q);
-  return sh ? __funnelshift_r(lo, lds32(q + 4), sh) : lo;
 }
 
 // ------------------------------------------------------------------ 8-bit samples
 template <int RB, int NW, bool OUT16, bool FLUSH>
 __global__ void __launch_bounds__(kThreads) k_sum_u8(SumLaunch L) {
-  extern __shared__ __align__(16) char smem[];
+  extern __shared__ __align__(16) uint32_t sw[];
+  __shared__ int rowq[2][2 * RB], rowsh[2][2 * RB];
   constexpr int T = kWarps * 32 * NW * 4;
   const Geo g = make_geo(L, T);
   if (g.nrows <= 0) return;
@@ -174,35 +167,31 @@ __global__ void __launch_bounds__(kThreads) k_sum_u8(SumLaunch L) {
 #pragma unroll
       for (int k = 0; k < NW * 4; ++k) w32[r][k] = 0;
   }
-  int oA[2][RB], oB[2][RB];  // row offsets of the pair staged in buffer A / B
-  const int wb = L.win_bytes;
-  char* const bufA = smem;
-  char* const bufB = smem + 2 * wb;
+  const int ww = L.win_bytes >> 2;  // words per window
   const int npairs = (g.nsrc + 1) / 2;
   int since = 0;
-  auto consume = [&](const char* w0, const int (&o)[2][RB], int p) {
-    const char* w1 = w0 + wb;
-    if (2 * p + 1 < g.nsrc) {
+  stage_pair<1, RB>(g, 0, sw, ww, T, rowq[0], rowsh[0]);
+  cp_async_commit();
+  for (int p = 0; p < npairs; ++p) {
+    const int cur = p & 1;
+    if (p + 1 < npairs)
+      stage_pair<1, RB>(g, 2 * (p + 1), sw + (cur ^ 1) * 2 * ww, ww, T, rowq[cur ^ 1], rowsh[cur ^ 1]);
+    cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    const uint32_t* win = sw + cur * 2 * ww;
+    const bool two = 2 * p + 1 < g.nsrc;
 #pragma unroll
-      for (int r = 0; r < RB; ++r) {
+    for (int r = 0; r < RB; ++r) {
+      const int q0 = rowq[cur][r] + wbase, q1 = rowq[cur][RB + r] + wbase;
+      const uint32_t s0 = rowsh[cur][r], s1 = rowsh[cur][RB + r];
 #pragma unroll
-        for (int k = 0; k < NW; ++k) {
-          const int w = wbase + 32 * k;
-          const uint32_t a = fetch(w0, o[0][r], w);
-          const uint32_t b = fetch(w1, o[1][r], w);
-          ev[r][k] += __byte_perm(a, 0u, 0x4240) + __byte_perm(b, 0u, 0x4240);
-          od[r][k] += __byte_perm(a, 0u, 0x4341) + __byte_perm(b, 0u, 0x4341);
-        }
-      }
-    } else {
-#pragma unroll
-      for (int r = 0; r < RB; ++r) {
-#pragma unroll
-        for (int k = 0; k < NW; ++k) {
-          const uint32_t a = fetch(w0, o[0][r], wbase + 32 * k);
-          ev[r][k] += __byte_perm(a, 0u, 0x4240);
-          od[r][k] += __byte_perm(a, 0u, 0x4341);
-        }
+      for (int k = 0; k < NW; ++k) {
+        const uint32_t a = __funnelshift_r(win[q0 + 32 * k], win[q0 + 32 * k + 1], s0);
+        uint32_t b = __funnelshift_r(win[q1 + 32 * k], win[q1 + 32 * k + 1], s1);
+        b = two ? b : 0u;
+        ev[r][k] += __byte_perm(a, 0u, 0x4240) + __byte_perm(b, 0u, 0x4240);
+        od[r][k] += __byte_perm(a, 0u, 0x4341) + __byte_perm(b, 0u, 0x4341);
       }
     }
     if constexpr (FLUSH) {
@@ -219,23 +208,6 @@ __global__ void __launch_bounds__(kThreads) k_sum_u8(SumLaunch L) {
         since = 0;
       }
     }
-  };
-  // Buffers alternate A, B, A, ...: pair p is staged while pair p-1 is summed.
-  stage_pair<1, RB>(g, 0, bufA, wb, T, oA);
-  cp_async_commit();
-  for (int p = 0; p < npairs; p += 2) {
-    if (p + 1 < npairs) stage_pair<1, RB>(g, 2 * (p + 1), bufB, wb, T, oB);
-    cp_async_commit();
-    cp_async_wait1();
-    __syncthreads();
-    consume(bufA, oA, p);
-    __syncthreads();
-    if (p + 1 >= npairs) break;
-    if (p + 2 < npairs) stage_pair<1, RB>(g, 2 * (p + 2), bufA, wb, T, oA);
-    cp_async_commit();
-    cp_async_wait1();
-    __syncthreads();
-    consume(bufB, oB, p + 1);
     __syncthreads();
   }
 #pragma unroll
@@ -282,7 +254,8 @@ __global__ void __launch_bounds__(kThreads) k_sum_u8(SumLaunch L) {
 // L.lane_per: sources summed in 16-bit lanes before widening (< 2: 32-bit sums).
 template <int RB, int NW>
 __global__ void __launch_bounds__(kThreads) k_sum_u16(SumLaunch L) {
-  extern __shared__ __align__(16) char smem[];
+  extern __shared__ __align__(16) uint32_t sw[];
+  __shared__ int rowq[2][2 * RB], rowsh[2][2 * RB];
   constexpr int T = kWarps * 32 * NW * 2;
   const Geo g = make_geo(L, T);
   if (g.nrows <= 0) return;
@@ -293,23 +266,31 @@ __global__ void __launch_bounds__(kThreads) k_sum_u16(SumLaunch L) {
   for (int r = 0; r < RB; ++r)
 #pragma unroll
     for (int k = 0; k < NW; ++k) a16[r][k] = lo32[r][k] = hi32[r][k] = 0;
-  int oA[2][RB], oB[2][RB];
-  const int wb = L.win_bytes;
-  char* const bufA = smem;
-  char* const bufB = smem + 2 * wb;
+  const int ww = L.win_bytes >> 2;
   const int npairs = (g.nsrc + 1) / 2;
   const int per = L.lane_per;
   int since = 0;
-  auto consume = [&](const char* w0, const int (&o)[2][RB], int p) {
-    const char* w1 = w0 + wb;
+  stage_pair<2, RB>(g, 0, sw, ww, 2 * T, rowq[0], rowsh[0]);
+  cp_async_commit();
+  for (int p = 0; p < npairs; ++p) {
+    const int cur = p & 1;
+    if (p + 1 < npairs)
+      stage_pair<2, RB>(g, 2 * (p + 1), sw + (cur ^ 1) * 2 * ww, ww, 2 * T, rowq[cur ^ 1], rowsh[cur ^ 1]);
+    cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    const uint32_t* win = sw + cur * 2 * ww;
     const bool two = 2 * p + 1 < g.nsrc;
     if (per >= 2) {
 #pragma unroll
       for (int r = 0; r < RB; ++r) {
+        const int q0 = rowq[cur][r] + wbase, q1 = rowq[cur][RB + r] + wbase;
+        const uint32_t s0 = rowsh[cur][r], s1 = rowsh[cur][RB + r];
 #pragma unroll
         for (int k = 0; k < NW; ++k) {
-          const int w = wbase + 32 * k;
-          a16[r][k] += fetch(w0, o[0][r], w) + (two ? fetch(w1, o[1][r], w) : 0u);
+          const uint32_t a = __funnelshift_r(win[q0 + 32 * k], win[q0 + 32 * k + 1], s0);
+          const uint32_t b = __funnelshift_r(win[q1 + 32 * k], win[q1 + 32 * k + 1], s1);
+          a16[r][k] += a + (two ? b : 0u);
         }
       }
       since += 2;
@@ -327,32 +308,18 @@ __global__ void __launch_bounds__(kThreads) k_sum_u16(SumLaunch L) {
     } else {
 #pragma unroll
       for (int r = 0; r < RB; ++r) {
+        const int q0 = rowq[cur][r] + wbase, q1 = rowq[cur][RB + r] + wbase;
+        const uint32_t s0 = rowsh[cur][r], s1 = rowsh[cur][RB + r];
 #pragma unroll
         for (int k = 0; k < NW; ++k) {
-          const int w = wbase + 32 * k;
-          const uint32_t a = fetch(w0, o[0][r], w);
-          const uint32_t b = two ? fetch(w1, o[1][r], w) : 0u;
+          const uint32_t a = __funnelshift_r(win[q0 + 32 * k], win[q0 + 32 * k + 1], s0);
+          uint32_t b = __funnelshift_r(win[q1 + 32 * k], win[q1 + 32 * k + 1], s1);
+          b = two ? b : 0u;
           lo32[r][k] += (a & 0xffffu) + (b & 0xffffu);
           hi32[r][k] += (a >> 16) + (b >> 16);
         }
       }
     }
-  };
-  stage_pair<2, RB>(g, 0, bufA, wb, 2 * T, oA);
-  cp_async_commit();
-  for (int p = 0; p < npairs; p += 2) {
-    if (p + 1 < npairs) stage_pair<2, RB>(g, 2 * (p + 1), bufB, wb, 2 * T, oB);
-    cp_async_commit();
-    cp_async_wait1();
-    __syncthreads();
-    consume(bufA, oA, p);
-    __syncthreads();
-    if (p + 1 >= npairs) break;
-    if (p + 2 < npairs) stage_pair<2, RB>(g, 2 * (p + 2), bufA, wb, 2 * T, oA);
-    cp_async_commit();
-    cp_async_wait1();
-    __syncthreads();
-    consume(bufB, oB, p + 1);
     __syncthreads();
   }
 #pragma unroll
