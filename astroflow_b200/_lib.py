@@ -27,7 +27,8 @@ FREQ_HEADER, FREQ_FIL = 0, 1
 # Every symbol include/astroflow_dd.h declares.
 EXPORTS = ("dd_plan_create", "dd_plan_destroy", "dd_plan_get_info", "dd_plan_get_tables",
            "dd_plan_set_delay_table", "dd_run", "dd_run_ex", "dd_run_host", "dd_run_profiled",
-           "dd_measure_int_add_rate", "dd_last_error", "dd_abi_version")
+           "dd_measure_int_add_rate", "dd_iqrm_masks_noalloc", "dd_last_error",
+           "dd_abi_version")
 
 
 class Header(ctypes.Structure):
@@ -99,6 +100,10 @@ def load():
     L.dd_run_host.argtypes = [P, P, P, P]
     L.dd_run_profiled.argtypes = [P, P, P, P, ctypes.POINTER(RunStats)]
     L.dd_measure_int_add_rate.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
+    L.dd_iqrm_masks_noalloc.argtypes = [P, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                        ctypes.POINTER(IqrmConfig), P, P, ctypes.c_int32,
+                                        ctypes.POINTER(ctypes.c_int32), P]
     L.dd_last_error.restype = ctypes.c_char_p
     L.dd_abi_version.restype = ctypes.c_int
     for name in EXPORTS:

@@ -36,6 +36,7 @@ UNITS = [
     ("dd_dedisp.cu", []),
     ("dd_probe.cu", []),
     ("dd_sumsmem.cu", []),
+    ("dd_noalloc.cu", []),
 ]
 HOST = ["dd_api.cpp"]
 HEADERS = ["dd_internal.h", os.path.join("..", "..", "include", "astroflow_dd.h")]

@@ -184,6 +184,28 @@ class Plan:
             pass
 
 
+def iqrm_masks_noalloc(x, nchans: int, chan_start: int, chan_end: int, tsamp: float,
+                       iqrm: IqrmParams, masks, bounds, stream=None) -> int:
+    """IQRM window masks through dd_iqrm_masks_noalloc: no device memory is
+    allocated by the library; `masks` ([max_windows, nchans] uint8) and `bounds`
+    ([max_windows, 2] int32/uint32) are caller-owned device tensors on the current
+    device.  For callers that cannot allocate while they run (deadline-bound
+    real-time loops, frameworks that own the GPU's memory).  Calls share one
+    static scratch array per GPU, so their GPU work must not overlap.  Returns
+    the number of windows."""
+    torch = _torch()
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    n = ctypes.c_int32()
+    q = _lib.IqrmConfig(int(iqrm.mode), iqrm.radius_frac, iqrm.nsigma, iqrm.geofactor,
+                        iqrm.win_sec, iqrm.hop_sec, int(bool(iqrm.include_tail)))
+    _lib.check(_lib.load().dd_iqrm_masks_noalloc(
+        x.data_ptr(), x.element_size() * 8, x.numel() // nchans, nchans, chan_start, chan_end,
+        tsamp, ctypes.byref(q), masks.data_ptr(), bounds.data_ptr(), masks.shape[0],
+        ctypes.byref(n), ctypes.c_void_p(stream.cuda_stream)))
+    return n.value
+
+
 def measure_int_add_rate(device: int = 0) -> float:
     """Sustained 32-bit integer additions per second on `device` (library probe)."""
     v = ctypes.c_double()

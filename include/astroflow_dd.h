@@ -221,6 +221,32 @@ int dd_run_profiled(dd_plan* plan, const void* input, void* output, void* stream
  * the denominator of the add-bound roofline of the dedispersion sums. */
 int dd_measure_int_add_rate(int32_t device, double* adds_per_second);
 
+/* IQRM channel masks of one chunk computed without allocating any device
+ * memory.  It has no counterpart in the reference (whose IQRM, iqrm.cu:203-345,
+ * allocates and frees device buffers on every call); it serves callers that
+ * cannot allocate while they run, such as real-time pipelines whose deadlines
+ * forbid cudaMalloc/cudaFree (both may synchronise the device) and host
+ * frameworks that have already reserved the GPU's memory for their own pools.
+ *
+ * input: device [nsamp][nchans] samples of nbits (the chunk as the IQRM stage
+ * sees it, after any time binning); channels [chan_start, chan_end) are
+ * examined (chan_end exclusive, as the reference's IQRM takes it); tsamp is the
+ * sampling time of `input` in seconds.  Outputs (device, caller-owned): masks
+ * [max_windows][nchans] uint8 and bounds [max_windows][2] uint32 (t0, t1), the
+ * same values dd_run_ex reports; *n_windows (host) receives the window count.
+ * Runs on the calling thread's current device, on `stream`.
+ *
+ * All working memory comes from an 8 MiB array that the library places in
+ * every GPU's memory for the life of the process; requests whose working set
+ * exceeds it fail with DD_ERR_INVALID.  The first call on a device resolves the
+ * array's address with that device current: make it before any stream capture.
+ * Calls share the array, so calls whose GPU work overlaps race with each other
+ * and must be serialised by the caller. */
+int dd_iqrm_masks_noalloc(const void* input, int32_t nbits, int64_t nsamp, int32_t nchans,
+                          int32_t chan_start, int32_t chan_end, double tsamp,
+                          const dd_iqrm_config* cfg, uint8_t* masks, uint32_t* bounds,
+                          int32_t max_windows, int32_t* n_windows, void* stream);
+
 /* Last error message of the calling thread ("" if none). */
 const char* dd_last_error(void);
 int dd_abi_version(void);
