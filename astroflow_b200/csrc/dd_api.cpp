@@ -329,7 +329,10 @@ void create_subband(dd_plan& P) {
   // Time tile of the stage-1 -> stage-2 pipeline: long enough that the stage-1
   // halo (max_res extra samples per tile) stays small, short enough that one
   // tile of subband sums stays below ~1 GiB.
-  const int64_t per_col = P.ndm_nom * P.nsb * (P.inter16 ? 2 : 4);
+  // Subband sums: uint16 for 8-bit samples in narrow subbands, else the
+  // reference's accumulator type (uint32, or uint64 for 32-bit samples).
+  const int64_t inter_elem = P.inter16 ? 2 : (P.nbits == 32 ? 8 : 4);
+  const int64_t per_col = P.ndm_nom * P.nsb * inter_elem;
   // Tile length L plus the stage-2 halo (max_res) should fill whole stage-1 block
   // tiles T1: L = n*T1 - R with R the halo rounded to the base tile.  n grows
   // while one tile of subband sums stays within 1 GiB and the tile is not
@@ -346,7 +349,7 @@ void create_subband(dd_plan& P) {
   P.xpitch = round_up(ntiles * L + round_up(L + P.max_res, 8192) + P.max_delay + 8192, 64);
   P.d_x.alloc(static_cast<size_t>(P.dch * P.xpitch) * P.elem);
   DD_CUDA_TRY(cudaMemset(P.d_x.p, 0, P.d_x.bytes));
-  P.d_inter.alloc(static_cast<size_t>(P.ndm_nom * P.nsb * P.tile_pitch) * (P.inter16 ? 2 : 4));
+  P.d_inter.alloc(static_cast<size_t>(P.ndm_nom * P.nsb * P.tile_pitch) * inter_elem);
   DD_CUDA_TRY(cudaMemset(P.d_inter.p, 0, P.d_inter.bytes));
   if (ds > 1 || callsite_zdm_active(P))
     P.d_binned.alloc(static_cast<size_t>(P.nbin * P.hdr.nchans) * P.elem);
@@ -572,7 +575,7 @@ void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out
     s2.out = output;
     s2.out_pitch = P.nbin;
     s2.col0 = t0;
-    s2.out64 = 0;
+    s2.out64 = P.nbits == 32 ? 1 : 0;
     s2.sbw = P.sbw;
     s2.src_max = P.sbw * 255;
     cudaEvent_t b2 = pf ? pf->mark() : nullptr;
@@ -789,7 +792,6 @@ int dd_plan_create(const dd_header* header, const dd_plan_params* params,
     if (P->p.algorithm == DD_ALGO_BRUTE) {
       create_brute(*P);
     } else if (P->p.algorithm == DD_ALGO_SUBBAND) {
-      if (P->nbits == 32) throw Error{DD_ERR_UNSUPPORTED, "32-bit samples are supported by the brute-force algorithm only"};
       create_subband(*P);
       create_rfi(*P);
     } else {

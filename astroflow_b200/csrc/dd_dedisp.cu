@@ -277,6 +277,84 @@ __global__ void __launch_bounds__(kThreads) k_stage2(Stage2Args a) {
   }
 }
 
+// ---------------------------------------------------------------- 32-bit samples
+// For 32-bit samples the subband sums and the output are 64-bit
+// (dedispersion_output_t<uint32_t> is uint64_t, include/data.h:98-118).  Four
+// rows per block keep the 64-bit accumulators in registers.
+constexpr int kRows64 = 4;
+
+__global__ void __launch_bounds__(kThreads) k_stage1_u32(Stage1Args a) {
+  const int64_t t_local = static_cast<int64_t>(blockIdx.x) * kTile + threadIdx.x * kRun;
+  const int64_t j0 = static_cast<int64_t>(blockIdx.y) * kRows64;
+  const int64_t sb = blockIdx.z;
+  const int64_t c0 = sb * a.sbw;
+  const int64_t c1 = c0 + a.sbw < a.dch ? c0 + a.sbw : a.dch;
+  const uint32_t* x = static_cast<const uint32_t*>(a.x);
+  unsigned long long acc[kRows64][kRun];
+#pragma unroll
+  for (int r = 0; r < kRows64; ++r)
+#pragma unroll
+    for (int k = 0; k < kRun; ++k) acc[r][k] = 0;
+  const int64_t nrows = a.ndm_nom - j0 < kRows64 ? a.ndm_nom - j0 : kRows64;
+  for (int64_t c = c0; c < c1; ++c) {
+    const uint32_t* row = x + c * a.xpitch;
+#pragma unroll
+    for (int r = 0; r < kRows64; ++r) {
+      if (r < nrows) {
+        const int64_t pos = a.t0 + t_local + __ldg(a.delay1 + (j0 + r) * a.dch + c);
+#pragma unroll
+        for (int k = 0; k < kRun; ++k) acc[r][k] += __ldg(row + pos + k);
+      }
+    }
+  }
+  const int64_t valid = a.ncols - t_local;
+  if (valid <= 0) return;
+  for (int r = 0; r < nrows; ++r) {
+    unsigned long long* dst = static_cast<unsigned long long*>(a.inter) +
+                              ((j0 + r) * a.nsb + sb) * a.tile_pitch + t_local;
+#pragma unroll
+    for (int k = 0; k < kRun; ++k)
+      if (k < valid) dst[k] = acc[r][k];
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_stage2_u64(Stage2Args a) {
+  const int64_t t_local = static_cast<int64_t>(blockIdx.x) * kTile + threadIdx.x * kRun;
+  const int blocks_per_nom = (a.ndm0 + kRows64 - 1) / kRows64;
+  const int64_t j = blockIdx.y / blocks_per_nom;
+  const int64_t m0 = j * a.ndm0 + static_cast<int64_t>(blockIdx.y % blocks_per_nom) * kRows64;
+  const int64_t mend_nom = (j + 1) * a.ndm0 < a.dm_steps ? (j + 1) * a.ndm0 : a.dm_steps;
+  const int64_t nrows = mend_nom - m0 < kRows64 ? mend_nom - m0 : kRows64;
+  if (nrows <= 0) return;
+  unsigned long long acc[kRows64][kRun];
+#pragma unroll
+  for (int r = 0; r < kRows64; ++r)
+#pragma unroll
+    for (int k = 0; k < kRun; ++k) acc[r][k] = 0;
+  const unsigned long long* inter =
+      static_cast<const unsigned long long*>(a.inter) + j * a.nsb * a.tile_pitch;
+  for (int64_t sb = 0; sb < a.nsb; ++sb) {
+    const unsigned long long* row = inter + sb * a.tile_pitch;
+#pragma unroll
+    for (int r = 0; r < kRows64; ++r) {
+      if (r < nrows) {
+        const int64_t pos = t_local + __ldg(a.res + (m0 + r) * a.nsb + sb);
+#pragma unroll
+        for (int k = 0; k < kRun; ++k) acc[r][k] += __ldg(row + pos + k);
+      }
+    }
+  }
+  const int64_t valid = a.ncols - t_local;
+  if (valid <= 0) return;
+  for (int r = 0; r < nrows; ++r) {
+    unsigned long long* dst =
+        static_cast<unsigned long long*>(a.out) + (m0 + r) * a.out_pitch + a.col0 + t_local;
+#pragma unroll
+    for (int k = 0; k < kRun; ++k)
+      if (k < valid) dst[k] = acc[r][k];
+  }
+}
+
 // ---------------------------------------------------------------- brute force
 // grid: x = time tile of the slice, y = block of kRows DMs.
 template <typename T>
@@ -375,17 +453,24 @@ __global__ void __launch_bounds__(kThreads) k_brute_u32(BruteArgs a) {
 void launch_stage1(const Stage1Args& a, cudaStream_t st) {
   dim3 grid(static_cast<unsigned>((a.ncols + kTile - 1) / kTile),
             static_cast<unsigned>((a.ndm_nom + kRows - 1) / kRows), static_cast<unsigned>(a.nsb));
-  if (a.nbits == 8) k_stage1_u8<<<grid, kThreads, 0, st>>>(a);
-  else if (a.nbits == 16) k_stage1_wide<uint16_t><<<grid, kThreads, 0, st>>>(a);
-  else k_stage1_wide<uint32_t><<<grid, kThreads, 0, st>>>(a);
+  if (a.nbits == 8) {
+    k_stage1_u8<<<grid, kThreads, 0, st>>>(a);
+  } else if (a.nbits == 16) {
+    k_stage1_wide<uint16_t><<<grid, kThreads, 0, st>>>(a);
+  } else {
+    grid.y = static_cast<unsigned>((a.ndm_nom + kRows64 - 1) / kRows64);
+    k_stage1_u32<<<grid, kThreads, 0, st>>>(a);
+  }
   DD_LAUNCHED();
 }
 
 void launch_stage2(const Stage2Args& a, cudaStream_t st) {
   const int64_t nnom = (a.dm_steps + a.ndm0 - 1) / a.ndm0;
-  const int64_t per_nom = (a.ndm0 + kRows - 1) / kRows;
+  const int rows = a.out64 ? kRows64 : kRows;
+  const int64_t per_nom = (a.ndm0 + rows - 1) / rows;
   dim3 grid(static_cast<unsigned>((a.ncols + kTile - 1) / kTile), static_cast<unsigned>(nnom * per_nom));
-  k_stage2<<<grid, kThreads, 0, st>>>(a);
+  if (a.out64) k_stage2_u64<<<grid, kThreads, 0, st>>>(a);
+  else k_stage2<<<grid, kThreads, 0, st>>>(a);
   DD_LAUNCHED();
 }
 

@@ -28,8 +28,8 @@ class ChunkSpec:
     bandwidth: float = 500.0      # MHz
     tsamp: float = 49.152e-6      # s
     seed: int = 0
-    mean: Optional[float] = None  # default 128 (8-bit) / 32768 (16-bit)
-    sigma: Optional[float] = None # default 20 / 2000
+    mean: Optional[float] = None  # default 128 (8-bit) / 32768 (16-bit) / 1e6 (32-bit)
+    sigma: Optional[float] = None # default 20 / 2000 / 6e4
     pulses: Sequence[Tuple[float, float, float, float]] = ()  # (dm, t0 s, width s, amplitude)
     rfi_frac: float = 0.0         # fraction of channels with a sinusoid
     rfi_amp: float = 60.0
@@ -58,6 +58,10 @@ class ChunkSpec:
 def _defaults(spec: ChunkSpec):
     if spec.nbits == 8:
         return (128.0 if spec.mean is None else spec.mean, 20.0 if spec.sigma is None else spec.sigma, 255)
+    if spec.nbits == 32:
+        # float32 holds every integer below 2^24 exactly
+        return (1e6 if spec.mean is None else spec.mean, 6e4 if spec.sigma is None else spec.sigma,
+                float(2 ** 32 - 1))
     return (32768.0 if spec.mean is None else spec.mean, 2000.0 if spec.sigma is None else spec.sigma, 65535)
 
 
@@ -93,7 +97,7 @@ def _extras(spec: ChunkSpec, rng: np.random.Generator):
 
 
 def make_chunk(spec: ChunkSpec) -> Tuple[np.ndarray, dict]:
-    """Host (numpy) chunk [nsamp, nchans] of uint8/uint16 and its header."""
+    """Host (numpy) chunk [nsamp, nchans] of uint8/uint16/uint32 and its header."""
     rng = np.random.default_rng(spec.seed)
     mean, sigma, vmax = _defaults(spec)
     x = rng.normal(mean, sigma, size=(spec.nsamp, spec.nchans)).astype(np.float32)
@@ -108,7 +112,9 @@ def make_chunk(spec: ChunkSpec) -> Tuple[np.ndarray, dict]:
         else:
             _, rows, cols, vals = item
             np.add.at(x, (rows, cols), vals)
-    dt = np.uint8 if spec.nbits == 8 else np.uint16
+    dt = {8: np.uint8, 16: np.uint16, 32: np.uint32}[spec.nbits]
+    if spec.nbits == 32:
+        return np.clip(np.rint(x.astype(np.float64)), 0, vmax).astype(dt), spec.header()
     return np.clip(np.rint(x), 0, vmax).astype(dt), spec.header()
 
 
@@ -116,6 +122,8 @@ def make_chunk_device(spec: ChunkSpec, device: int = 0):
     """Device (torch) chunk with the same construction, generated on the GPU."""
     import torch
 
+    if spec.nbits not in (8, 16):
+        raise ValueError("device chunks are generated for 8- and 16-bit samples")
     mean, sigma, vmax = _defaults(spec)
     rng = np.random.default_rng(spec.seed)
     g = torch.Generator(device=f"cuda:{device}")

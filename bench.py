@@ -67,38 +67,6 @@ DEFAULT_WORKLOAD = "wideband-4096ch-u8-2^20-6001dm-subband64-rfi"
 
 
 # ---------------------------------------------------------------- distributed plumbing
-class Dist:
-    def __init__(self, gpus: int):
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        self.pg = None
-        if self.world > 1:
-            import datetime
-
-            import torch.distributed as dist
-
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-            self.pg = dist
-
-    def barrier(self):
-        if self.pg:
-            self.pg.barrier()
-
-    def max(self, v: float) -> float:
-        if not self.pg:
-            return v
-        import torch
-
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
-        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
-        return float(t.item())
-
-    def close(self):
-        if self.pg:
-            self.pg.destroy_process_group()
-
-
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
@@ -255,8 +223,10 @@ def e2e_run(plan, x, out, units, dist, dev, stream, steps):
         plan.run_host(h_in_np, h_out_np, stream)
     e3.record(stream)
     torch.cuda.synchronize(dev)
-    e2e_ms = dist.max(e2.elapsed_time(e3) / steps)
-    e2e = {"value": dist.world * units / (e2e_ms * 1e-3), "unit": UNIT,
+    e2e_rank_ms = e2.elapsed_time(e3) / steps
+    e2e_rate = dist.job_rate(units, e2e_rank_ms * 1e-3)
+    e2e_ms = dist.max(e2e_rank_ms)
+    e2e = {"value": e2e_rate, "unit": UNIT,
            "h2d_bytes_per_step": int(h_in.numel() * h_in.element_size()),
            "d2h_bytes_per_step": int(h_out.numel() * h_out.element_size()),
            "ms_per_step": e2e_ms}
@@ -282,10 +252,12 @@ def main():
 
     from astroflow_b200.synth import ChunkSpec, make_chunk_device
 
-    dist = Dist(args.gpus)
+    from astroflow_b200.replicas import Replicas
+
+    dist = Replicas("nccl", timeout_s=300.0)
     dev = dist.local
     torch.cuda.set_device(dev)
-    spec = ChunkSpec(nchans=wl["nchans"], nsamp=wl["nsamp"], nbits=wl["nbits"], seed=1234 + dist.rank,
+    spec = ChunkSpec(nchans=wl["nchans"], nsamp=wl["nsamp"], nbits=wl["nbits"], seed=dist.chunk_seed(1234),
                      **wl["chunk"])
     hdr = spec.header()
     f32 = np.float32
@@ -363,9 +335,9 @@ def main():
     torch.cuda.synchronize(dev)
     dist.barrier()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1) / args.steps
-    ms = dist.max(ms)
-    value = dist.world * units / (ms * 1e-3)
+    ms_rank = e0.elapsed_time(e1) / args.steps
+    value = dist.job_rate(units, ms_rank * 1e-3)
+    ms = dist.max(ms_rank)
 
     # per-stage breakdown from the timed steps (device time, CUDA events on the run's stream)
     st = {k: float(np.mean([s[k] for s in stats])) for k in ("total_ms", "prep_ms", "stage1_ms", "stage2_ms")}

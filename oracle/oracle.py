@@ -404,6 +404,10 @@ def ref_gpu(sb_width: int):
         L.ref_gpu_rfi.argtypes = [_c_int, _P, _c_float, _c_float, _c_float, _c_int, _c_long,
                                   _c_float, _c_float, _c_int, ctypes.c_char_p, _P, _P, _c_long, _P,
                                   _P, _P, _c_long, _P, _P, ctypes.c_char_p, _c_int]
+        L.ref_gpu_dedispered_fil.restype = _c_int
+        L.ref_gpu_dedispered_fil.argtypes = [
+            ctypes.c_char_p, _c_float, _c_float, _c_float, _c_float, _c_float, _c_int, _c_float,
+            _c_int, ctypes.c_char_p, _P, _P, _c_long, _P, _P, ctypes.c_char_p, _c_int]
         _ref_gpu[sb_width] = L
     return _ref_gpu[sb_width]
 
@@ -426,6 +430,24 @@ def ref_gpu_dedisperse_spec(data, nchans, tsamp, fch1, foff, dm_low, dm_high, fr
         nbits, _ptr(data), 0.0, tsamp, fch1, foff, nchans, ndata, dm_low, dm_high, freq_start,
         freq_end, dm_step, ds, t_sample, device, mask_file.encode(), ctypes.byref(r), _ptr(out),
         cap, ctypes.byref(rows), ctypes.byref(cols), err, 512)
+    if rc:
+        raise ValueError(f"reference GPU call failed: {err.value.decode()}")
+    return out[:rows.value * cols.value].reshape(rows.value, cols.value)
+
+
+def ref_gpu_dedispered_fil(filename, dm_low, dm_high, freq_start, freq_end, dm_step, ds,
+                           t_sample=0.5, sb_width=32, mask_file="", use_mask=False,
+                           use_zero_dm=False, use_iqrm=False, iq=None, cap=1 << 22, device=0):
+    """Raw [dm_steps, down_ndata] output of the reference's file entry point
+    (Filterbank reader + gpucal::dedispered_fil_cuda)."""
+    out = np.zeros(cap, np.uint64)
+    rows, cols = _c_long(), _c_long()
+    err = ctypes.create_string_buffer(512)
+    r = _tap_rfi(use_mask, use_zero_dm, use_iqrm, iq)
+    rc = ref_gpu(sb_width).ref_gpu_dedispered_fil(
+        str(filename).encode(), dm_low, dm_high, freq_start, freq_end, dm_step, ds, t_sample,
+        device, mask_file.encode(), ctypes.byref(r), _ptr(out), cap, ctypes.byref(rows),
+        ctypes.byref(cols), err, 512)
     if rc:
         raise ValueError(f"reference GPU call failed: {err.value.decode()}")
     return out[:rows.value * cols.value].reshape(rows.value, cols.value)

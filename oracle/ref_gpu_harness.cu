@@ -277,3 +277,50 @@ extern "C" int ref_gpu_rfi(int nbits, const void* data, float tsamp, float fch1,
   std::snprintf(err, errlen, "unsupported nbits");
   return 5;
 }
+
+// The file entry point: Filterbank(filename) (src/data/filterbank.cpp:64-116, header,
+// data and channel flip) then gpucal::dedispered_fil_cuda<T>
+// (src/core/dedispered.cu:483-986), as _dedispered_fil calls them for target 1
+// (src/bindpy/pyapi.cpp:6-51).  Raw sums captured before the image step.
+extern "C" int ref_gpu_dedispered_fil(const char* filename, float dm_low, float dm_high,
+                                      float freq_start, float freq_end, float dm_step, int ds,
+                                      float t_sample, int device, const char* mask_file,
+                                      const void* rfi, uint64_t* out, long out_cap, long* rows,
+                                      long* cols, char* err, int errlen) {
+  const TapRfi* r = static_cast<const TapRfi*>(rfi);
+  try {
+    Filterbank fil{std::string(filename)};
+    switch (fil.nbits) {
+      case 8:
+        gpucal::dedispered_fil_cuda<uint8_t>(fil, dm_low, dm_high, freq_start, freq_end, dm_step,
+                                             REF_FREQ_END, ds, t_sample, device,
+                                             std::string(mask_file), make_rfi(r));
+        break;
+      case 16:
+        gpucal::dedispered_fil_cuda<uint16_t>(fil, dm_low, dm_high, freq_start, freq_end,
+                                              dm_step, REF_FREQ_END, ds, t_sample, device,
+                                              std::string(mask_file), make_rfi(r));
+        break;
+      case 32:
+        gpucal::dedispered_fil_cuda<uint32_t>(fil, dm_low, dm_high, freq_start, freq_end,
+                                              dm_step, REF_FREQ_END, ds, t_sample, device,
+                                              std::string(mask_file), make_rfi(r));
+        break;
+      default:
+        std::snprintf(err, errlen, "unsupported nbits %d", fil.nbits);
+        return 5;
+    }
+  } catch (const std::exception& e) {
+    std::snprintf(err, errlen, "%s", e.what());
+    return 2;
+  }
+  const RefCapture& cap = ref_capture();
+  if (static_cast<long>(cap.rows * cap.cols) > out_cap) {
+    std::snprintf(err, errlen, "output capacity too small");
+    return 3;
+  }
+  std::memcpy(out, cap.typed.data(), cap.rows * cap.cols * sizeof(uint64_t));
+  *rows = static_cast<long>(cap.rows);
+  *cols = static_cast<long>(cap.cols);
+  return 0;
+}

@@ -110,6 +110,8 @@ SUB = [
     (512, 4096, 16, 1e-4, 1500.0, 500.0, 0.0, 1000.0, 2.0, 1, 32, None),
     (200, 5000, 8, 49.152e-6, 1500.0, 400.0, 0.0, 200.0, 0.7, 3, 16, (0.2, 0.9)),
     (128, 3333, 8, 64e-6, 1400.0, 200.0, 0.0, 500.0, 1.0, 1, 64, (0.0, 0.5)),
+    (256, 4096, 32, 64e-6, 1500.0, 400.0, 0.0, 400.0, 1.0, 1, 32, None),
+    (96, 3000, 32, 1e-4, 1450.0, 300.0, 3.0, 600.0, 0.9, 2, 16, (0.1, 0.8)),
 ]
 
 

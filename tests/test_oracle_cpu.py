@@ -111,7 +111,7 @@ def golden_files(prefix):
     return sorted(os.path.join(GOLDEN, f) for f in os.listdir(GOLDEN) if f.startswith(prefix) and f.endswith(".npz"))
 
 
-@pytest.mark.parametrize("path", golden_files("ref_cpu_"))
+@pytest.mark.parametrize("path", golden_files("ref_cpu_"), ids=os.path.basename)
 def test_oracle_matches_reference_cpu_golden(path):
     """Fixtures produced by the reference's cpucal::dedispered_fil_omp (see
     tests/golden/make_golden.py); the oracle reproduces the stored sums from the
@@ -129,3 +129,47 @@ def test_oracle_matches_reference_cpu_golden(path):
     cs, ce = O.chan_range(freq, kw["freq_start"], kw["freq_end"])
     ieee = O.cpu_delay_table(freq, cs, ce, kw["dm_low"], kw["dm_step"], g["delay"].shape[0], kw["tsamp"])
     assert int((ieee != g["delay"]).sum()) <= max(2, g["delay"].size // 1000)
+
+
+@pytest.mark.parametrize("path", golden_files("ref_gpu_sub_"), ids=os.path.basename)
+def test_oracle_subband_sums_match_reference_gpu_golden(path):
+    """Fixtures produced by the reference's gpucal::dedisperse_spec on a B200 (see
+    tests/golden/make_golden.py): the oracle's channel range, DM count and subband
+    sums (from the stored reference tables) reproduce the stored raw output."""
+    g = np.load(path)
+    x, nchans, ds = g["data"], int(g["nchans"]), int(g["ds"])
+    freq = O.freq_table_header(float(g["fch1"]), float(g["foff"]), nchans)
+    plan = O.subband_plan(freq, x.shape[0], float(g["dm_low"]), float(g["dm_high"]),
+                          float(g["freq_start"]), float(g["freq_end"]), float(g["dm_step"]), ds,
+                          sb_width=int(g["sb_width"]))
+    assert (plan.chan_start, plan.chan_end) == (int(g["chan_start"]), int(g["chan_end"]))
+    assert plan.dm_steps == g["out"].shape[0]
+    xb = O.time_binning(x, nchans, ds) if ds > 1 else x
+    out = O.subband_sums(xb, nchans, plan, g["delay1"], g["residual2"])
+    assert np.array_equal(out, g["out"].astype(np.uint64))
+
+
+@pytest.mark.parametrize("path", golden_files("ref_gpu_rfi_"), ids=os.path.basename)
+def test_oracle_rfi_stages_match_reference_gpu_golden(path):
+    """The RFI stages of the reference GPU call (binning, IQRM window masks, zero-DM
+    at the reference's call site, mask file) from the fixtures: the oracle gives the
+    same window bounds, masks and processed input."""
+    import types
+
+    g = np.load(path)
+    x, nchans, ds = g["data"], int(g["nchans"]), int(g["ds"])
+    freq = O.freq_table_header(float(g["fch1"]), float(g["foff"]), nchans)
+    cs, ce = O.chan_range(freq, float(g["freq_start"]), float(g["freq_end"]))
+    mode, rf, ns, win, hop = (float(v) for v in g["iq"])
+    iq = types.SimpleNamespace(mode=int(mode), radius_frac=rf, nsigma=ns, geofactor=1.5,
+                               win_sec=win, hop_sec=hop, include_tail=True)
+    xb = O.time_binning(x, nchans, ds) if ds > 1 else x.copy()
+    t0, t1, masks = O.iqrm_masks(xb, nchans, cs, ce, float(F32(F32(g["tsamp"]) * F32(ds))), iq)
+    assert np.array_equal(t0, g["win_t0"]) and np.array_equal(t1, g["win_t1"])
+    assert np.array_equal(masks, g["masks"])
+    O.apply_window_masks(xb, nchans, t0, t1, masks)
+    if bool(g["use_zero_dm"]):
+        O.zero_dm_callsite(xb, cs, ce, xb.shape[0])
+    if bool(g["use_mask"]):
+        O.mark_channels(xb, nchans, [int(c) for c in g["bad"]])
+    assert np.array_equal(xb, g["processed"])
