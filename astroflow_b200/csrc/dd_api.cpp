@@ -249,7 +249,12 @@ int table_spread(const std::vector<int32_t>& tab, int64_t nrows, int64_t ncols, 
 // would not fit comfortably in shared memory.
 int window_bytes(int spread, int tile, int elem) {
   const int64_t w = round_up(static_cast<int64_t>(spread + tile) * elem + 40, 16);
-  return sum_smem_bytes(static_cast<int>(w)) <= 200 * 1024 ? static_cast<int>(w) : 0;
+  return sum_smem_bytes(static_cast<int>(w), 2) <= 200 * 1024 ? static_cast<int>(w) : 0;
+}
+
+void upload_desc(DevBuf& b, const std::vector<SumDesc>& d) {
+  b.alloc(sizeof(SumDesc) * d.size());
+  DD_CUDA_TRY(cudaMemcpy(b.p, d.data(), sizeof(SumDesc) * d.size(), cudaMemcpyHostToDevice));
 }
 
 bool callsite_zdm_active(const dd_plan& P) {
@@ -325,6 +330,8 @@ void create_subband(dd_plan& P) {
     const int T2 = sum_variant_tile(2, false);
     P.win2 = window_bytes(table_spread(P.h_res, P.dm_steps, P.nsb, kSumRows, P.ndm0), T2, 2);
   }
+  if (P.win1) upload_desc(P.d_desc1, build_sum_desc(P.h_delay, P.ndm_nom, P.dch, 0));
+  if (P.win2) upload_desc(P.d_desc2, build_sum_desc(P.h_res, P.dm_steps, P.nsb, P.ndm0));
   const int64_t kT = tile_samples();
   // Time tile of the stage-1 -> stage-2 pipeline: long enough that the stage-1
   // halo (max_res extra samples per tile) stays small, short enough that one
@@ -365,6 +372,7 @@ void set_brute_window(dd_plan& P) {
     const int T = sum_variant_tile(P.elem, P.nbits == 8);
     P.winb = window_bytes(table_spread(P.h_delay, P.dm_steps, P.nc, kSumRows, 0), T, P.elem);
   }
+  if (P.winb) upload_desc(P.d_descb, build_sum_desc(P.h_delay, P.dm_steps, P.nc, 0));
 }
 
 void create_brute(dd_plan& P) {
@@ -558,6 +566,10 @@ void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out
       L.lane_per = 1;
       L.grid_y = static_cast<unsigned>((P.ndm_nom + kSumRows - 1) / kSumRows);
       L.grid_z = static_cast<unsigned>(P.nsb);
+      L.desc = P.d_desc1.as<SumDesc>();
+      L.desc_pitch = P.dch;
+      L.stages = sum_stages(P.win1);
+      L.err = P.d_err.as<int>();
       launch_sum(L, st);
     } else {
       launch_stage1(s1, st);
@@ -602,6 +614,10 @@ void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out
       L.lane_per = 65535 / (255 * P.sbw);
       L.grid_y = static_cast<unsigned>(P.ndm_nom * ((P.ndm0 + kSumRows - 1) / kSumRows));
       L.grid_z = 1;
+      L.desc = P.d_desc2.as<SumDesc>();
+      L.desc_pitch = P.nsb;
+      L.stages = sum_stages(P.win2);
+      L.err = P.d_err.as<int>();
       launch_sum(L, st);
     } else {
       launch_stage2(s2, st);
@@ -660,6 +676,10 @@ void run_brute(dd_plan& P, const void* input, void* output, void* prepped, cudaS
     L.lane_per = 1;
     L.grid_y = static_cast<unsigned>((P.dm_steps + kSumRows - 1) / kSumRows);
     L.grid_z = 1;
+    L.desc = P.d_descb.as<SumDesc>();
+    L.desc_pitch = P.nc;
+    L.stages = sum_stages(P.winb);
+    L.err = P.d_err.as<int>();
     launch_sum(L, st);
   } else if (P.phases_merge) {
     b.start = 0;
@@ -678,10 +698,26 @@ void run_brute(dd_plan& P, const void* input, void* output, void* prepped, cudaS
 }
 
 
+// After a synchronising call: report (and clear) a bounded wait that gave up
+// inside a staged-sum kernel.
+void check_device_error(dd_plan& P, cudaStream_t st) {
+  int e = 0;
+  DD_CUDA_TRY(cudaMemcpyAsync(&e, P.d_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DD_CUDA_TRY(cudaStreamSynchronize(st));
+  if (e) {
+    DD_CUDA_TRY(cudaMemsetAsync(P.d_err.p, 0, sizeof(int), st));
+    DD_CUDA_TRY(cudaStreamSynchronize(st));
+    throw Error{DD_ERR_RUNTIME, e == kErrWaitFull
+                                    ? "a staged-sum block timed out waiting for its input window"
+                                    : "a staged-sum block timed out waiting for a free stage"};
+  }
+}
+
 int64_t workspace_of(const dd_plan& P) {
   const DevBuf* bufs[] = {&P.d_delay, &P.d_res, &P.d_lags, &P.d_bad_keep, &P.d_win, &P.d_seg_t0,
                           &P.d_binned, &P.d_x, &P.d_inter, &P.d_stats, &P.d_iqrm_scratch,
-                          &P.d_masks, &P.d_segmask, &P.d_zdm};
+                          &P.d_masks, &P.d_segmask, &P.d_zdm, &P.d_desc1, &P.d_desc2,
+                          &P.d_descb, &P.d_err};
   int64_t t = 0;
   for (auto* b : bufs) t += static_cast<int64_t>(b->bytes);
   return t;
@@ -787,6 +823,8 @@ int dd_plan_create(const dd_header* header, const dd_plan_params* params,
     // The _dedisperse_spec path's Header carries tsamp as float.
     P->tsamp = P->p.freq_mode == DD_FREQ_FIL ? header->tsamp
                                               : static_cast<double>(static_cast<float>(header->tsamp));
+    P->d_err.alloc(sizeof(int));
+    DD_CUDA_TRY(cudaMemset(P->d_err.p, 0, sizeof(int)));
     build_freq(*P);
     build_band(*P);
     if (P->p.algorithm == DD_ALGO_BRUTE) {
@@ -911,6 +949,7 @@ int dd_run_profiled(dd_plan* P, const void* input, void* output, void* stream,
     o.stage2_launches = P->p.algorithm == DD_ALGO_BRUTE
                             ? static_cast<int32_t>((P->winb || P->phases_merge) ? 1 : P->nslices)
                             : static_cast<int32_t>(pf.s2.size());
+    check_device_error(*P, st);
     *stats = o;
   });
 }
@@ -947,6 +986,7 @@ int dd_run_host(dd_plan* P, const void* h_input, void* h_output, void* stream) {
     DD_CUDA_TRY(cudaFreeAsync(d_in, st));
     DD_CUDA_TRY(cudaFreeAsync(d_out, st));
     DD_CUDA_TRY(cudaStreamSynchronize(st));
+    check_device_error(*P, st);
   });
 }
 

@@ -114,6 +114,8 @@ struct dd_plan {
   dd::DevBuf d_masks;    // IQRM window masks [nwin][nchans]
   dd::DevBuf d_segmask;  // [nseg][nchans]
   dd::DevBuf d_zdm;      // per-sample zero-DM offsets [nbin]
+  dd::DevBuf d_desc1, d_desc2, d_descb;  // staging descriptors: stage 1, stage 2, brute force
+  dd::DevBuf d_err;      // device error word of the staged sums (0: no error)
   double adds = 0;
   std::vector<cudaEvent_t> events;  // timing events of dd_run_profiled
   ~dd_plan() {
@@ -220,6 +222,17 @@ void launch_brute(const BruteArgs& a, cudaStream_t st);
 
 // ---- shared-memory staged sums (dd_sumsmem.cu) ----
 constexpr int kSumRows = 8;  // output rows per block
+// Staging descriptor of one (row group, source) pair of a staged sum: the
+// smallest offset of the group's rows for that source, the spread of their
+// offsets, and each row's offset relative to the smallest.  Built on the host
+// from the plan's tables; the kernels read one per source and row group.
+struct SumDesc {
+  int32_t lo;
+  int32_t span;
+  uint16_t rel[kSumRows];
+  int32_t pad[2];
+};
+static_assert(sizeof(SumDesc) == 32, "SumDesc is 32 bytes");
 struct SumLaunch {
   enum Mode { kStage1 = 0, kStage2 = 1, kBrute = 2 };
   int mode;
@@ -243,10 +256,25 @@ struct SumLaunch {
   int flush;               // 8-bit sources: widen lanes every 256 sources
   int lane_per;            // 16-bit sources: sources per 16-bit lane before widening
   unsigned grid_y, grid_z;
+  const SumDesc* desc;     // [grid_y][desc_pitch] staging descriptors
+  int64_t desc_pitch;      // descriptors per row group (= columns of the offset table)
+  int stages;              // staged source pairs in flight (2..4)
+  int* err;                // device error word: set when a bounded wait gives up
 };
 void launch_sum(const SumLaunch& L, cudaStream_t st);
 int sum_tile_samples(int src_bytes, int nw);
-size_t sum_smem_bytes(int win_bytes);
+// Shared memory of a staged sum with `stages` pairs in flight.
+size_t sum_smem_bytes(int win_bytes, int stages);
+// Pairs in flight that fit the shared memory of two blocks per SM (at least 2).
+int sum_stages(int win_bytes);
+// Descriptors of a [nrows][ncols] offset table for row groups of kSumRows rows,
+// grouped within blocks of `group` rows (0: one block), in the launch's
+// blockIdx.y order.  Fails if a group's spread exceeds 65535.
+std::vector<SumDesc> build_sum_desc(const std::vector<int32_t>& tab, int64_t nrows,
+                                    int64_t ncols, int64_t group);
+// Device error codes of the staged sums.
+constexpr int kErrWaitFull = 1;   // a consumer gave up waiting for a staged window
+constexpr int kErrWaitEmpty = 2;  // the producer gave up waiting for a free stage
 // Tile (samples per block) of the kernel launch_sum picks for these sources.
 inline int sum_variant_tile(int src_bytes, bool flush) {
   return sum_tile_samples(src_bytes, (src_bytes == 2 || flush) ? 2 : 4);

@@ -5,21 +5,33 @@
 //   out[r][t] = sum_i src_i[base + off(r, i) + t],   t in [0, T) of the block's tile.
 //
 // A block owns RB output rows and T consecutive samples.  Sources are processed
-// two at a time: the time window of each source that the block's rows need,
-// [base + min_r off, base + max_r off + T), is copied once into shared memory with
-// cp.async (16-byte chunks, double-buffered: the next pair streams in while the
-// current pair is summed), and every row then reads its shifted samples from
-// there.  Lanes own interleaved 32-bit output words (lane l: words l, l+32, ...),
-// so each shared load touches 32 consecutive words, free of bank conflicts; a shift
-// that is not a multiple of 4 bytes costs one funnel shift of two words.
+// two at a time.  The time window of each source that the block's rows need,
+// [base + min_r off, base + max_r off + T), is brought into shared memory by one
+// bulk asynchronous copy (cp.async.bulk, completion counted in bytes on an
+// mbarrier); up to `stages` source pairs are in flight in a ring of buffers.
+// Lanes 0-1 of warp 0 act as the producer: before summing pair p they refill
+// the buffer pair p-1 used with pair p+stages-1, once every warp has released it
+// (an "empty" mbarrier with one arrival per warp).  The window bounds and each
+// row's offset inside its window come from descriptors precomputed on the host
+// (SumDesc), so the producer does no per-row work beyond unpacking them.
 //
-// 8-bit samples: each word is split into two 16-bit-lane words by byte permutes
-// and two sources are added by one three-input add, i.e. four sample additions
-// per add instruction; lanes are widened to 32 bits every 256 sources.  16-bit
-// samples are added as lane pairs and widened before they can overflow.
+// Summing: lanes own interleaved 32-bit output words (lane l: words l, l+32, ...),
+// so each shared load touches 32 consecutive words, free of bank conflicts; a
+// shift that is not a multiple of 4 bytes costs one funnel shift of two words.
+// 8-bit samples are split into two 16-bit-lane words by byte permutes and two
+// sources are added by one three-input add (four sample additions per add);
+// lanes are widened to 32 bits every 256 sources.  16-bit samples are added as
+// lane pairs and widened before they can overflow.  A missing second source (odd
+// source count) reads a zeroed window.
+//
+// Every wait on an mbarrier is bounded (about two seconds of SM clock); a wait
+// that gives up records an error code in L.err and the block stops summing, and
+// the other blocks of the launch stop at their next wait.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <vector>
 
 #include "dd_internal.h"
 
@@ -28,20 +40,62 @@ namespace {
 
 constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
+constexpr int kMaxStages = 4;
+constexpr long long kWaitCycles = 4000000000LL;
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+// ------------------------------------------------------------------ mbarrier helpers
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for the phase with the given parity to complete; false after ~2 s, or
+// as soon as this block (*failed) or any block of the launch (*gerr) has failed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* failed,
+                                          volatile int* gerr) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (true) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (*failed || *gerr) return false;
+    if (clock64() - t0 > kWaitCycles) return false;
+  }
+}
+// One bulk copy global -> shared, completing `bytes` on `bar`.
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
 
 // Per-block view of the sum.
 struct Geo {
   const char* src;     // source 0 (byte address)
   int64_t src_pitch;   // bytes between consecutive sources
-  const int32_t* off;  // off[r * off_pitch + i]
-  int64_t off_pitch;
+  const SumDesc* desc; // descriptor of source 0 for this block's row group
   int64_t base;        // element index added to every offset
   int nsrc, nrows;
   char* out;           // row 0, first column of the block (byte address)
@@ -54,6 +108,7 @@ __device__ __forceinline__ Geo make_geo(const SumLaunch& L, int T) {
   const int64_t tile = blockIdx.x;
   const int64_t col = tile * T;  // launch-local column of the block
   g.valid = L.ncols - col;
+  const SumDesc* drow = L.desc + static_cast<int64_t>(blockIdx.y) * L.desc_pitch;
   switch (L.mode) {
     case SumLaunch::kStage1: {
       // rows: nominal DMs j0.. of subband sb; sources: the subband's channels
@@ -61,9 +116,7 @@ __device__ __forceinline__ Geo make_geo(const SumLaunch& L, int T) {
       const int64_t sb = blockIdx.z;
       const int64_t c0 = sb * L.group;
       g.src = L.src + c0 * L.src_pitch;
-      g.src_pitch = L.src_pitch;
-      g.off = L.off + j0 * L.off_pitch + c0;
-      g.off_pitch = L.off_pitch;
+      g.desc = drow + c0;
       g.nsrc = static_cast<int>(min(static_cast<int64_t>(L.group), L.nsrc_total - c0));
       g.nrows = static_cast<int>(min(static_cast<int64_t>(L.rows_per_block), L.nrows_total - j0));
       g.out = L.out + (j0 * L.nsb_out + sb) * L.out_pitch + (L.out_col0 + col) * L.out_elem;
@@ -77,9 +130,7 @@ __device__ __forceinline__ Geo make_geo(const SumLaunch& L, int T) {
       const int64_t m0 = j * L.group + static_cast<int64_t>(blockIdx.y % per_nom) * L.rows_per_block;
       const int64_t mend = min((j + 1) * L.group, L.nrows_total);
       g.src = L.src + j * L.nsrc_total * L.src_pitch;
-      g.src_pitch = L.src_pitch;
-      g.off = L.off + m0 * L.off_pitch;
-      g.off_pitch = L.off_pitch;
+      g.desc = drow;
       g.nsrc = static_cast<int>(L.nsrc_total);
       g.nrows = static_cast<int>(max(static_cast<int64_t>(0), min(static_cast<int64_t>(L.rows_per_block), mend - m0)));
       g.out = L.out + m0 * L.out_pitch + (L.out_col0 + col) * L.out_elem;
@@ -89,9 +140,7 @@ __device__ __forceinline__ Geo make_geo(const SumLaunch& L, int T) {
     default: {  // brute force: rows = DMs, sources = channels
       const int64_t m0 = static_cast<int64_t>(blockIdx.y) * L.rows_per_block;
       g.src = L.src;
-      g.src_pitch = L.src_pitch;
-      g.off = L.off + m0 * L.off_pitch;
-      g.off_pitch = L.off_pitch;
+      g.desc = drow;
       g.nsrc = static_cast<int>(L.nsrc_total);
       g.nrows = static_cast<int>(min(static_cast<int64_t>(L.rows_per_block), L.nrows_total - m0));
       g.out = L.out + m0 * L.out_pitch + (L.out_col0 + col) * L.out_elem;
@@ -99,48 +148,129 @@ __device__ __forceinline__ Geo make_geo(const SumLaunch& L, int T) {
       break;
     }
   }
+  g.src_pitch = L.src_pitch;
   g.base = L.base + col;
   return g;
 }
 
-// Stage the windows of sources i, i+1 into words [wbase_s, wbase_s + win_words) of
-// the shared array (one window per source), and publish, for every row, the
-// word index and byte shift of its sample 0 inside the window.
-template <int SB, int RB>
-__device__ __forceinline__ void stage_pair(const Geo& g, int i, uint32_t* sw, int win_words,
-                                           int tile_bytes, int* rowq, int* rowsh) {
+// Shared state of the pipeline.
+struct Pipe {
+  uint64_t full[kMaxStages];   // completes when a stage's two windows have landed
+  uint64_t empty[kMaxStages];  // completes when all warps released a stage
+  int rowq[kMaxStages][2 * kSumRows];   // word index of each row's sample 0 (source 0, 1)
+  int rowsh[kMaxStages][2 * kSumRows];  // byte shift (bits) of each row's sample 0
+  int failed;
+};
+
+// Producer step for source pair q in stage s (warp 0, lanes 0 and 1; lane l
+// handles source 2q + l).  The caller has made sure stage s is free.
+template <int SB>
+__device__ __forceinline__ void produce(const Geo& g, Pipe& P, uint32_t* sw, int ww, int zero_q,
+                                        int tile_bytes, int q, int s, int lane) {
+  const int src = 2 * q + lane;
+  uint32_t nbytes = 0;
+  const char* gsrc = nullptr;
+  uint32_t* dst = sw + (2 * s + lane) * ww;
+  if (lane < 2) {
+    if (src < g.nsrc) {
+      const SumDesc d = g.desc[src];
+      const int64_t first = (g.base + d.lo) * SB;
+      const int64_t a0 = first & ~int64_t(15);
+      const int64_t last = (g.base + d.lo + d.span) * SB + tile_bytes + 8;  // + funnel word
+      nbytes = static_cast<uint32_t>((last - a0 + 15) & ~int64_t(15));
+      gsrc = g.src + static_cast<int64_t>(src) * g.src_pitch + a0;
+      const int qbase = (2 * s + lane) * ww;
+      const int ob0 = static_cast<int>(first - a0);
 #pragma unroll
-  for (int s = 0; s < 2; ++s) {
-    const int src = i + s;
-    if (src >= g.nsrc) {
-      if (threadIdx.x < RB) { rowq[s * RB + threadIdx.x] = 0; rowsh[s * RB + threadIdx.x] = 0; }
-      continue;
-    }
-    int lo = 0x7fffffff, hi = -0x7fffffff;
+      for (int r = 0; r < kSumRows; ++r) {
+        // rows past nrows take offset lo (rel 0): their reads stay in the window
+        const int ob = ob0 + (r < g.nrows ? static_cast<int>(d.rel[r]) : 0) * SB;
+        P.rowq[s][lane * kSumRows + r] = qbase + (ob >> 2);
+        P.rowsh[s][lane * kSumRows + r] = (ob & 3) * 8;
+      }
+    } else {
 #pragma unroll
-    for (int r = 0; r < RB; ++r) {
-      if (r < g.nrows) {
-        const int o = __ldg(g.off + r * g.off_pitch + src);
-        lo = min(lo, o);
-        hi = max(hi, o);
+      for (int r = 0; r < kSumRows; ++r) {
+        P.rowq[s][lane * kSumRows + r] = zero_q;
+        P.rowsh[s][lane * kSumRows + r] = 0;
       }
     }
-    const int64_t first = (g.base + lo) * SB;
-    const int64_t a0 = first & ~int64_t(15);
-    const int64_t last = (g.base + hi) * SB + tile_bytes + 8;  // + the funnel's second word
-    const int nbytes = static_cast<int>((last - a0 + 15) & ~int64_t(15));
-    const char* gsrc = g.src + static_cast<int64_t>(src) * g.src_pitch + a0;
-    uint32_t* dst = sw + s * win_words;
-    for (int b = threadIdx.x * 16; b < nbytes; b += kThreads * 16)
-      cp_async16(reinterpret_cast<char*>(dst) + b, gsrc + b);
-    if (threadIdx.x < RB) {
-      // Rows past nrows are summed too (their results are never stored); they
-      // take the window's first offset so their reads stay inside the window.
-      const int r = threadIdx.x;
-      const int o = r < g.nrows ? __ldg(g.off + r * g.off_pitch + src) : lo;
-      const int ob = static_cast<int>(first - a0) + (o - lo) * SB;  // byte offset of sample 0
-      rowq[s * RB + r] = s * win_words + (ob >> 2);
-      rowsh[s * RB + r] = (ob & 3) * 8;
+  }
+  const uint32_t other = __shfl_xor_sync(0xffffffffu, nbytes, 1);
+  __syncwarp();
+  if (lane == 0) mbar_arrive_expect_tx(&P.full[s], nbytes + other);
+  __syncwarp();
+  if (lane < 2 && nbytes) bulk_copy(dst, gsrc, nbytes, &P.full[s]);
+}
+
+// Pipeline driver shared by the kernels: calls body(stage, cur) for every
+// source pair once its windows are in shared memory.
+template <int SB, typename Body>
+__device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, Pipe& P,
+                                             uint32_t* sw, int tile_bytes, Body&& body) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ww = L.win_bytes >> 2;
+  const int S = L.stages;
+  const int zero_q = 2 * S * ww;
+  const int npairs = (g.nsrc + 1) / 2;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&P.full[s], 1);
+      mbar_init(&P.empty[s], kWarps);
+    }
+    P.failed = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  for (int i = threadIdx.x; i < ww; i += kThreads) sw[zero_q + i] = 0u;
+  __syncthreads();
+  volatile int* failed = &P.failed;
+  int issued = 0;  // pairs whose copies warp 0 has issued
+  if (warp == 0)
+    for (; issued < min(S - 1, npairs); ++issued)
+      produce<SB>(g, P, sw, ww, zero_q, tile_bytes, issued, issued, lane);
+  int s_cur = 0, p = 0;
+  uint32_t ph_cur = 0;
+  for (; p < npairs; ++p) {
+    if (warp == 0 && issued < npairs) {
+      const int q = issued;  // == p + S - 1: refills the stage pair p-1 used
+      const int s = q % S;
+      bool ok = true;
+      if (q >= S) {
+        if (lane == 0) ok = mbar_wait(&P.empty[s], ((q / S) - 1) & 1, failed, L.err);
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+      }
+      if (!ok) {
+        if (lane == 0) {
+          if (!*failed) atomicCAS(L.err, 0, kErrWaitEmpty);
+          *failed = 1;
+        }
+        break;
+      }
+      produce<SB>(g, P, sw, ww, zero_q, tile_bytes, q, s, lane);
+      ++issued;
+    }
+    const bool ok = mbar_wait(&P.full[s_cur], ph_cur, failed, L.err);
+    if (!ok) {
+      if (lane == 0) {
+        if (!*failed) atomicCAS(L.err, 0, kErrWaitFull);
+        *failed = 1;
+      }
+      break;
+    }
+    body(s_cur, sw);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&P.empty[s_cur]);
+    if (++s_cur == S) {
+      s_cur = 0;
+      ph_cur ^= 1u;
+    }
+  }
+  if (warp == 0 && lane == 0 && *failed) {
+    // let the copies already issued land before the block's shared memory goes away
+    for (int q = p; q < issued; ++q) {
+      const long long t0 = clock64();
+      while (!mbar_try_wait(&P.full[q % S], (q / S) & 1) && clock64() - t0 < kWaitCycles) {
+      }
     }
   }
 }
@@ -148,8 +278,8 @@ __device__ __forceinline__ void stage_pair(const Geo& g, int i, uint32_t* sw, in
 // ------------------------------------------------------------------ 8-bit samples
 template <int RB, int NW, bool OUT16, bool FLUSH>
 __global__ void __launch_bounds__(kThreads) k_sum_u8(SumLaunch L) {
-  extern __shared__ __align__(16) uint32_t sw[];
-  __shared__ int rowq[2][2 * RB], rowsh[2][2 * RB];
+  extern __shared__ __align__(128) uint32_t sw[];
+  __shared__ Pipe P;
   constexpr int T = kWarps * 32 * NW * 4;
   const Geo g = make_geo(L, T);
   if (g.nrows <= 0) return;
@@ -167,29 +297,16 @@ __global__ void __launch_bounds__(kThreads) k_sum_u8(SumLaunch L) {
 #pragma unroll
       for (int k = 0; k < NW * 4; ++k) w32[r][k] = 0;
   }
-  const int ww = L.win_bytes >> 2;  // words per window
-  const int npairs = (g.nsrc + 1) / 2;
   int since = 0;
-  stage_pair<1, RB>(g, 0, sw, ww, T, rowq[0], rowsh[0]);
-  cp_async_commit();
-  for (int p = 0; p < npairs; ++p) {
-    const int cur = p & 1;
-    if (p + 1 < npairs)
-      stage_pair<1, RB>(g, 2 * (p + 1), sw + (cur ^ 1) * 2 * ww, ww, T, rowq[cur ^ 1], rowsh[cur ^ 1]);
-    cp_async_commit();
-    cp_async_wait1();
-    __syncthreads();
-    const uint32_t* win = sw + cur * 2 * ww;
-    const bool two = 2 * p + 1 < g.nsrc;
+  run_pipeline<1>(L, g, P, sw, T, [&](int s, const uint32_t* win) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
-      const int q0 = rowq[cur][r] + wbase, q1 = rowq[cur][RB + r] + wbase;
-      const uint32_t s0 = rowsh[cur][r], s1 = rowsh[cur][RB + r];
+      const int q0 = P.rowq[s][r] + wbase, q1 = P.rowq[s][RB + r] + wbase;
+      const uint32_t s0 = P.rowsh[s][r], s1 = P.rowsh[s][RB + r];
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
         const uint32_t a = __funnelshift_r(win[q0 + 32 * k], win[q0 + 32 * k + 1], s0);
-        uint32_t b = __funnelshift_r(win[q1 + 32 * k], win[q1 + 32 * k + 1], s1);
-        b = two ? b : 0u;
+        const uint32_t b = __funnelshift_r(win[q1 + 32 * k], win[q1 + 32 * k + 1], s1);
         ev[r][k] += __byte_perm(a, 0u, 0x4240) + __byte_perm(b, 0u, 0x4240);
         od[r][k] += __byte_perm(a, 0u, 0x4341) + __byte_perm(b, 0u, 0x4341);
       }
@@ -208,8 +325,8 @@ __global__ void __launch_bounds__(kThreads) k_sum_u8(SumLaunch L) {
         since = 0;
       }
     }
-    __syncthreads();
-  }
+  });
+  if (P.failed) return;
 #pragma unroll
   for (int r = 0; r < RB; ++r) {
     if (r >= g.nrows) break;
@@ -254,8 +371,8 @@ __global__ void __launch_bounds__(kThreads) k_sum_u8(SumLaunch L) {
 // L.lane_per: sources summed in 16-bit lanes before widening (< 2: 32-bit sums).
 template <int RB, int NW>
 __global__ void __launch_bounds__(kThreads) k_sum_u16(SumLaunch L) {
-  extern __shared__ __align__(16) uint32_t sw[];
-  __shared__ int rowq[2][2 * RB], rowsh[2][2 * RB];
+  extern __shared__ __align__(128) uint32_t sw[];
+  __shared__ Pipe P;
   constexpr int T = kWarps * 32 * NW * 2;
   const Geo g = make_geo(L, T);
   if (g.nrows <= 0) return;
@@ -266,35 +383,25 @@ __global__ void __launch_bounds__(kThreads) k_sum_u16(SumLaunch L) {
   for (int r = 0; r < RB; ++r)
 #pragma unroll
     for (int k = 0; k < NW; ++k) a16[r][k] = lo32[r][k] = hi32[r][k] = 0;
-  const int ww = L.win_bytes >> 2;
   const int npairs = (g.nsrc + 1) / 2;
   const int per = L.lane_per;
-  int since = 0;
-  stage_pair<2, RB>(g, 0, sw, ww, 2 * T, rowq[0], rowsh[0]);
-  cp_async_commit();
-  for (int p = 0; p < npairs; ++p) {
-    const int cur = p & 1;
-    if (p + 1 < npairs)
-      stage_pair<2, RB>(g, 2 * (p + 1), sw + (cur ^ 1) * 2 * ww, ww, 2 * T, rowq[cur ^ 1], rowsh[cur ^ 1]);
-    cp_async_commit();
-    cp_async_wait1();
-    __syncthreads();
-    const uint32_t* win = sw + cur * 2 * ww;
-    const bool two = 2 * p + 1 < g.nsrc;
+  int since = 0, done = 0;
+  run_pipeline<2>(L, g, P, sw, 2 * T, [&](int s, const uint32_t* win) {
+    ++done;
     if (per >= 2) {
 #pragma unroll
       for (int r = 0; r < RB; ++r) {
-        const int q0 = rowq[cur][r] + wbase, q1 = rowq[cur][RB + r] + wbase;
-        const uint32_t s0 = rowsh[cur][r], s1 = rowsh[cur][RB + r];
+        const int q0 = P.rowq[s][r] + wbase, q1 = P.rowq[s][RB + r] + wbase;
+        const uint32_t s0 = P.rowsh[s][r], s1 = P.rowsh[s][RB + r];
 #pragma unroll
         for (int k = 0; k < NW; ++k) {
           const uint32_t a = __funnelshift_r(win[q0 + 32 * k], win[q0 + 32 * k + 1], s0);
           const uint32_t b = __funnelshift_r(win[q1 + 32 * k], win[q1 + 32 * k + 1], s1);
-          a16[r][k] += a + (two ? b : 0u);
+          a16[r][k] += a + b;
         }
       }
       since += 2;
-      if (since + 2 > per || p + 1 == npairs) {
+      if (since + 2 > per || done == npairs) {
 #pragma unroll
         for (int r = 0; r < RB; ++r)
 #pragma unroll
@@ -308,20 +415,19 @@ __global__ void __launch_bounds__(kThreads) k_sum_u16(SumLaunch L) {
     } else {
 #pragma unroll
       for (int r = 0; r < RB; ++r) {
-        const int q0 = rowq[cur][r] + wbase, q1 = rowq[cur][RB + r] + wbase;
-        const uint32_t s0 = rowsh[cur][r], s1 = rowsh[cur][RB + r];
+        const int q0 = P.rowq[s][r] + wbase, q1 = P.rowq[s][RB + r] + wbase;
+        const uint32_t s0 = P.rowsh[s][r], s1 = P.rowsh[s][RB + r];
 #pragma unroll
         for (int k = 0; k < NW; ++k) {
           const uint32_t a = __funnelshift_r(win[q0 + 32 * k], win[q0 + 32 * k + 1], s0);
-          uint32_t b = __funnelshift_r(win[q1 + 32 * k], win[q1 + 32 * k + 1], s1);
-          b = two ? b : 0u;
+          const uint32_t b = __funnelshift_r(win[q1 + 32 * k], win[q1 + 32 * k + 1], s1);
           lo32[r][k] += (a & 0xffffu) + (b & 0xffffu);
           hi32[r][k] += (a >> 16) + (b >> 16);
         }
       }
     }
-    __syncthreads();
-  }
+  });
+  if (P.failed) return;
 #pragma unroll
   for (int r = 0; r < RB; ++r) {
     if (r >= g.nrows) break;
@@ -353,12 +459,54 @@ void launch_k(K kernel, dim3 grid, size_t smem, const SumLaunch& L, cudaStream_t
 
 int sum_tile_samples(int src_bytes, int nw) { return kWarps * 32 * nw * (4 / src_bytes); }
 
-size_t sum_smem_bytes(int win_bytes) { return static_cast<size_t>(4) * win_bytes; }
+// Ring of `stages` window pairs plus one zeroed window.
+size_t sum_smem_bytes(int win_bytes, int stages) {
+  return static_cast<size_t>(2 * stages + 1) * win_bytes;
+}
+
+int sum_stages(int win_bytes) {
+  int s = kMaxStages;
+  while (s > 2 && sum_smem_bytes(win_bytes, s) > 100 * 1024) --s;
+  return s;
+}
+
+std::vector<SumDesc> build_sum_desc(const std::vector<int32_t>& tab, int64_t nrows,
+                                    int64_t ncols, int64_t group) {
+  const int64_t blk = group > 0 ? group : nrows;
+  const int64_t per = (blk + kSumRows - 1) / kSumRows;  // row groups per block of rows
+  const int64_t nblk = (nrows + blk - 1) / blk;
+  std::vector<SumDesc> d(static_cast<size_t>(nblk * per * ncols));
+  for (int64_t b = 0; b < nblk; ++b) {
+    const int64_t b0 = b * blk, b1 = std::min(nrows, b0 + blk);
+    for (int64_t gi = 0; gi < per; ++gi) {
+      const int64_t r0 = b0 + gi * kSumRows;
+      const int64_t r1 = std::min(b1, r0 + kSumRows);
+      SumDesc* row = d.data() + (b * per + gi) * ncols;
+      if (r0 >= r1) continue;
+      for (int64_t c = 0; c < ncols; ++c) {
+        int lo = tab[r0 * ncols + c], hi = lo;
+        for (int64_t r = r0 + 1; r < r1; ++r) {
+          lo = std::min(lo, tab[r * ncols + c]);
+          hi = std::max(hi, tab[r * ncols + c]);
+        }
+        if (hi - lo > 65535) throw Error{DD_ERR_RUNTIME, "staged-sum offsets spread too far"};
+        SumDesc& e = row[c];
+        e.lo = lo;
+        e.span = hi - lo;
+        for (int r = 0; r < kSumRows; ++r)
+          e.rel[r] = static_cast<uint16_t>(r0 + r < r1 ? tab[(r0 + r) * ncols + c] - lo : 0);
+      }
+    }
+  }
+  return d;
+}
 
 void launch_sum(const SumLaunch& L, cudaStream_t st) {
   const int T = sum_variant_tile(L.src_bytes, L.flush && L.out_elem != 2);
   dim3 grid(static_cast<unsigned>((L.ncols + T - 1) / T), L.grid_y, L.grid_z);
-  const size_t smem = sum_smem_bytes(L.win_bytes);
+  if (L.stages < 2 || L.stages > kMaxStages) throw Error{DD_ERR_RUNTIME, "bad stage count"};
+  if (!L.desc || !L.err) throw Error{DD_ERR_RUNTIME, "staged sum without descriptors"};
+  const size_t smem = sum_smem_bytes(L.win_bytes, L.stages);
   if (L.rows_per_block != kSumRows) throw Error{DD_ERR_RUNTIME, "unsupported rows per block"};
   if (L.src_bytes == 1) {
     if (L.out_elem == 2) {
