@@ -9,7 +9,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libastroflow_dd.so")
+# ASTROFLOW_DD_LIB selects another build of the library (e.g. a tuning variant).
+LIB_PATH = os.environ.get("ASTROFLOW_DD_LIB") or os.path.join(HERE, "libastroflow_dd.so")
 
 DD_OK = 0
 DD_ERR_INVALID = 1

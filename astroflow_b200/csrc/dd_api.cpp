@@ -351,7 +351,10 @@ void create_subband(dd_plan& P) {
   while (((n + 1) * T1 - R) * per_col <= (int64_t(1) << 30) && (n * T1 - R) < P.nbin) ++n;
   int64_t L = std::max<int64_t>(kT, n * T1 - R);
   P.tile = L;
-  P.tile_pitch = round_up(round_up(L + P.max_res, kT) + 64, 64);
+  // Stage-2 blocks past the tile's last column read up to one block tile beyond it
+  // (their columns are not stored).
+  const int64_t T2 = P.win2 ? sum_variant_tile(2, false) : kT;
+  P.tile_pitch = round_up(round_up(L + P.max_res, kT) + T2 + 64, 64);
   const int64_t ntiles = (P.nbin + L - 1) / L;
   P.xpitch = round_up(ntiles * L + round_up(L + P.max_res, 8192) + P.max_delay + 8192, 64);
   P.d_x.alloc(static_cast<size_t>(P.dch * P.xpitch) * P.elem);
@@ -570,6 +573,7 @@ void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out
       L.desc_pitch = P.dch;
       L.stages = sum_stages(P.win1);
       L.err = P.d_err.as<int>();
+      L.one = 1;
       launch_sum(L, st);
     } else {
       launch_stage1(s1, st);
@@ -618,6 +622,7 @@ void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out
       L.desc_pitch = P.nsb;
       L.stages = sum_stages(P.win2);
       L.err = P.d_err.as<int>();
+      L.one = 1;
       launch_sum(L, st);
     } else {
       launch_stage2(s2, st);
@@ -680,6 +685,7 @@ void run_brute(dd_plan& P, const void* input, void* output, void* prepped, cudaS
     L.desc_pitch = P.nc;
     L.stages = sum_stages(P.winb);
     L.err = P.d_err.as<int>();
+    L.one = 1;
     launch_sum(L, st);
   } else if (P.phases_merge) {
     b.start = 0;

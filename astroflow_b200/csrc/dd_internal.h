@@ -260,6 +260,7 @@ struct SumLaunch {
   int64_t desc_pitch;      // descriptors per row group (= columns of the offset table)
   int stages;              // staged source pairs in flight (2..4)
   int* err;                // device error word: set when a bounded wait gives up
+  unsigned one;            // 1 (a multiplier the compiler cannot fold)
 };
 void launch_sum(const SumLaunch& L, cudaStream_t st);
 int sum_tile_samples(int src_bytes, int nw);
@@ -276,8 +277,26 @@ std::vector<SumDesc> build_sum_desc(const std::vector<int32_t>& tab, int64_t nro
 constexpr int kErrWaitFull = 1;   // a consumer gave up waiting for a staged window
 constexpr int kErrWaitEmpty = 2;  // the producer gave up waiting for a free stage
 // Tile (samples per block) of the kernel launch_sum picks for these sources.
+// Words per lane of the staged sums (tile = 8 warps x 32 lanes x words x samples
+// per word): 16-bit sources, 8-bit sources, 8-bit sources widened to 32 bits.
+#ifndef DD_SUM16_NW
+#define DD_SUM16_NW 4
+#endif
+#ifndef DD_SUM8_NW
+#define DD_SUM8_NW 4
+#endif
+#ifndef DD_SUM8F_NW
+#define DD_SUM8F_NW 2
+#endif
+// Blocks per SM the staged-sum kernels are compiled for (register budget).
+#ifndef DD_SUM16_MINB
+#define DD_SUM16_MINB 2
+#endif
+#ifndef DD_SUM8_MINB
+#define DD_SUM8_MINB 2
+#endif
 inline int sum_variant_tile(int src_bytes, bool flush) {
-  return sum_tile_samples(src_bytes, (src_bytes == 2 || flush) ? 2 : 4);
+  return sum_tile_samples(src_bytes, src_bytes == 2 ? DD_SUM16_NW : (flush ? DD_SUM8F_NW : DD_SUM8_NW));
 }
 
 // ---- probes (dd_probe.cu) ----

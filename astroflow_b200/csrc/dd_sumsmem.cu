@@ -75,10 +75,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
                                           volatile int* gerr) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
-  while (true) {
+  for (uint32_t i = 1;; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (*failed || *gerr) return false;
-    if (clock64() - t0 > kWaitCycles) return false;
+    if ((i & 255u) == 0) {  // the failure checks read memory: keep them off the wake-up path
+      if (*failed || *gerr) return false;
+      if (clock64() - t0 > kWaitCycles) return false;
+    }
   }
 }
 // One bulk copy global -> shared, completing `bytes` on `bar`.
@@ -89,6 +91,17 @@ __device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t b
           smem_addr(dst)),
       "l"(src), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
+}
+
+#ifndef DD_SUM_IMAD
+#define DD_SUM_IMAD 0
+#endif
+// Accumulate with integer multiply-adds (by a runtime 1) instead of adds.
+constexpr bool kSumImad = DD_SUM_IMAD != 0;
+__device__ __forceinline__ uint32_t mad_u32(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t d;
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
 }
 
 // Per-block view of the sum.
@@ -157,8 +170,9 @@ __device__ __forceinline__ Geo make_geo(const SumLaunch& L, int T) {
 struct Pipe {
   uint64_t full[kMaxStages];   // completes when a stage's two windows have landed
   uint64_t empty[kMaxStages];  // completes when all warps released a stage
-  int rowq[kMaxStages][2 * kSumRows];   // word index of each row's sample 0 (source 0, 1)
-  int rowsh[kMaxStages][2 * kSumRows];  // byte shift (bits) of each row's sample 0
+  // per row: word index and shift (bits) of sample 0 in source 0's window, then
+  // the same for source 1
+  int4 row[kMaxStages][kSumRows];
   int failed;
 };
 
@@ -181,18 +195,20 @@ __device__ __forceinline__ void produce(const Geo& g, Pipe& P, uint32_t* sw, int
       gsrc = g.src + static_cast<int64_t>(src) * g.src_pitch + a0;
       const int qbase = (2 * s + lane) * ww;
       const int ob0 = static_cast<int>(first - a0);
+      int* rw = reinterpret_cast<int*>(P.row[s]) + 2 * lane;
 #pragma unroll
       for (int r = 0; r < kSumRows; ++r) {
         // rows past nrows take offset lo (rel 0): their reads stay in the window
         const int ob = ob0 + (r < g.nrows ? static_cast<int>(d.rel[r]) : 0) * SB;
-        P.rowq[s][lane * kSumRows + r] = qbase + (ob >> 2);
-        P.rowsh[s][lane * kSumRows + r] = (ob & 3) * 8;
+        rw[4 * r] = qbase + (ob >> 2);
+        rw[4 * r + 1] = (ob & 3) * 8;
       }
     } else {
+      int* rw = reinterpret_cast<int*>(P.row[s]) + 2 * lane;
 #pragma unroll
       for (int r = 0; r < kSumRows; ++r) {
-        P.rowq[s][lane * kSumRows + r] = zero_q;
-        P.rowsh[s][lane * kSumRows + r] = 0;
+        rw[4 * r] = zero_q;
+        rw[4 * r + 1] = 0;
       }
     }
   }
@@ -277,14 +293,19 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
 
 // ------------------------------------------------------------------ 8-bit samples
 template <int RB, int NW, bool OUT16, bool FLUSH>
-__global__ void __launch_bounds__(kThreads) k_sum_u8(SumLaunch L) {
+__global__ void __launch_bounds__(kThreads, DD_SUM8_MINB) k_sum_u8(SumLaunch L) {
   extern __shared__ __align__(128) uint32_t sw[];
   __shared__ Pipe P;
   constexpr int T = kWarps * 32 * NW * 4;
   const Geo g = make_geo(L, T);
   if (g.nrows <= 0) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wbase = warp * 32 * NW + lane;
+  // odd NW: lane owns NW consecutive words (NW+1 conflict-free loads per row and
+  // source); even NW: lane owns words lane, lane+32, ... (2 loads per word)
+  constexpr bool kConsec = (NW & 1) != 0;
+  constexpr int kStride = kConsec ? 1 : 32;
+  const int wbase = kConsec ? warp * 32 * NW + lane * NW : warp * 32 * NW + lane;
+  const uint32_t one = L.one;
   uint32_t ev[RB][NW], od[RB][NW];  // 16-bit lanes: samples (4w, 4w+2) and (4w+1, 4w+3)
   uint32_t w32[FLUSH ? RB : 1][FLUSH ? NW * 4 : 1];
 #pragma unroll
@@ -301,14 +322,29 @@ __global__ void __launch_bounds__(kThreads) k_sum_u8(SumLaunch L) {
   run_pipeline<1>(L, g, P, sw, T, [&](int s, const uint32_t* win) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
-      const int q0 = P.rowq[s][r] + wbase, q1 = P.rowq[s][RB + r] + wbase;
-      const uint32_t s0 = P.rowsh[s][r], s1 = P.rowsh[s][RB + r];
+      const int4 rw = P.row[s][r];
+      const uint32_t* w0 = win + rw.x + wbase;
+      const uint32_t* w1 = win + rw.z + wbase;
+      uint32_t va[NW + 1], vb[NW + 1];
+      if constexpr (kConsec) {
+#pragma unroll
+        for (int i = 0; i <= NW; ++i) { va[i] = w0[i]; vb[i] = w1[i]; }
+      }
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
-        const uint32_t a = __funnelshift_r(win[q0 + 32 * k], win[q0 + 32 * k + 1], s0);
-        const uint32_t b = __funnelshift_r(win[q1 + 32 * k], win[q1 + 32 * k + 1], s1);
-        ev[r][k] += __byte_perm(a, 0u, 0x4240) + __byte_perm(b, 0u, 0x4240);
-        od[r][k] += __byte_perm(a, 0u, 0x4341) + __byte_perm(b, 0u, 0x4341);
+        const uint32_t a = kConsec ? __funnelshift_r(va[k], va[k + 1], rw.y)
+                                   : __funnelshift_r(w0[32 * k], w0[32 * k + 1], rw.y);
+        const uint32_t b = kConsec ? __funnelshift_r(vb[k], vb[k + 1], rw.w)
+                                   : __funnelshift_r(w1[32 * k], w1[32 * k + 1], rw.w);
+        if constexpr (kSumImad) {
+          ev[r][k] = mad_u32(__byte_perm(a, 0u, 0x4240), one, ev[r][k]);
+          ev[r][k] = mad_u32(__byte_perm(b, 0u, 0x4240), one, ev[r][k]);
+          od[r][k] = mad_u32(__byte_perm(a, 0u, 0x4341), one, od[r][k]);
+          od[r][k] = mad_u32(__byte_perm(b, 0u, 0x4341), one, od[r][k]);
+        } else {
+          ev[r][k] += __byte_perm(a, 0u, 0x4240) + __byte_perm(b, 0u, 0x4240);
+          od[r][k] += __byte_perm(a, 0u, 0x4341) + __byte_perm(b, 0u, 0x4341);
+        }
       }
     }
     if constexpr (FLUSH) {
@@ -332,7 +368,7 @@ __global__ void __launch_bounds__(kThreads) k_sum_u8(SumLaunch L) {
     if (r >= g.nrows) break;
 #pragma unroll
     for (int k = 0; k < NW; ++k) {
-      const int64_t t = static_cast<int64_t>(wbase + 32 * k) * 4;  // block-local sample
+      const int64_t t = static_cast<int64_t>(wbase + kStride * k) * 4;  // block-local sample
       if (t >= g.valid) continue;
       uint32_t s0, s1, s2, s3;
       if constexpr (FLUSH) {
@@ -370,14 +406,16 @@ __global__ void __launch_bounds__(kThreads) k_sum_u8(SumLaunch L) {
 // ------------------------------------------------------------------ 16-bit samples
 // L.lane_per: sources summed in 16-bit lanes before widening (< 2: 32-bit sums).
 template <int RB, int NW>
-__global__ void __launch_bounds__(kThreads) k_sum_u16(SumLaunch L) {
+__global__ void __launch_bounds__(kThreads, DD_SUM16_MINB) k_sum_u16(SumLaunch L) {
   extern __shared__ __align__(128) uint32_t sw[];
   __shared__ Pipe P;
   constexpr int T = kWarps * 32 * NW * 2;
   const Geo g = make_geo(L, T);
   if (g.nrows <= 0) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wbase = warp * 32 * NW + lane;
+  constexpr bool kConsec = (NW & 1) != 0;  // lane layout as in k_sum_u8
+  constexpr int kStride = kConsec ? 1 : 32;
+  const int wbase = kConsec ? warp * 32 * NW + lane * NW : warp * 32 * NW + lane;
   uint32_t a16[RB][NW], lo32[RB][NW], hi32[RB][NW];
 #pragma unroll
   for (int r = 0; r < RB; ++r)
@@ -391,13 +429,27 @@ __global__ void __launch_bounds__(kThreads) k_sum_u16(SumLaunch L) {
     if (per >= 2) {
 #pragma unroll
       for (int r = 0; r < RB; ++r) {
-        const int q0 = P.rowq[s][r] + wbase, q1 = P.rowq[s][RB + r] + wbase;
-        const uint32_t s0 = P.rowsh[s][r], s1 = P.rowsh[s][RB + r];
+        const int4 rw = P.row[s][r];
+        const uint32_t* w0 = win + rw.x + wbase;
+        const uint32_t* w1 = win + rw.z + wbase;
+        if ((rw.y | rw.w) == 0) {  // both sources word-aligned (uniform over the block)
 #pragma unroll
-        for (int k = 0; k < NW; ++k) {
-          const uint32_t a = __funnelshift_r(win[q0 + 32 * k], win[q0 + 32 * k + 1], s0);
-          const uint32_t b = __funnelshift_r(win[q1 + 32 * k], win[q1 + 32 * k + 1], s1);
-          a16[r][k] += a + b;
+          for (int k = 0; k < NW; ++k) a16[r][k] += w0[kStride * k] + w1[kStride * k];
+        } else if constexpr (kConsec) {
+          uint32_t va[NW + 1], vb[NW + 1];
+#pragma unroll
+          for (int i = 0; i <= NW; ++i) { va[i] = w0[i]; vb[i] = w1[i]; }
+#pragma unroll
+          for (int k = 0; k < NW; ++k)
+            a16[r][k] += __funnelshift_r(va[k], va[k + 1], rw.y) +
+                         __funnelshift_r(vb[k], vb[k + 1], rw.w);
+        } else {
+#pragma unroll
+          for (int k = 0; k < NW; ++k) {
+            const uint32_t a = __funnelshift_r(w0[32 * k], w0[32 * k + 1], rw.y);
+            const uint32_t b = __funnelshift_r(w1[32 * k], w1[32 * k + 1], rw.w);
+            a16[r][k] += a + b;
+          }
         }
       }
       since += 2;
@@ -415,12 +467,13 @@ __global__ void __launch_bounds__(kThreads) k_sum_u16(SumLaunch L) {
     } else {
 #pragma unroll
       for (int r = 0; r < RB; ++r) {
-        const int q0 = P.rowq[s][r] + wbase, q1 = P.rowq[s][RB + r] + wbase;
-        const uint32_t s0 = P.rowsh[s][r], s1 = P.rowsh[s][RB + r];
+        const int4 rw = P.row[s][r];
+        const uint32_t* w0 = win + rw.x + wbase;
+        const uint32_t* w1 = win + rw.z + wbase;
 #pragma unroll
         for (int k = 0; k < NW; ++k) {
-          const uint32_t a = __funnelshift_r(win[q0 + 32 * k], win[q0 + 32 * k + 1], s0);
-          const uint32_t b = __funnelshift_r(win[q1 + 32 * k], win[q1 + 32 * k + 1], s1);
+          const uint32_t a = __funnelshift_r(w0[kStride * k], w0[kStride * k + 1], rw.y);
+          const uint32_t b = __funnelshift_r(w1[kStride * k], w1[kStride * k + 1], rw.w);
           lo32[r][k] += (a & 0xffffu) + (b & 0xffffu);
           hi32[r][k] += (a >> 16) + (b >> 16);
         }
@@ -433,7 +486,7 @@ __global__ void __launch_bounds__(kThreads) k_sum_u16(SumLaunch L) {
     if (r >= g.nrows) break;
 #pragma unroll
     for (int k = 0; k < NW; ++k) {
-      const int64_t t = static_cast<int64_t>(wbase + 32 * k) * 2;
+      const int64_t t = static_cast<int64_t>(wbase + kStride * k) * 2;
       if (t >= g.valid) continue;
       uint32_t* dst = reinterpret_cast<uint32_t*>(g.out + r * g.out_pitch) + t;
       if (t + 2 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
@@ -510,14 +563,14 @@ void launch_sum(const SumLaunch& L, cudaStream_t st) {
   if (L.rows_per_block != kSumRows) throw Error{DD_ERR_RUNTIME, "unsupported rows per block"};
   if (L.src_bytes == 1) {
     if (L.out_elem == 2) {
-      launch_k(k_sum_u8<kSumRows, 4, true, false>, grid, smem, L, st);
+      launch_k(k_sum_u8<kSumRows, DD_SUM8_NW, true, false>, grid, smem, L, st);
     } else if (L.flush) {
-      launch_k(k_sum_u8<kSumRows, 2, false, true>, grid, smem, L, st);
+      launch_k(k_sum_u8<kSumRows, DD_SUM8F_NW, false, true>, grid, smem, L, st);
     } else {
-      launch_k(k_sum_u8<kSumRows, 4, false, false>, grid, smem, L, st);
+      launch_k(k_sum_u8<kSumRows, DD_SUM8_NW, false, false>, grid, smem, L, st);
     }
   } else {
-    launch_k(k_sum_u16<kSumRows, 2>, grid, smem, L, st);
+    launch_k(k_sum_u16<kSumRows, DD_SUM16_NW>, grid, smem, L, st);
   }
 }
 

@@ -16,7 +16,9 @@ ranks (weak scaling: every rank dedisperses its own chunk; the path has no
 exchange between GPUs).  `e2e` is the same metric through the C ABI with host
 buffers (dd_run_host: host->device copy, run, device->host copy per step).
 `--impl reference` times the reference's own CPU implementation of the path
-(include/cpucal.hpp, built from source into oracle/_ref) on this host's cores.
+(include/cpucal.hpp, built from source into oracle/_ref) on this host's cores;
+`--impl reference-gpu` times the reference's own GPU path (src/core/dedispered.cu
+built for sm_100a, its own per-stage timers) on the same chunk.
 """
 from __future__ import annotations
 
@@ -156,6 +158,67 @@ def reference_cpu_rate(x_host: np.ndarray, hdr: dict, wl: dict, target_s: float)
     return rate, threads, sample, dt
 
 
+def reference_gpu_arm(args, wl, spec, hdr, config, dist, dev):
+    """The reference's own plain GPU call (gpucal::dedisperse_spec from
+    src/core/dedispered.cu, built for sm_100a into oracle/_ref with its AF_DEBUG
+    timers on) on the workload's chunk, one call per step.  `value` uses the
+    reference's device-timed stages (binning, RFI, stage 1, stage 2); `e2e` the
+    host time of the whole call (allocations, pageable copies, sums)."""
+    from astroflow_b200.synth import make_chunk_device
+    from oracle import oracle as O
+
+    if dist.rank != 0:
+        dist.close()
+        return
+    sbw = wl["subband_width"] if wl["algorithm"] == "subband" else None
+    if sbw is None or not O.ref_gpu_timed_available(sbw):
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "the reference GPU path has no "
+                          "brute-force kernels compiled in (AF_USE_SUBBAND), or its timing build "
+                          "oracle/_ref/libref_gpu_timed_sb*.so is missing"}))
+        return
+    x, _ = make_chunk_device(spec, dev)
+    x_host = x.cpu().numpy()
+    del x
+    lo, hi, step = wl["dm"]
+    f32 = np.float32
+    fs = float(f32(hdr["fch1"]))
+    fe = float(f32(f32(hdr["fch1"]) + f32(hdr["nchans"] - 1) * f32(hdr["foff"])))
+    r = wl["rfi"] or {}
+    iq = None
+    if r.get("use_iqrm"):
+        from types import SimpleNamespace
+        iq = SimpleNamespace(**r["iqrm"])
+
+    def call():
+        return O.ref_gpu_time_spec(x_host, hdr["nchans"], hdr["tsamp"], hdr["fch1"], hdr["foff"], lo,
+                                   hi, fs, fe, step, wl["ds"], sb_width=sbw,
+                                   use_zero_dm=r.get("use_zero_dm", False),
+                                   use_iqrm=r.get("use_iqrm", False), iq=iq, device=dev)
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        call()
+    runs = [call() for _ in range(max(1, args.steps))]
+    rows, cols = runs[0][0], runs[0][1]
+    units = rows * cols
+    keys = ["Time binning", "IQRM generate", "IQRM mask", "Zero-DM filtering", "Maskfile marking",
+            "Stage1 (subband)", "Stage2 (subband)"]
+    dev_ms = [sum(t.get(k, 0.0) for k in keys) for _, _, t in runs]
+    wall_ms = [t["wall"] for _, _, t in runs]
+    med = lambda v: float(np.median(v))
+    timers = {k: med([t.get(k, 0.0) for _, _, t in runs]) for k in runs[0][2]}
+    line = {"impl": "reference-gpu", "metric": METRIC, "value": units / (med(dev_ms) * 1e-3),
+            "unit": UNIT, "n_gpus": 1, "steps": len(runs), "warmup": args.warmup,
+            "ms_per_step": med(dev_ms), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": f"u{wl['nbits']}", "data": "synthetic", "config": config,
+            "e2e": {"value": units / (med(wall_ms) * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(x_host.nbytes),
+                    "d2h_bytes_per_step": int(units * 4), "ms_per_step": med(wall_ms)},
+            "reference_timers_ms": timers,
+            "note": "value: the reference's device-timed stages (its AF_DEBUG CUDA-event timers); "
+                    "e2e: host time of the whole reference call"}
+    print(json.dumps(line))
+
+
 # ---------------------------------------------------------------- helpers
 def roofline_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -240,7 +303,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -272,6 +335,10 @@ def main():
                      if wl["rfi"] else "off",
               "l2": "inputs larger than L2 (chunk >> 126 MB), no flush between steps",
               "parallelism": f"replicas x{dist.world} (independent chunks, no exchange)"}
+
+    if args.impl == "reference-gpu":
+        reference_gpu_arm(args, wl, spec, hdr, config, dist, dev)
+        return
 
     if args.impl == "reference":
         if dist.rank != 0:

@@ -435,6 +435,59 @@ def ref_gpu_dedisperse_spec(data, nchans, tsamp, fch1, foff, dm_low, dm_high, fr
     return out[:rows.value * cols.value].reshape(rows.value, cols.value)
 
 
+def ref_gpu_timed_available(sb_width: int) -> bool:
+    return os.path.exists(os.path.join(REF_DIR, f"libref_gpu_timed_sb{sb_width}.so"))
+
+
+def ref_gpu_time_spec(data, nchans, tsamp, fch1, foff, dm_low, dm_high, freq_start, freq_end,
+                      dm_step, ds, t_sample=0.5, sb_width=64, use_mask=False, use_zero_dm=False,
+                      use_iqrm=False, iq=None, device=0):
+    """One call of the reference's gpucal::dedisperse_spec from its timing build:
+    returns (rows, cols, {timer label: ms}) from the reference's own AF_DEBUG
+    timers (CUDA events around H2D, binning, IQRM, zero-DM, stage 1, stage 2,
+    D2H) plus "wall" (host time of the whole call)."""
+    import re
+    import tempfile
+    import time
+
+    data = np.ascontiguousarray(data)
+    nbits = data.dtype.itemsize * 8
+    ndata = data.size // nchans
+    L = ctypes.CDLL(os.path.join(REF_DIR, f"libref_gpu_timed_sb{sb_width}.so"))
+    L.ref_gpu_dedisperse_spec.restype = _c_int
+    L.ref_gpu_dedisperse_spec.argtypes = [
+        _c_int, _P, _c_float, _c_float, _c_float, _c_float, _c_int, _c_long, _c_float,
+        _c_float, _c_float, _c_float, _c_float, _c_int, _c_float, _c_int, ctypes.c_char_p, _P,
+        _P, _c_long, _P, _P, ctypes.c_char_p, _c_int]
+    rows, cols = _c_long(), _c_long()
+    err = ctypes.create_string_buffer(512)
+    r = _tap_rfi(use_mask, use_zero_dm, use_iqrm, iq)
+    libc = ctypes.CDLL(None)
+    with tempfile.TemporaryFile(mode="w+b") as tf:
+        libc.fflush(None)
+        saved = os.dup(1)
+        os.dup2(tf.fileno(), 1)
+        try:
+            t0 = time.perf_counter()
+            rc = L.ref_gpu_dedisperse_spec(
+                nbits, _ptr(data), 0.0, tsamp, fch1, foff, nchans, ndata, dm_low, dm_high,
+                freq_start, freq_end, dm_step, ds, t_sample, device, b"", ctypes.byref(r), None,
+                0, ctypes.byref(rows), ctypes.byref(cols), err, 512)
+            wall = (time.perf_counter() - t0) * 1e3
+            libc.fflush(None)
+        finally:
+            os.dup2(saved, 1)
+            os.close(saved)
+        tf.seek(0)
+        text = tf.read().decode(errors="replace")
+    if rc:
+        raise ValueError(f"reference GPU call failed: {err.value.decode()}")
+    timers = {m.group(1).strip(): float(m.group(2))
+              for m in re.finditer(r"\[TIMER\]\s*(.+?)\s*:\s*([0-9.]+)\s*ms", text)}
+    timers["wall"] = wall
+    return rows.value, cols.value, timers
+
+
 def ref_gpu_dedispered_fil(filename, dm_low, dm_high, freq_start, freq_end, dm_step, ds,
                            t_sample=0.5, sb_width=32, mask_file="", use_mask=False,
                            use_zero_dm=False, use_iqrm=False, iq=None, cap=1 << 22, device=0):

