@@ -28,8 +28,9 @@ FREQ_HEADER, FREQ_FIL = 0, 1
 # Every symbol include/astroflow_dd.h declares.
 EXPORTS = ("dd_plan_create", "dd_plan_destroy", "dd_plan_get_info", "dd_plan_get_tables",
            "dd_plan_set_delay_table", "dd_run", "dd_run_ex", "dd_run_host", "dd_run_profiled",
-           "dd_measure_int_add_rate", "dd_iqrm_masks_noalloc", "dd_last_error",
-           "dd_abi_version")
+           "dd_measure_int_add_rate", "dd_iqrm_masks_noalloc", "dd_batch_create",
+           "dd_batch_run", "dd_batch_status", "dd_batch_get_info", "dd_batch_destroy",
+           "dd_last_error", "dd_abi_version")
 
 
 class Header(ctypes.Structure):
@@ -66,6 +67,11 @@ class PlanInfo(ctypes.Structure):
         "out_elem_bytes", "nsb", "ndm_nom", "max_delay", "max_residual", "nslices",
         "n_iqrm_windows", "workspace_bytes", "delay_rows", "delay_cols",
         "table_mismatch_fp64", "tile_samples")] + [("adds_per_run", ctypes.c_double)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("nplans", "groups", "blocks", "grid", "launches")] + \
+               [("graph", ctypes.c_int32), ("graph_captures", ctypes.c_int32)]
 
 
 class RunStats(ctypes.Structure):
@@ -107,6 +113,12 @@ def load():
                                         ctypes.POINTER(ctypes.c_int32), P]
     L.dd_last_error.restype = ctypes.c_char_p
     L.dd_abi_version.restype = ctypes.c_int
+    L.dd_batch_create.argtypes = [ctypes.POINTER(P), ctypes.c_int32, ctypes.c_int32,
+                                  ctypes.POINTER(P)]
+    L.dd_batch_run.argtypes = [P, ctypes.POINTER(P), ctypes.POINTER(P), P]
+    L.dd_batch_status.argtypes = [P]
+    L.dd_batch_get_info.argtypes = [P, ctypes.POINTER(BatchInfo)]
+    L.dd_batch_destroy.argtypes = [P]
     for name in EXPORTS:
         if name not in ("dd_last_error", "dd_abi_version"):
             getattr(L, name).restype = ctypes.c_int

@@ -44,6 +44,10 @@ Error invalid(const char* fmt, double a = 0, double b = 0, double c = 0, double 
 
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
+// Bytes of one stage-1 sum: uint16 for 8-bit input in narrow subbands, else the
+// reference's accumulator type (uint32, or uint64 for 32-bit samples).
+int64_t inter_elem(const dd_plan& P) { return P.inter16 ? 2 : (P.nbits == 32 ? 8 : 4); }
+
 // ---- frequency table and band (dedispered.cu:1003-1031, cpucal.hpp:85-116)
 void build_freq(dd_plan& P) {
   const int n = P.hdr.nchans;
@@ -326,9 +330,11 @@ void create_subband(dd_plan& P) {
     const int T1 = sum_variant_tile(P.elem, P.nbits == 8 && !P.inter16);
     P.win1 = window_bytes(table_spread(P.h_delay, P.ndm_nom, P.dch, kSumRows, 0), T1, P.elem);
   }
-  if (P.inter16) {
-    const int T2 = sum_variant_tile(2, false);
-    P.win2 = window_bytes(table_spread(P.h_res, P.dm_steps, P.nsb, kSumRows, P.ndm0), T2, 2);
+  if (P.nbits <= 16) {
+    // stage-2 sources: the stage-1 sums (uint16 or uint32)
+    const int e2 = static_cast<int>(inter_elem(P));
+    const int T2 = sum_variant_tile(e2, false);
+    P.win2 = window_bytes(table_spread(P.h_res, P.dm_steps, P.nsb, kSumRows, P.ndm0), T2, e2);
   }
   if (P.win1) upload_desc(P.d_desc1, build_sum_desc(P.h_delay, P.ndm_nom, P.dch, 0));
   if (P.win2) upload_desc(P.d_desc2, build_sum_desc(P.h_res, P.dm_steps, P.nsb, P.ndm0));
@@ -338,8 +344,7 @@ void create_subband(dd_plan& P) {
   // tile of subband sums stays below ~1 GiB.
   // Subband sums: uint16 for 8-bit samples in narrow subbands, else the
   // reference's accumulator type (uint32, or uint64 for 32-bit samples).
-  const int64_t inter_elem = P.inter16 ? 2 : (P.nbits == 32 ? 8 : 4);
-  const int64_t per_col = P.ndm_nom * P.nsb * inter_elem;
+  const int64_t per_col = P.ndm_nom * P.nsb * inter_elem(P);
   // Tile length L plus the stage-2 halo (max_res) should fill whole stage-1 block
   // tiles T1: L = n*T1 - R with R the halo rounded to the base tile.  n grows
   // while one tile of subband sums stays within 1 GiB and the tile is not
@@ -353,13 +358,13 @@ void create_subband(dd_plan& P) {
   P.tile = L;
   // Stage-2 blocks past the tile's last column read up to one block tile beyond it
   // (their columns are not stored).
-  const int64_t T2 = P.win2 ? sum_variant_tile(2, false) : kT;
+  const int64_t T2 = P.win2 ? sum_variant_tile(static_cast<int>(inter_elem(P)), false) : kT;
   P.tile_pitch = round_up(round_up(L + P.max_res, kT) + T2 + 64, 64);
   const int64_t ntiles = (P.nbin + L - 1) / L;
   P.xpitch = round_up(ntiles * L + round_up(L + P.max_res, 8192) + P.max_delay + 8192, 64);
   P.d_x.alloc(static_cast<size_t>(P.dch * P.xpitch) * P.elem);
   DD_CUDA_TRY(cudaMemset(P.d_x.p, 0, P.d_x.bytes));
-  P.d_inter.alloc(static_cast<size_t>(P.ndm_nom * P.nsb * P.tile_pitch) * inter_elem);
+  P.d_inter.alloc(static_cast<size_t>(P.ndm_nom * P.nsb * P.tile_pitch) * inter_elem(P));
   DD_CUDA_TRY(cudaMemset(P.d_inter.p, 0, P.d_inter.bytes));
   if (ds > 1 || callsite_zdm_active(P))
     P.d_binned.alloc(static_cast<size_t>(P.nbin * P.hdr.nchans) * P.elem);
@@ -524,116 +529,155 @@ void run_rfi_and_prep(dd_plan& P, const void* input, uint8_t* masks_out, uint32_
   launch_prep(a, st);
 }
 
+// Staged-sum launches of one subband time tile starting at t0 (stage 1: the
+// prepared input into the tile of subband sums; stage 2: the tile into the output).
+SumLaunch stage1_launch(const dd_plan& P, int64_t t0) {
+  SumLaunch L{};
+  L.mode = SumLaunch::kStage1;
+  L.src = static_cast<const char*>(P.d_x.p);
+  L.src_pitch = P.xpitch * P.elem;
+  L.off = P.d_delay.as<int32_t>();
+  L.off_pitch = P.dch;
+  L.base = t0;
+  L.nsrc_total = P.dch;
+  L.nrows_total = P.ndm_nom;
+  L.group = P.sbw;
+  L.rows_per_block = kSumRows;
+  L.nsb_out = P.nsb;
+  L.out = static_cast<char*>(P.d_inter.p);
+  L.out_pitch = P.tile_pitch * inter_elem(P);
+  L.out_col0 = 0;
+  L.out_elem = static_cast<int>(inter_elem(P));
+  L.ncols = P.tile + P.max_res;
+  L.win_bytes = P.win1;
+  L.src_bytes = P.elem;
+  L.flush = (P.nbits == 8 && !P.inter16) ? 1 : 0;
+  L.lane_per = 1;
+  L.grid_y = static_cast<unsigned>((P.ndm_nom + kSumRows - 1) / kSumRows);
+  L.grid_z = static_cast<unsigned>(P.nsb);
+  L.desc = P.d_desc1.as<SumDesc>();
+  L.desc_pitch = P.dch;
+  L.stages = sum_stages(P.win1);
+  L.err = P.d_err.as<int>();
+  L.one = 1;
+  return L;
+}
+
+SumLaunch stage2_launch(const dd_plan& P, int64_t t0, void* output) {
+  SumLaunch L{};
+  L.mode = SumLaunch::kStage2;
+  L.src = static_cast<const char*>(P.d_inter.p);
+  L.src_pitch = P.tile_pitch * inter_elem(P);
+  L.off = P.d_res.as<int32_t>();
+  L.off_pitch = P.nsb;
+  L.base = 0;
+  L.nsrc_total = P.nsb;
+  L.nrows_total = P.dm_steps;
+  L.group = P.ndm0;
+  L.rows_per_block = kSumRows;
+  L.out = static_cast<char*>(output);
+  L.out_pitch = P.nbin * 4;
+  L.out_col0 = t0;
+  L.out_elem = 4;
+  L.ncols = std::min<int64_t>(P.tile, P.nbin - t0);
+  L.win_bytes = P.win2;
+  L.src_bytes = static_cast<int>(inter_elem(P));
+  L.flush = 0;
+  L.lane_per = P.inter16 ? 65535 / (255 * P.sbw) : 1;
+  L.grid_y = static_cast<unsigned>(P.ndm_nom * ((P.ndm0 + kSumRows - 1) / kSumRows));
+  L.grid_z = 1;
+  L.desc = P.d_desc2.as<SumDesc>();
+  L.desc_pitch = P.nsb;
+  L.stages = sum_stages(P.win2);
+  L.err = P.d_err.as<int>();
+  L.one = 1;
+  return L;
+}
+
 void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out,
                  uint32_t* bounds_out, void* prepped, cudaStream_t st, Prof* pf = nullptr) {
   cudaEvent_t a = pf ? pf->mark() : nullptr;
   run_rfi_and_prep(P, input, masks_out, bounds_out, prepped, st);
   if (pf) pf->prep.emplace_back(a, pf->mark());
   for (int64_t t0 = 0; t0 < P.nbin; t0 += P.tile) {
-    Stage1Args s1{};
-    s1.x = P.d_x.p;
-    s1.xpitch = P.xpitch;
-    s1.nbits = P.nbits;
-    s1.delay1 = P.d_delay.as<int32_t>();
-    s1.dch = P.dch;
-    s1.nsb = P.nsb;
-    s1.ndm_nom = P.ndm_nom;
-    s1.sbw = P.sbw;
-    s1.t0 = t0;
-    s1.ncols = P.tile + P.max_res;
-    s1.inter = P.d_inter.p;
-    s1.tile_pitch = P.tile_pitch;
-    s1.inter16 = P.inter16;
     cudaEvent_t b1 = pf ? pf->mark() : nullptr;
     if (P.win1) {
-      SumLaunch L{};
-      L.mode = SumLaunch::kStage1;
-      L.src = static_cast<const char*>(P.d_x.p);
-      L.src_pitch = P.xpitch * P.elem;
-      L.off = P.d_delay.as<int32_t>();
-      L.off_pitch = P.dch;
-      L.base = t0;
-      L.nsrc_total = P.dch;
-      L.nrows_total = P.ndm_nom;
-      L.group = P.sbw;
-      L.rows_per_block = kSumRows;
-      L.nsb_out = P.nsb;
-      L.out = static_cast<char*>(P.d_inter.p);
-      L.out_pitch = P.tile_pitch * (P.inter16 ? 2 : 4);
-      L.out_col0 = 0;
-      L.out_elem = P.inter16 ? 2 : 4;
-      L.ncols = P.tile + P.max_res;
-      L.win_bytes = P.win1;
-      L.src_bytes = P.elem;
-      L.flush = (P.nbits == 8 && !P.inter16) ? 1 : 0;
-      L.lane_per = 1;
-      L.grid_y = static_cast<unsigned>((P.ndm_nom + kSumRows - 1) / kSumRows);
-      L.grid_z = static_cast<unsigned>(P.nsb);
-      L.desc = P.d_desc1.as<SumDesc>();
-      L.desc_pitch = P.dch;
-      L.stages = sum_stages(P.win1);
-      L.err = P.d_err.as<int>();
-      L.one = 1;
-      launch_sum(L, st);
+      launch_sum(stage1_launch(P, t0), st);
     } else {
+      Stage1Args s1{};
+      s1.x = P.d_x.p;
+      s1.xpitch = P.xpitch;
+      s1.nbits = P.nbits;
+      s1.delay1 = P.d_delay.as<int32_t>();
+      s1.dch = P.dch;
+      s1.nsb = P.nsb;
+      s1.ndm_nom = P.ndm_nom;
+      s1.sbw = P.sbw;
+      s1.t0 = t0;
+      s1.ncols = P.tile + P.max_res;
+      s1.inter = P.d_inter.p;
+      s1.tile_pitch = P.tile_pitch;
+      s1.inter16 = P.inter16;
       launch_stage1(s1, st);
     }
     if (pf) pf->s1.emplace_back(b1, pf->mark());
-    Stage2Args s2{};
-    s2.inter = P.d_inter.p;
-    s2.tile_pitch = P.tile_pitch;
-    s2.inter16 = P.inter16;
-    s2.res = P.d_res.as<int32_t>();
-    s2.nsb = P.nsb;
-    s2.dm_steps = P.dm_steps;
-    s2.ndm0 = P.ndm0;
-    s2.ncols = std::min<int64_t>(P.tile, P.nbin - t0);
-    s2.out = output;
-    s2.out_pitch = P.nbin;
-    s2.col0 = t0;
-    s2.out64 = P.nbits == 32 ? 1 : 0;
-    s2.sbw = P.sbw;
-    s2.src_max = P.sbw * 255;
     cudaEvent_t b2 = pf ? pf->mark() : nullptr;
     if (P.win2) {
-      SumLaunch L{};
-      L.mode = SumLaunch::kStage2;
-      L.src = static_cast<const char*>(P.d_inter.p);
-      L.src_pitch = P.tile_pitch * 2;
-      L.off = P.d_res.as<int32_t>();
-      L.off_pitch = P.nsb;
-      L.base = 0;
-      L.nsrc_total = P.nsb;
-      L.nrows_total = P.dm_steps;
-      L.group = P.ndm0;
-      L.rows_per_block = kSumRows;
-      L.out = static_cast<char*>(output);
-      L.out_pitch = P.nbin * 4;
-      L.out_col0 = t0;
-      L.out_elem = 4;
-      L.ncols = s2.ncols;
-      L.win_bytes = P.win2;
-      L.src_bytes = 2;
-      L.flush = 0;
-      L.lane_per = 65535 / (255 * P.sbw);
-      L.grid_y = static_cast<unsigned>(P.ndm_nom * ((P.ndm0 + kSumRows - 1) / kSumRows));
-      L.grid_z = 1;
-      L.desc = P.d_desc2.as<SumDesc>();
-      L.desc_pitch = P.nsb;
-      L.stages = sum_stages(P.win2);
-      L.err = P.d_err.as<int>();
-      L.one = 1;
-      launch_sum(L, st);
+      launch_sum(stage2_launch(P, t0, output), st);
     } else {
+      Stage2Args s2{};
+      s2.inter = P.d_inter.p;
+      s2.tile_pitch = P.tile_pitch;
+      s2.inter16 = P.inter16;
+      s2.res = P.d_res.as<int32_t>();
+      s2.nsb = P.nsb;
+      s2.dm_steps = P.dm_steps;
+      s2.ndm0 = P.ndm0;
+      s2.ncols = std::min<int64_t>(P.tile, P.nbin - t0);
+      s2.out = output;
+      s2.out_pitch = P.nbin;
+      s2.col0 = t0;
+      s2.out64 = P.nbits == 32 ? 1 : 0;
+      s2.sbw = P.sbw;
+      s2.src_max = P.sbw * 255;
       launch_stage2(s2, st);
     }
     if (pf) pf->s2.emplace_back(b2, pf->mark());
   }
 }
 
-void run_brute(dd_plan& P, const void* input, void* output, void* prepped, cudaStream_t st,
-               Prof* pf = nullptr) {
-  cudaEvent_t e0 = pf ? pf->mark() : nullptr;
+// Staged-sum launch of the brute-force sums (all DMs, all slices at once).
+SumLaunch brute_launch(const dd_plan& P, void* output) {
+  SumLaunch L{};
+  L.mode = SumLaunch::kBrute;
+  L.src = static_cast<const char*>(P.d_x.p);
+  L.src_pitch = P.phase_len * P.elem;
+  L.off = P.d_delay.as<int32_t>();
+  L.off_pitch = P.nc;
+  L.base = 0;
+  L.nsrc_total = P.nc;
+  L.nrows_total = P.dm_steps;
+  L.rows_per_block = kSumRows;
+  L.out = static_cast<char*>(output);
+  L.out_pitch = P.out_cols * 4;
+  L.out_col0 = 0;
+  L.out_elem = 4;
+  L.ncols = P.out_cols;
+  L.win_bytes = P.winb;
+  L.src_bytes = P.elem;
+  L.flush = P.nbits == 8 ? 1 : 0;
+  L.lane_per = 1;
+  L.grid_y = static_cast<unsigned>((P.dm_steps + kSumRows - 1) / kSumRows);
+  L.grid_z = 1;
+  L.desc = P.d_descb.as<SumDesc>();
+  L.desc_pitch = P.nc;
+  L.stages = sum_stages(P.winb);
+  L.err = P.d_err.as<int>();
+  L.one = 1;
+  return L;
+}
+
+void run_brute_prep(dd_plan& P, const void* input, void* prepped, cudaStream_t st) {
   PrepArgs a{};
   a.x = input;
   a.nbits = P.nbits;
@@ -646,6 +690,12 @@ void run_brute(dd_plan& P, const void* input, void* output, void* prepped, cudaS
   a.pitch = P.phase_len;
   a.full_out = prepped;
   launch_prep(a, st);
+}
+
+void run_brute(dd_plan& P, const void* input, void* output, void* prepped, cudaStream_t st,
+               Prof* pf = nullptr) {
+  cudaEvent_t e0 = pf ? pf->mark() : nullptr;
+  run_brute_prep(P, input, prepped, st);
   if (pf) pf->prep.emplace_back(e0, pf->mark());
   cudaEvent_t e1 = pf ? pf->mark() : nullptr;
   BruteArgs b{};
@@ -660,33 +710,7 @@ void run_brute(dd_plan& P, const void* input, void* output, void* prepped, cudaS
   b.out_pitch = P.out_cols;
   b.out64 = P.nbits == 32;
   if (P.winb) {
-    SumLaunch L{};
-    L.mode = SumLaunch::kBrute;
-    L.src = static_cast<const char*>(P.d_x.p);
-    L.src_pitch = P.phase_len * P.elem;
-    L.off = P.d_delay.as<int32_t>();
-    L.off_pitch = P.nc;
-    L.base = 0;
-    L.nsrc_total = P.nc;
-    L.nrows_total = P.dm_steps;
-    L.rows_per_block = kSumRows;
-    L.out = static_cast<char*>(output);
-    L.out_pitch = P.out_cols * 4;
-    L.out_col0 = 0;
-    L.out_elem = 4;
-    L.ncols = P.out_cols;
-    L.win_bytes = P.winb;
-    L.src_bytes = P.elem;
-    L.flush = P.nbits == 8 ? 1 : 0;
-    L.lane_per = 1;
-    L.grid_y = static_cast<unsigned>((P.dm_steps + kSumRows - 1) / kSumRows);
-    L.grid_z = 1;
-    L.desc = P.d_descb.as<SumDesc>();
-    L.desc_pitch = P.nc;
-    L.stages = sum_stages(P.winb);
-    L.err = P.d_err.as<int>();
-    L.one = 1;
-    launch_sum(L, st);
+    launch_sum(brute_launch(P, output), st);
   } else if (P.phases_merge) {
     b.start = 0;
     b.ncols = P.out_cols;
@@ -911,6 +935,7 @@ int dd_plan_set_delay_table(dd_plan* P, const int32_t* delay) {
     if (need + tile_samples() > P->phase_len) throw Error{DD_ERR_INVALID, "delay larger than the plan's padding"};
     std::memcpy(P->h_delay.data(), delay, sizeof(int32_t) * P->h_delay.size());
     P->max_delay = mx;
+    ++P->generation;
     set_brute_window(*P);
     DD_CUDA_TRY(cudaMemcpy(P->d_delay.p, delay, sizeof(int32_t) * P->h_delay.size(), cudaMemcpyHostToDevice));
   });
@@ -997,3 +1022,266 @@ int dd_run_host(dd_plan* P, const void* h_input, void* h_output, void* stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- batches
+// A batch runs one chunk through each of its plans: every plan's RFI and layout
+// kernels, then one persistent launch (k_sum_batch) over the staged sums of all
+// plans, ordered tile by tile (stage 1 of every plan's first tile, stage 2 of
+// every plan's first tile, stage 1 of the second tiles, ...) with completion
+// counters between a plan's dependent stages.  With use_graph the whole
+// sequence is captured into a CUDA graph on the batch's own stream and replayed
+// while the caller passes the same buffers.
+struct dd_batch {
+  int device = 0;
+  std::vector<dd_plan*> plans;
+  std::vector<int64_t> generations;
+  bool use_graph = true;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int captures = 0;
+  std::vector<const void*> cur_in;
+  std::vector<void*> cur_out;
+  bool table_ready = false;
+  std::vector<dd::SumBatchGroup> groups;
+  long long total = 0;
+  size_t smem = 0;
+  unsigned grid = 0;
+  int64_t launches = 0;
+  dd::DevBuf d_groups, d_ctrs, d_next, d_err;
+  ~dd_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_out) cudaEventDestroy(ev_out);
+    if (st) cudaStreamDestroy(st);
+  }
+};
+
+namespace dd {
+namespace {
+
+bool batchable(const dd_plan& P) {
+  if (P.nbits > 16) return false;
+  if (P.p.algorithm == DD_ALGO_BRUTE) return P.winb != 0;
+  return P.win1 != 0 && P.win2 != 0;
+}
+
+long long group_blocks(const SumBatchGroup& g) {
+  return static_cast<long long>(g.gx) * g.L.grid_y * g.L.grid_z;
+}
+
+// The group table for the given outputs (stage-2 / brute-force sums write there).
+void build_groups(dd_batch& B, void* const* outputs) {
+  B.groups.clear();
+  const int n = static_cast<int>(B.plans.size());
+  std::vector<int> prev_ctr(n, -1), prev_need(n, 0);
+  int ctr = 0;
+  long long first = 0;
+  auto add = [&](const SumLaunch& L, int wait_ctr, int wait_need) {
+    SumBatchGroup g{};
+    g.L = L;
+    g.kind = sum_kind(L);
+    g.gx = sum_grid_x(L);
+    g.first = first;
+    g.wait_ctr = wait_ctr;
+    g.wait_need = wait_need;
+    g.done_ctr = ctr++;
+    first += group_blocks(g);
+    B.groups.push_back(g);
+    return B.groups.back();
+  };
+  int64_t max_tiles = 1;
+  for (dd_plan* P : B.plans)
+    if (P->p.algorithm == DD_ALGO_SUBBAND)
+      max_tiles = std::max<int64_t>(max_tiles, (P->nbin + P->tile - 1) / P->tile);
+  for (int64_t k = 0; k < max_tiles; ++k) {
+    std::vector<int> s1_ctr(n, -1), s1_need(n, 0);
+    for (int p = 0; p < n; ++p) {
+      const dd_plan& P = *B.plans[p];
+      if (P.p.algorithm == DD_ALGO_BRUTE) {
+        if (k == 0) add(brute_launch(P, outputs[p]), -1, 0);
+        continue;
+      }
+      if (k * P.tile >= P.nbin) continue;
+      // stage 1 of tile k overwrites the sums stage 2 of tile k-1 reads
+      const SumBatchGroup& g = add(stage1_launch(P, k * P.tile), prev_ctr[p], prev_need[p]);
+      s1_ctr[p] = g.done_ctr;
+      s1_need[p] = static_cast<int>(group_blocks(g));
+    }
+    for (int p = 0; p < n; ++p) {
+      const dd_plan& P = *B.plans[p];
+      if (P.p.algorithm == DD_ALGO_BRUTE || k * P.tile >= P.nbin) continue;
+      const SumBatchGroup& g = add(stage2_launch(P, k * P.tile, outputs[p]), s1_ctr[p], s1_need[p]);
+      prev_ctr[p] = g.done_ctr;
+      prev_need[p] = static_cast<int>(group_blocks(g));
+    }
+  }
+  B.total = first;
+  B.smem = 0;
+  for (const SumBatchGroup& g : B.groups)
+    B.smem = std::max(B.smem, sum_smem_bytes(g.L.win_bytes, g.L.stages));
+  B.d_groups.alloc(sizeof(SumBatchGroup) * B.groups.size());
+  DD_CUDA_TRY(cudaMemcpy(B.d_groups.p, B.groups.data(), sizeof(SumBatchGroup) * B.groups.size(),
+                         cudaMemcpyHostToDevice));
+  B.d_ctrs.alloc(sizeof(int) * std::max(ctr, 1));
+  int dev = 0, sms = 0, per_sm = 0;
+  DD_CUDA_TRY(cudaGetDevice(&dev));
+  DD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  per_sm = sum_batch_blocks_per_sm();
+  int by_smem = 0;
+  DD_CUDA_TRY(cudaDeviceGetAttribute(&by_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  const int fit = static_cast<int>(by_smem / (B.smem + 2048));
+  per_sm = std::max(1, std::min(per_sm, fit));
+  B.grid = static_cast<unsigned>(std::min<long long>(static_cast<long long>(sms) * per_sm,
+                                                     std::max(B.total, 1LL)));
+}
+
+// Everything one run launches, on stream s.
+void enqueue_batch(dd_batch& B, const void* const* inputs, cudaStream_t s) {
+  const long long l0 = launch_count();
+  for (size_t p = 0; p < B.plans.size(); ++p) {
+    dd_plan& P = *B.plans[p];
+    if (P.p.algorithm == DD_ALGO_BRUTE) run_brute_prep(P, inputs[p], nullptr, s);
+    else run_rfi_and_prep(P, inputs[p], nullptr, nullptr, nullptr, s);
+  }
+  DD_CUDA_TRY(cudaMemsetAsync(B.d_ctrs.p, 0, B.d_ctrs.bytes, s));
+  DD_CUDA_TRY(cudaMemsetAsync(B.d_next.p, 0, B.d_next.bytes, s));
+  launch_sum_batch(B.d_groups.as<SumBatchGroup>(), static_cast<int>(B.groups.size()), B.total,
+                   B.d_ctrs.as<int>(), B.d_next.as<unsigned long long>(), B.d_err.as<int>(),
+                   B.smem, B.grid, s);
+  B.launches = launch_count() - l0;
+}
+
+}  // namespace
+}  // namespace dd
+
+extern "C" {
+
+int dd_batch_create(dd_plan* const* plans, int32_t nplans, int32_t use_graph, dd_batch** batch) {
+  if (!plans || nplans < 1 || !batch) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  dd_batch* B = nullptr;
+  const int rc = guarded([&] {
+    for (int i = 0; i < nplans; ++i) {
+      if (!plans[i]) throw Error{DD_ERR_INVALID, "NULL plan"};
+      if (plans[i]->device != plans[0]->device)
+        throw Error{DD_ERR_INVALID, "all plans of a batch must be on one device"};
+      for (int j = 0; j < i; ++j)
+        if (plans[j] == plans[i]) throw Error{DD_ERR_INVALID, "a plan appears twice in the batch"};
+      if (!batchable(*plans[i]))
+        throw Error{DD_ERR_UNSUPPORTED, "plan " + std::to_string(i) +
+                                            " runs direct-load kernels (32-bit samples or offsets "
+                                            "too spread for the staged sums) and cannot be batched"};
+    }
+    DeviceGuard g(plans[0]->device);
+    B = new dd_batch();
+    B->device = plans[0]->device;
+    B->plans.assign(plans, plans + nplans);
+    B->use_graph = use_graph != 0;
+    DD_CUDA_TRY(cudaStreamCreateWithFlags(&B->st, cudaStreamNonBlocking));
+    DD_CUDA_TRY(cudaEventCreateWithFlags(&B->ev_in, cudaEventDisableTiming));
+    DD_CUDA_TRY(cudaEventCreateWithFlags(&B->ev_out, cudaEventDisableTiming));
+    B->d_next.alloc(sizeof(unsigned long long));
+    B->d_err.alloc(sizeof(int));
+    DD_CUDA_TRY(cudaMemset(B->d_err.p, 0, sizeof(int)));
+  });
+  if (rc != DD_OK) {
+    delete B;
+    return rc;
+  }
+  *batch = B;
+  return DD_OK;
+}
+
+int dd_batch_destroy(dd_batch* batch) {
+  if (!batch) return DD_OK;
+  return guarded([&] {
+    DeviceGuard g(batch->device);
+    delete batch;
+  });
+}
+
+int dd_batch_run(dd_batch* B, const void* const* inputs, void* const* outputs, void* stream) {
+  if (!B || !inputs || !outputs) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  return guarded([&] {
+    DeviceGuard g(B->device);
+    const size_t n = B->plans.size();
+    for (size_t p = 0; p < n; ++p)
+      if (!inputs[p] || !outputs[p]) throw Error{DD_ERR_INVALID, "NULL input or output buffer"};
+    std::vector<int64_t> gens(n);
+    for (size_t p = 0; p < n; ++p) gens[p] = B->plans[p]->generation;
+    const bool same = B->table_ready && gens == B->generations &&
+                      std::equal(B->cur_in.begin(), B->cur_in.end(), inputs) &&
+                      std::equal(B->cur_out.begin(), B->cur_out.end(), outputs);
+    cudaStream_t user = static_cast<cudaStream_t>(stream);
+    if (!same) {
+      // the previous run may still read the old table
+      DD_CUDA_TRY(cudaStreamSynchronize(B->st));
+      build_groups(*B, outputs);
+      B->cur_in.assign(inputs, inputs + n);
+      B->cur_out.assign(outputs, outputs + n);
+      B->generations = gens;
+      B->table_ready = true;
+      if (B->exec) {
+        DD_CUDA_TRY(cudaGraphExecDestroy(B->exec));
+        B->exec = nullptr;
+      }
+    }
+    DD_CUDA_TRY(cudaEventRecord(B->ev_in, user));
+    DD_CUDA_TRY(cudaStreamWaitEvent(B->st, B->ev_in, 0));
+    if (B->use_graph) {
+      if (!B->exec) {
+        cudaGraph_t graph = nullptr;
+        DD_CUDA_TRY(cudaStreamBeginCapture(B->st, cudaStreamCaptureModeThreadLocal));
+        try {
+          enqueue_batch(*B, inputs, B->st);
+        } catch (...) {
+          cudaStreamEndCapture(B->st, &graph);
+          if (graph) cudaGraphDestroy(graph);
+          throw;
+        }
+        DD_CUDA_TRY(cudaStreamEndCapture(B->st, &graph));
+        const cudaError_t e = cudaGraphInstantiate(&B->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        DD_CUDA_TRY(e);
+        ++B->captures;
+      }
+      DD_CUDA_TRY(cudaGraphLaunch(B->exec, B->st));
+    } else {
+      enqueue_batch(*B, inputs, B->st);
+    }
+    DD_CUDA_TRY(cudaEventRecord(B->ev_out, B->st));
+    DD_CUDA_TRY(cudaStreamWaitEvent(user, B->ev_out, 0));
+  });
+}
+
+int dd_batch_status(dd_batch* B) {
+  if (!B) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  return guarded([&] {
+    DeviceGuard g(B->device);
+    DD_CUDA_TRY(cudaStreamSynchronize(B->st));
+    int e = 0;
+    DD_CUDA_TRY(cudaMemcpy(&e, B->d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+      DD_CUDA_TRY(cudaMemset(B->d_err.p, 0, sizeof(int)));
+      throw Error{DD_ERR_RUNTIME, "a batched group timed out waiting for its inputs"};
+    }
+    for (dd_plan* P : B->plans) check_device_error(*P, B->st);
+  });
+}
+
+int dd_batch_get_info(const dd_batch* B, dd_batch_info* info) {
+  if (!B || !info) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  dd_batch_info o{};
+  o.nplans = static_cast<int64_t>(B->plans.size());
+  o.groups = static_cast<int64_t>(B->groups.size());
+  o.blocks = B->total;
+  o.grid = B->grid;
+  o.launches = B->launches;
+  o.graph = B->use_graph ? 1 : 0;
+  o.graph_captures = B->captures;
+  *info = o;
+  return DD_OK;
+}
+
+}  // extern "C"
+

@@ -117,6 +117,7 @@ struct dd_plan {
   dd::DevBuf d_desc1, d_desc2, d_descb;  // staging descriptors: stage 1, stage 2, brute force
   dd::DevBuf d_err;      // device error word of the staged sums (0: no error)
   double adds = 0;
+  int64_t generation = 0;  // bumped whenever device tables are replaced
   std::vector<cudaEvent_t> events;  // timing events of dd_run_profiled
   ~dd_plan() {
     for (cudaEvent_t e : events) cudaEventDestroy(e);
@@ -295,9 +296,34 @@ constexpr int kErrWaitEmpty = 2;  // the producer gave up waiting for a free sta
 #ifndef DD_SUM8_MINB
 #define DD_SUM8_MINB 2
 #endif
+constexpr int kSum32NW = 8;  // words per lane of the 32-bit staged sum
 inline int sum_variant_tile(int src_bytes, bool flush) {
-  return sum_tile_samples(src_bytes, src_bytes == 2 ? DD_SUM16_NW : (flush ? DD_SUM8F_NW : DD_SUM8_NW));
+  return sum_tile_samples(src_bytes, src_bytes == 4   ? kSum32NW
+                                     : src_bytes == 2 ? DD_SUM16_NW
+                                                      : (flush ? DD_SUM8F_NW : DD_SUM8_NW));
 }
+// Kernel variant of a staged sum: 8-bit sources into 16-bit sums, 8-bit sources
+// widened to 32 bits (many sources), 8-bit, 16-bit and 32-bit sources.
+enum SumKind { kSumKindU8Out16 = 0, kSumKindU8Flush = 1, kSumKindU8 = 2, kSumKindU16 = 3,
+               kSumKindU32 = 4 };
+int sum_kind(const SumLaunch& L);
+unsigned sum_grid_x(const SumLaunch& L);
+// One group of a batched (persistent) launch: all blocks of one staged sum.
+struct SumBatchGroup {
+  SumLaunch L;
+  int kind;
+  unsigned gx;           // blocks along x (time tiles)
+  long long first;       // index of the group's first block in the batch
+  int wait_ctr;          // counter to wait for (-1: none)
+  int wait_need;         // ... until it reaches this value
+  int done_ctr;          // counter each finished block increments
+  int pad;
+};
+constexpr int kErrWaitGroup = 3;  // a batched group gave up waiting for its inputs
+int sum_batch_blocks_per_sm();
+void launch_sum_batch(const SumBatchGroup* d_groups, int ngroups, long long total, int* d_ctrs,
+                      unsigned long long* d_next, int* d_err, size_t smem, unsigned grid,
+                      cudaStream_t st);
 
 // ---- probes (dd_probe.cu) ----
 double measure_int_add_rate(int device);

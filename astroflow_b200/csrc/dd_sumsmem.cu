@@ -116,17 +116,17 @@ struct Geo {
   int64_t valid;       // columns of this block to store (<= T)
 };
 
-__device__ __forceinline__ Geo make_geo(const SumLaunch& L, int T) {
+__device__ __forceinline__ Geo make_geo(const SumLaunch& L, int T, uint3 blk) {
   Geo g;
-  const int64_t tile = blockIdx.x;
+  const int64_t tile = blk.x;
   const int64_t col = tile * T;  // launch-local column of the block
   g.valid = L.ncols - col;
-  const SumDesc* drow = L.desc + static_cast<int64_t>(blockIdx.y) * L.desc_pitch;
+  const SumDesc* drow = L.desc + static_cast<int64_t>(blk.y) * L.desc_pitch;
   switch (L.mode) {
     case SumLaunch::kStage1: {
       // rows: nominal DMs j0.. of subband sb; sources: the subband's channels
-      const int64_t j0 = static_cast<int64_t>(blockIdx.y) * L.rows_per_block;
-      const int64_t sb = blockIdx.z;
+      const int64_t j0 = static_cast<int64_t>(blk.y) * L.rows_per_block;
+      const int64_t sb = blk.z;
       const int64_t c0 = sb * L.group;
       g.src = L.src + c0 * L.src_pitch;
       g.desc = drow + c0;
@@ -139,8 +139,8 @@ __device__ __forceinline__ Geo make_geo(const SumLaunch& L, int T) {
     case SumLaunch::kStage2: {
       // rows: fine DMs of nominal DM j; sources: the subband sums of j
       const int per_nom = (L.group + L.rows_per_block - 1) / L.rows_per_block;
-      const int64_t j = blockIdx.y / per_nom;
-      const int64_t m0 = j * L.group + static_cast<int64_t>(blockIdx.y % per_nom) * L.rows_per_block;
+      const int64_t j = blk.y / per_nom;
+      const int64_t m0 = j * L.group + static_cast<int64_t>(blk.y % per_nom) * L.rows_per_block;
       const int64_t mend = min((j + 1) * L.group, L.nrows_total);
       g.src = L.src + j * L.nsrc_total * L.src_pitch;
       g.desc = drow;
@@ -151,7 +151,7 @@ __device__ __forceinline__ Geo make_geo(const SumLaunch& L, int T) {
       break;
     }
     default: {  // brute force: rows = DMs, sources = channels
-      const int64_t m0 = static_cast<int64_t>(blockIdx.y) * L.rows_per_block;
+      const int64_t m0 = static_cast<int64_t>(blk.y) * L.rows_per_block;
       g.src = L.src;
       g.desc = drow;
       g.nsrc = static_cast<int>(L.nsrc_total);
@@ -236,6 +236,9 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
     }
     P.failed = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    // order earlier generic accesses to the windows (a previous task of a
+    // persistent block) before the bulk copies that refill them
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   }
   for (int i = threadIdx.x; i < ww; i += kThreads) sw[zero_q + i] = 0u;
   __syncthreads();
@@ -289,15 +292,22 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
       }
     }
   }
+  // every phase has completed: retire the barriers so the next task of a
+  // persistent block can initialise them again
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < S; ++st) {
+      asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_addr(&P.full[st])) : "memory");
+      asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_addr(&P.empty[st])) : "memory");
+    }
+  }
 }
 
 // ------------------------------------------------------------------ 8-bit samples
 template <int RB, int NW, bool OUT16, bool FLUSH>
-__global__ void __launch_bounds__(kThreads, DD_SUM8_MINB) k_sum_u8(SumLaunch L) {
-  extern __shared__ __align__(128) uint32_t sw[];
-  __shared__ Pipe P;
+__device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* sw, Pipe& P) {
   constexpr int T = kWarps * 32 * NW * 4;
-  const Geo g = make_geo(L, T);
+  const Geo g = make_geo(L, T, blk);
   if (g.nrows <= 0) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // odd NW: lane owns NW consecutive words (NW+1 conflict-free loads per row and
@@ -406,11 +416,9 @@ __global__ void __launch_bounds__(kThreads, DD_SUM8_MINB) k_sum_u8(SumLaunch L) 
 // ------------------------------------------------------------------ 16-bit samples
 // L.lane_per: sources summed in 16-bit lanes before widening (< 2: 32-bit sums).
 template <int RB, int NW>
-__global__ void __launch_bounds__(kThreads, DD_SUM16_MINB) k_sum_u16(SumLaunch L) {
-  extern __shared__ __align__(128) uint32_t sw[];
-  __shared__ Pipe P;
+__device__ __forceinline__ void sum_u16(const SumLaunch& L, uint3 blk, uint32_t* sw, Pipe& P) {
   constexpr int T = kWarps * 32 * NW * 2;
-  const Geo g = make_geo(L, T);
+  const Geo g = make_geo(L, T, blk);
   if (g.nrows <= 0) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr bool kConsec = (NW & 1) != 0;  // lane layout as in k_sum_u8
@@ -499,6 +507,137 @@ __global__ void __launch_bounds__(kThreads, DD_SUM16_MINB) k_sum_u16(SumLaunch L
   }
 }
 
+// ------------------------------------------------------------------ 32-bit samples
+// Sources of 32-bit words (stage-1 sums stored as uint32): every sample is a whole
+// word, so no shifts; sums wrap modulo 2^32 like the reference's uint32 accumulators.
+template <int RB, int NW>
+__device__ __forceinline__ void sum_u32(const SumLaunch& L, uint3 blk, uint32_t* sw, Pipe& P) {
+  constexpr int T = kWarps * 32 * NW;
+  const Geo g = make_geo(L, T, blk);
+  if (g.nrows <= 0) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wbase = warp * 32 * NW + lane;
+  uint32_t acc[RB][NW];
+#pragma unroll
+  for (int r = 0; r < RB; ++r)
+#pragma unroll
+    for (int k = 0; k < NW; ++k) acc[r][k] = 0;
+  run_pipeline<4>(L, g, P, sw, 4 * T, [&](int s, const uint32_t* win) {
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+      const int4 rw = P.row[s][r];
+      const uint32_t* w0 = win + rw.x + wbase;
+      const uint32_t* w1 = win + rw.z + wbase;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) acc[r][k] += w0[32 * k] + w1[32 * k];
+    }
+  });
+  if (P.failed) return;
+#pragma unroll
+  for (int r = 0; r < RB; ++r) {
+    if (r >= g.nrows) break;
+    uint32_t* row = reinterpret_cast<uint32_t*>(g.out + r * g.out_pitch);
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      const int64_t t = wbase + 32 * k;
+      if (t < g.valid) row[t] = acc[r][k];
+    }
+  }
+}
+
+template <int RB, int NW, bool OUT16, bool FLUSH>
+__global__ void __launch_bounds__(kThreads, DD_SUM8_MINB) k_sum_u8(SumLaunch L) {
+  extern __shared__ __align__(128) uint32_t sw[];
+  __shared__ Pipe P;
+  sum_u8<RB, NW, OUT16, FLUSH>(L, blockIdx, sw, P);
+}
+template <int RB, int NW>
+__global__ void __launch_bounds__(kThreads, DD_SUM16_MINB) k_sum_u16(SumLaunch L) {
+  extern __shared__ __align__(128) uint32_t sw[];
+  __shared__ Pipe P;
+  sum_u16<RB, NW>(L, blockIdx, sw, P);
+}
+template <int RB, int NW>
+__global__ void __launch_bounds__(kThreads, 2) k_sum_u32(SumLaunch L) {
+  extern __shared__ __align__(128) uint32_t sw[];
+  __shared__ Pipe P;
+  sum_u32<RB, NW>(L, blockIdx, sw, P);
+}
+
+// ------------------------------------------------------------------ batched (persistent)
+// One persistent launch over the blocks of many staged sums (the stages of many
+// plans).  Blocks are handed out in order by an atomic counter; a group whose
+// input is produced by an earlier group waits (bounded) until that group's
+// blocks have all signalled completion.  Since every block of an earlier group
+// has already been handed to a resident block, the waits always end.
+__device__ __forceinline__ void run_kind(int kind, const SumLaunch& L, uint3 blk, uint32_t* sw,
+                                         Pipe& P) {
+  switch (kind) {
+    case kSumKindU8Out16: sum_u8<kSumRows, DD_SUM8_NW, true, false>(L, blk, sw, P); break;
+    case kSumKindU8Flush: sum_u8<kSumRows, DD_SUM8F_NW, false, true>(L, blk, sw, P); break;
+    case kSumKindU8: sum_u8<kSumRows, DD_SUM8_NW, false, false>(L, blk, sw, P); break;
+    case kSumKindU16: sum_u16<kSumRows, DD_SUM16_NW>(L, blk, sw, P); break;
+    default: sum_u32<kSumRows, kSum32NW>(L, blk, sw, P); break;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 2) k_sum_batch(const SumBatchGroup* groups,
+                                                          int ngroups, long long total,
+                                                          int* ctrs, unsigned long long* next,
+                                                          int* err) {
+  extern __shared__ __align__(128) uint32_t sw[];
+  __shared__ Pipe P;
+  __shared__ long long s_blk;
+  __shared__ int s_group, s_ok;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const long long b = static_cast<long long>(atomicAdd(next, 1ull));
+      s_blk = b;
+      s_ok = 1;
+      if (b < total) {
+        int lo = 0, hi = ngroups - 1;  // last group whose first block <= b
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (groups[mid].first <= b) lo = mid; else hi = mid - 1;
+        }
+        s_group = lo;
+        const int wc = groups[lo].wait_ctr;
+        if (wc >= 0) {
+          const int need = groups[lo].wait_need;
+          const long long t0 = clock64();
+          for (;;) {
+            int v;
+            asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(ctrs + wc) : "memory");
+            if (v >= need) break;
+            if (*reinterpret_cast<volatile int*>(err) || clock64() - t0 > kWaitCycles) {
+              atomicCAS(err, 0, kErrWaitGroup);
+              s_ok = 0;
+              break;
+            }
+            __nanosleep(256);
+          }
+          // the bulk copies that follow read what the other blocks wrote
+          asm volatile("fence.proxy.async.global;\n" ::: "memory");
+        }
+      }
+    }
+    __syncthreads();
+    const long long b = s_blk;
+    if (b >= total) break;
+    const SumBatchGroup& G = groups[s_group];
+    long long local = b - G.first;
+    uint3 blk;
+    blk.x = static_cast<unsigned>(local % G.gx);
+    local /= G.gx;
+    blk.y = static_cast<unsigned>(local % G.L.grid_y);
+    blk.z = static_cast<unsigned>(local / G.L.grid_y);
+    if (s_ok) run_kind(G.kind, G.L, blk, sw, P);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(ctrs + G.done_ctr, 1);
+  }
+}
+
 template <typename K>
 void launch_k(K kernel, dim3 grid, size_t smem, const SumLaunch& L, cudaStream_t st) {
   if (smem > 48 * 1024)
@@ -555,23 +694,47 @@ std::vector<SumDesc> build_sum_desc(const std::vector<int32_t>& tab, int64_t nro
 }
 
 void launch_sum(const SumLaunch& L, cudaStream_t st) {
-  const int T = sum_variant_tile(L.src_bytes, L.flush && L.out_elem != 2);
-  dim3 grid(static_cast<unsigned>((L.ncols + T - 1) / T), L.grid_y, L.grid_z);
+  dim3 grid(sum_grid_x(L), L.grid_y, L.grid_z);
   if (L.stages < 2 || L.stages > kMaxStages) throw Error{DD_ERR_RUNTIME, "bad stage count"};
   if (!L.desc || !L.err) throw Error{DD_ERR_RUNTIME, "staged sum without descriptors"};
   const size_t smem = sum_smem_bytes(L.win_bytes, L.stages);
   if (L.rows_per_block != kSumRows) throw Error{DD_ERR_RUNTIME, "unsupported rows per block"};
-  if (L.src_bytes == 1) {
-    if (L.out_elem == 2) {
-      launch_k(k_sum_u8<kSumRows, DD_SUM8_NW, true, false>, grid, smem, L, st);
-    } else if (L.flush) {
-      launch_k(k_sum_u8<kSumRows, DD_SUM8F_NW, false, true>, grid, smem, L, st);
-    } else {
-      launch_k(k_sum_u8<kSumRows, DD_SUM8_NW, false, false>, grid, smem, L, st);
-    }
-  } else {
-    launch_k(k_sum_u16<kSumRows, DD_SUM16_NW>, grid, smem, L, st);
+  switch (sum_kind(L)) {
+    case kSumKindU8Out16: launch_k(k_sum_u8<kSumRows, DD_SUM8_NW, true, false>, grid, smem, L, st); break;
+    case kSumKindU8Flush: launch_k(k_sum_u8<kSumRows, DD_SUM8F_NW, false, true>, grid, smem, L, st); break;
+    case kSumKindU8: launch_k(k_sum_u8<kSumRows, DD_SUM8_NW, false, false>, grid, smem, L, st); break;
+    case kSumKindU16: launch_k(k_sum_u16<kSumRows, DD_SUM16_NW>, grid, smem, L, st); break;
+    default: launch_k(k_sum_u32<kSumRows, kSum32NW>, grid, smem, L, st); break;
   }
+}
+
+int sum_kind(const SumLaunch& L) {
+  if (L.src_bytes == 1) {
+    if (L.out_elem == 2) return kSumKindU8Out16;
+    return L.flush ? kSumKindU8Flush : kSumKindU8;
+  }
+  return L.src_bytes == 2 ? kSumKindU16 : kSumKindU32;
+}
+
+unsigned sum_grid_x(const SumLaunch& L) {
+  const int T = sum_variant_tile(L.src_bytes, L.flush && L.out_elem != 2);
+  return static_cast<unsigned>((L.ncols + T - 1) / T);
+}
+
+int sum_batch_blocks_per_sm() {
+  int n = 0;
+  DD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sum_batch, kThreads, 0));
+  return n;
+}
+
+void launch_sum_batch(const SumBatchGroup* d_groups, int ngroups, long long total, int* d_ctrs,
+                      unsigned long long* d_next, int* d_err, size_t smem, unsigned grid,
+                      cudaStream_t st) {
+  if (smem > 48 * 1024)
+    DD_CUDA_TRY(cudaFuncSetAttribute(k_sum_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+  k_sum_batch<<<grid, kThreads, smem, st>>>(d_groups, ngroups, total, d_ctrs, d_next, d_err);
+  DD_LAUNCHED();
 }
 
 }  // namespace dd

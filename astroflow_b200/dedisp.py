@@ -184,6 +184,67 @@ class Plan:
             pass
 
 
+class Batch:
+    """Many chunks of different geometries in one run (dd_batch_*): each plan's
+    RFI/layout kernels, then one persistent launch over the dedispersion sums of
+    all plans, captured in a CUDA graph and replayed while the same buffers are
+    passed.  Results equal Plan.run of each plan on its chunk."""
+
+    def __init__(self, plans: Sequence[Plan], use_graph: bool = True):
+        if not plans:
+            raise ValueError("a batch needs at least one plan")
+        self.plans = list(plans)
+        arr = (ctypes.c_void_p * len(self.plans))(*[p._h.value for p in self.plans])
+        self._h = ctypes.c_void_p()
+        _lib.check(_lib.load().dd_batch_create(arr, len(self.plans), int(bool(use_graph)),
+                                               ctypes.byref(self._h)))
+
+    def empty_outputs(self):
+        return [p.empty_output() for p in self.plans]
+
+    def run(self, inputs, outputs=None, stream=None):
+        """inputs/outputs: one device tensor per plan (as for Plan.run)."""
+        torch = _torch()
+        if len(inputs) != len(self.plans):
+            raise ValueError(f"expected {len(self.plans)} inputs")
+        if outputs is None:
+            outputs = self.empty_outputs()
+        for p, x, o in zip(self.plans, inputs, outputs):
+            if not x.is_cuda or not x.is_contiguous() or x.element_size() * 8 != p.nbits:
+                raise ValueError(f"input must be a contiguous CUDA tensor of uint{p.nbits}")
+            if x.numel() < p.in_shape[0] * p.in_shape[1]:
+                raise ValueError("input holds fewer than ndata * nchans samples")
+            if tuple(o.shape) != p.out_shape or not o.is_cuda:
+                raise ValueError(f"output must be a CUDA tensor of shape {p.out_shape}")
+        if stream is None:
+            stream = torch.cuda.current_stream(self.plans[0].device)
+        ins = (ctypes.c_void_p * len(inputs))(*[x.data_ptr() for x in inputs])
+        outs = (ctypes.c_void_p * len(outputs))(*[o.data_ptr() for o in outputs])
+        _lib.check(_lib.load().dd_batch_run(self._h, ins, outs, ctypes.c_void_p(stream.cuda_stream)))
+        return outputs
+
+    def status(self) -> None:
+        """Wait for the batch's work; raise if a bounded device wait gave up."""
+        _lib.check(_lib.load().dd_batch_status(self._h))
+
+    @property
+    def info(self) -> dict:
+        i = _lib.BatchInfo()
+        _lib.check(_lib.load().dd_batch_get_info(self._h, ctypes.byref(i)))
+        return {n: getattr(i, n) for n, _ in _lib.BatchInfo._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.load().dd_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def iqrm_masks_noalloc(x, nchans: int, chan_start: int, chan_end: int, tsamp: float,
                        iqrm: IqrmParams, masks, bounds, stream=None) -> int:
     """IQRM window masks through dd_iqrm_masks_noalloc: no device memory is

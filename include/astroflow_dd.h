@@ -247,6 +247,37 @@ int dd_iqrm_masks_noalloc(const void* input, int32_t nbits, int64_t nsamp, int32
                           const dd_iqrm_config* cfg, uint8_t* masks, uint32_t* bounds,
                           int32_t max_windows, int32_t* n_windows, void* stream);
 
+/* ---- Batches: many chunks of different geometries in one persistent launch.
+ * The reference dedisperses one chunk per call (gpucal::dedisperse_spec,
+ * src/core/dedispered.cu:988-1304); a batch runs one chunk through each of its
+ * plans: each plan's binning/RFI/layout kernels, then a single persistent
+ * kernel over the dedispersion sums of all plans (blocks handed out in order,
+ * dependent stages of a plan ordered by completion counters).  Results equal
+ * dd_run of each plan on its chunk.  With use_graph != 0 the run is captured
+ * into a CUDA graph on the batch's own stream and replayed while the same
+ * buffers are passed; new buffers (or a plan whose tables were replaced) cause
+ * one new capture.  Plans must stay alive and unused elsewhere while the batch
+ * runs; plans with 32-bit samples are rejected (DD_ERR_UNSUPPORTED). */
+typedef struct dd_batch dd_batch;
+typedef struct dd_batch_info {
+  int64_t nplans;
+  int64_t groups;          /* staged sums in the persistent launch */
+  int64_t blocks;          /* blocks the persistent launch hands out */
+  int64_t grid;            /* resident blocks of the persistent launch */
+  int64_t launches;        /* kernels one run launches (RFI/layout per plan + 1) */
+  int32_t graph;           /* runs replay a captured CUDA graph */
+  int32_t graph_captures;  /* graphs captured so far */
+} dd_batch_info;
+int dd_batch_create(dd_plan* const* plans, int32_t nplans, int32_t use_graph, dd_batch** batch);
+/* inputs[i], outputs[i]: device buffers of plan i as for dd_run.  Asynchronous
+ * with respect to the host; ordered after earlier work on `stream`, and later
+ * work on `stream` is ordered after it. */
+int dd_batch_run(dd_batch* batch, const void* const* inputs, void* const* outputs, void* stream);
+/* Waits for the batch's work and reports a bounded device wait that gave up. */
+int dd_batch_status(dd_batch* batch);
+int dd_batch_get_info(const dd_batch* batch, dd_batch_info* info);
+int dd_batch_destroy(dd_batch* batch);
+
 /* Last error message of the calling thread ("" if none). */
 const char* dd_last_error(void);
 int dd_abi_version(void);
