@@ -70,8 +70,13 @@ class PlanInfo(ctypes.Structure):
 
 
 class BatchInfo(ctypes.Structure):
-    _fields_ = [(n, ctypes.c_int64) for n in ("nplans", "groups", "blocks", "grid", "launches")] + \
-               [("graph", ctypes.c_int32), ("graph_captures", ctypes.c_int32)]
+    _fields_ = [(n, ctypes.c_int64) for n in ("nplans", "groups", "blocks", "sum_launches",
+                                               "launches", "own_plans")] + \
+               [(n, ctypes.c_int32) for n in ("graph", "persistent", "graph_captures", "pad")]
+
+
+BATCH_GRAPH = 1
+BATCH_PERSISTENT = 2
 
 
 class RunStats(ctypes.Structure):

@@ -1024,18 +1024,25 @@ int dd_run_host(dd_plan* P, const void* h_input, void* h_output, void* stream) {
 }  // extern "C"
 
 // ---------------------------------------------------------------- batches
-// A batch runs one chunk through each of its plans: every plan's RFI and layout
-// kernels, then one persistent launch (k_sum_batch) over the staged sums of all
-// plans, ordered tile by tile (stage 1 of every plan's first tile, stage 2 of
-// every plan's first tile, stage 1 of the second tiles, ...) with completion
-// counters between a plan's dependent stages.  With use_graph the whole
-// sequence is captured into a CUDA graph on the batch's own stream and replayed
-// while the caller passes the same buffers.
+// A batch runs one chunk through each of its plans.  Every plan's RFI and layout
+// kernels run first; then the dedispersion sums of all plans run batched:
+//  * grouped (default): one launch per (time tile, stage, kernel variant) over
+//    that stage of every plan, stage 1 of the first tiles, stage 2 of the first
+//    tiles, stage 1 of the second tiles, ... (stream order keeps each plan's
+//    stages in sequence);
+//  * persistent (DD_BATCH_PERSISTENT): a single launch (k_sum_batch) over all
+//    of them, a plan's dependent stages ordered by completion counters.
+// Plans whose sums cannot be batched (32-bit samples, windows wider than the
+// staged kernels take, or in persistent mode wider than two resident blocks per
+// SM allow) run their own kernels in the same run.  With DD_BATCH_GRAPH the
+// whole sequence is captured into a CUDA graph on the batch's own stream and
+// replayed while the caller passes the same buffers.
 struct dd_batch {
   int device = 0;
   std::vector<dd_plan*> plans;
   std::vector<int64_t> generations;
   bool use_graph = true;
+  bool persistent = false;
   cudaStream_t st = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -1044,9 +1051,17 @@ struct dd_batch {
   std::vector<void*> cur_out;
   bool table_ready = false;
   std::vector<dd::SumBatchGroup> groups;
-  long long total = 0;
-  size_t smem = 0;
-  unsigned grid = 0;
+  struct Launch {  // one batched sum launch over groups [begin, end)
+    int begin = 0, end = 0;
+    long long blocks = 0;
+    size_t smem = 0;
+    int kind = 0;
+    unsigned grid = 0;  // persistent launch: resident blocks
+  };
+  std::vector<Launch> sums;
+  std::vector<char> own;  // per plan: runs its own kernels
+  int nctrs = 0;
+  long long blocks = 0;
   int64_t launches = 0;
   dd::DevBuf d_groups, d_ctrs, d_next, d_err;
   ~dd_batch() {
@@ -1060,95 +1075,157 @@ struct dd_batch {
 namespace dd {
 namespace {
 
-bool batchable(const dd_plan& P) {
+// Shared memory of a staged sum that leaves two persistent blocks per SM.
+constexpr size_t kBatchSmemCap = 100 * 1024;
+
+size_t win_smem(int win) { return win ? sum_smem_bytes(win, sum_stages(win)) : 0; }
+
+// Whether plan P's sums run in the batched launches.
+bool batched_plan(const dd_plan& P, bool persistent) {
   if (P.nbits > 16) return false;
-  if (P.p.algorithm == DD_ALGO_BRUTE) return P.winb != 0;
-  return P.win1 != 0 && P.win2 != 0;
+  const bool brute = P.p.algorithm == DD_ALGO_BRUTE;
+  if (brute ? !P.winb : (!P.win1 || !P.win2)) return false;
+  if (!persistent) return true;
+  return brute ? win_smem(P.winb) <= kBatchSmemCap
+               : win_smem(P.win1) <= kBatchSmemCap && win_smem(P.win2) <= kBatchSmemCap;
 }
 
 long long group_blocks(const SumBatchGroup& g) {
   return static_cast<long long>(g.gx) * g.L.grid_y * g.L.grid_z;
 }
 
-// The group table for the given outputs (stage-2 / brute-force sums write there).
+SumBatchGroup make_group(const SumLaunch& L) {
+  SumBatchGroup g{};
+  g.L = L;
+  g.kind = sum_kind(L);
+  g.gx = sum_grid_x(L);
+  g.wait_ctr = -1;
+  return g;
+}
+
+// The batched sums for the given outputs (stage-2 / brute-force sums write there).
 void build_groups(dd_batch& B, void* const* outputs) {
   B.groups.clear();
+  B.sums.clear();
   const int n = static_cast<int>(B.plans.size());
-  std::vector<int> prev_ctr(n, -1), prev_need(n, 0);
-  int ctr = 0;
-  long long first = 0;
-  auto add = [&](const SumLaunch& L, int wait_ctr, int wait_need) {
-    SumBatchGroup g{};
-    g.L = L;
-    g.kind = sum_kind(L);
-    g.gx = sum_grid_x(L);
-    g.first = first;
-    g.wait_ctr = wait_ctr;
-    g.wait_need = wait_need;
-    g.done_ctr = ctr++;
-    first += group_blocks(g);
-    B.groups.push_back(g);
-    return B.groups.back();
-  };
+  B.own.assign(n, 0);
+  for (int p = 0; p < n; ++p) B.own[p] = batched_plan(*B.plans[p], B.persistent) ? 0 : 1;
   int64_t max_tiles = 1;
-  for (dd_plan* P : B.plans)
-    if (P->p.algorithm == DD_ALGO_SUBBAND)
-      max_tiles = std::max<int64_t>(max_tiles, (P->nbin + P->tile - 1) / P->tile);
-  for (int64_t k = 0; k < max_tiles; ++k) {
-    std::vector<int> s1_ctr(n, -1), s1_need(n, 0);
+  for (int p = 0; p < n; ++p)
+    if (!B.own[p] && B.plans[p]->p.algorithm == DD_ALGO_SUBBAND)
+      max_tiles = std::max<int64_t>(max_tiles, (B.plans[p]->nbin + B.plans[p]->tile - 1) / B.plans[p]->tile);
+  // The sums of one stage of every plan, tile by tile: stage[k][0] = stage 1 of tile
+  // k, stage[k][1] = stage 2 of tile k (and the brute-force sums at k = 0).
+  std::vector<std::vector<std::pair<int, SumLaunch>>> stage(2 * max_tiles);
+  for (int64_t k = 0; k < max_tiles; ++k)
     for (int p = 0; p < n; ++p) {
       const dd_plan& P = *B.plans[p];
+      if (B.own[p]) continue;
       if (P.p.algorithm == DD_ALGO_BRUTE) {
-        if (k == 0) add(brute_launch(P, outputs[p]), -1, 0);
+        if (k == 0) stage[1].emplace_back(p, brute_launch(P, outputs[p]));
         continue;
       }
       if (k * P.tile >= P.nbin) continue;
-      // stage 1 of tile k overwrites the sums stage 2 of tile k-1 reads
-      const SumBatchGroup& g = add(stage1_launch(P, k * P.tile), prev_ctr[p], prev_need[p]);
-      s1_ctr[p] = g.done_ctr;
-      s1_need[p] = static_cast<int>(group_blocks(g));
+      stage[2 * k].emplace_back(p, stage1_launch(P, k * P.tile));
+      stage[2 * k + 1].emplace_back(p, stage2_launch(P, k * P.tile, outputs[p]));
     }
-    for (int p = 0; p < n; ++p) {
-      const dd_plan& P = *B.plans[p];
-      if (P.p.algorithm == DD_ALGO_BRUTE || k * P.tile >= P.nbin) continue;
-      const SumBatchGroup& g = add(stage2_launch(P, k * P.tile, outputs[p]), s1_ctr[p], s1_need[p]);
-      prev_ctr[p] = g.done_ctr;
-      prev_need[p] = static_cast<int>(group_blocks(g));
+  int dev = 0, sms = 0;
+  DD_CUDA_TRY(cudaGetDevice(&dev));
+  DD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  B.nctrs = 0;
+  if (B.persistent) {
+    dd_batch::Launch la;
+    la.begin = 0;
+    std::vector<int> prev_ctr(n, -1), prev_need(n, 0), s1_ctr(n, -1), s1_need(n, 0);
+    for (size_t st = 0; st < stage.size(); ++st)
+      for (auto& [p, L] : stage[st]) {
+        SumBatchGroup g = make_group(L);
+        const bool s1 = (st % 2) == 0;
+        const bool brute = B.plans[p]->p.algorithm == DD_ALGO_BRUTE;
+        // stage 1 of tile k overwrites the sums stage 2 of tile k-1 reads;
+        // stage 2 of tile k reads what stage 1 of tile k wrote
+        if (!brute) {
+          g.wait_ctr = s1 ? prev_ctr[p] : s1_ctr[p];
+          g.wait_need = s1 ? prev_need[p] : s1_need[p];
+        }
+        g.first = la.blocks;
+        g.done_ctr = B.nctrs++;
+        la.blocks += group_blocks(g);
+        la.smem = std::max(la.smem, sum_smem_bytes(L.win_bytes, L.stages));
+        if (!brute) {
+          (s1 ? s1_ctr[p] : prev_ctr[p]) = g.done_ctr;
+          (s1 ? s1_need[p] : prev_need[p]) = static_cast<int>(group_blocks(g));
+        }
+        B.groups.push_back(g);
+      }
+    la.end = static_cast<int>(B.groups.size());
+    if (la.end > 0) {
+      const int per_sm = std::max(1, sum_batch_blocks_per_sm(la.smem));
+      la.grid = static_cast<unsigned>(std::min<long long>(static_cast<long long>(sms) * per_sm, la.blocks));
+      B.sums.push_back(la);
+    }
+  } else {
+    for (auto& list : stage) {
+      // one launch per kernel variant; windows too wide for two blocks per SM get
+      // their own launch so they do not lower the others' occupancy
+      for (int kind = 0; kind <= kSumKindU32; ++kind)
+        for (int wide = 0; wide < 2; ++wide) {
+          dd_batch::Launch la;
+          la.begin = static_cast<int>(B.groups.size());
+          la.kind = kind;
+          for (auto& [p, L] : list) {
+            SumBatchGroup g = make_group(L);
+            const size_t sm = sum_smem_bytes(L.win_bytes, L.stages);
+            if (g.kind != kind || (sm > kBatchSmemCap) != (wide != 0)) continue;
+            g.first = la.blocks;
+            la.blocks += group_blocks(g);
+            la.smem = std::max(la.smem, sm);
+            B.groups.push_back(g);
+          }
+          la.end = static_cast<int>(B.groups.size());
+          if (la.end > la.begin) B.sums.push_back(la);
+        }
     }
   }
-  B.total = first;
-  B.smem = 0;
-  for (const SumBatchGroup& g : B.groups)
-    B.smem = std::max(B.smem, sum_smem_bytes(g.L.win_bytes, g.L.stages));
+  B.blocks = 0;
+  for (const auto& la : B.sums) B.blocks += la.blocks;
+  if (B.groups.empty()) return;
   B.d_groups.alloc(sizeof(SumBatchGroup) * B.groups.size());
   DD_CUDA_TRY(cudaMemcpy(B.d_groups.p, B.groups.data(), sizeof(SumBatchGroup) * B.groups.size(),
                          cudaMemcpyHostToDevice));
-  B.d_ctrs.alloc(sizeof(int) * std::max(ctr, 1));
-  int dev = 0, sms = 0, per_sm = 0;
-  DD_CUDA_TRY(cudaGetDevice(&dev));
-  DD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  per_sm = sum_batch_blocks_per_sm();
-  int by_smem = 0;
-  DD_CUDA_TRY(cudaDeviceGetAttribute(&by_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
-  const int fit = static_cast<int>(by_smem / (B.smem + 2048));
-  per_sm = std::max(1, std::min(per_sm, fit));
-  B.grid = static_cast<unsigned>(std::min<long long>(static_cast<long long>(sms) * per_sm,
-                                                     std::max(B.total, 1LL)));
+  if (B.persistent) {
+    B.d_ctrs.alloc(sizeof(int) * std::max(B.nctrs, 1));
+    B.d_next.alloc(sizeof(unsigned long long));
+  }
 }
 
 // Everything one run launches, on stream s.
-void enqueue_batch(dd_batch& B, const void* const* inputs, cudaStream_t s) {
+void enqueue_batch(dd_batch& B, const void* const* inputs, void* const* outputs,
+                   cudaStream_t s) {
   const long long l0 = launch_count();
   for (size_t p = 0; p < B.plans.size(); ++p) {
     dd_plan& P = *B.plans[p];
-    if (P.p.algorithm == DD_ALGO_BRUTE) run_brute_prep(P, inputs[p], nullptr, s);
-    else run_rfi_and_prep(P, inputs[p], nullptr, nullptr, nullptr, s);
+    const bool brute = P.p.algorithm == DD_ALGO_BRUTE;
+    if (B.own[p]) {
+      if (brute) run_brute(P, inputs[p], outputs[p], nullptr, s);
+      else run_subband(P, inputs[p], outputs[p], nullptr, nullptr, nullptr, s);
+    } else if (brute) {
+      run_brute_prep(P, inputs[p], nullptr, s);
+    } else {
+      run_rfi_and_prep(P, inputs[p], nullptr, nullptr, nullptr, s);
+    }
   }
-  DD_CUDA_TRY(cudaMemsetAsync(B.d_ctrs.p, 0, B.d_ctrs.bytes, s));
-  DD_CUDA_TRY(cudaMemsetAsync(B.d_next.p, 0, B.d_next.bytes, s));
-  launch_sum_batch(B.d_groups.as<SumBatchGroup>(), static_cast<int>(B.groups.size()), B.total,
-                   B.d_ctrs.as<int>(), B.d_next.as<unsigned long long>(), B.d_err.as<int>(),
-                   B.smem, B.grid, s);
+  const SumBatchGroup* dg = B.d_groups.as<SumBatchGroup>();
+  for (const auto& la : B.sums) {
+    if (B.persistent) {
+      DD_CUDA_TRY(cudaMemsetAsync(B.d_ctrs.p, 0, B.d_ctrs.bytes, s));
+      DD_CUDA_TRY(cudaMemsetAsync(B.d_next.p, 0, B.d_next.bytes, s));
+      launch_sum_batch(dg + la.begin, la.end - la.begin, la.blocks, B.d_ctrs.as<int>(),
+                       B.d_next.as<unsigned long long>(), B.d_err.as<int>(), la.smem, la.grid, s);
+    } else {
+      launch_sum_grouped(dg + la.begin, la.end - la.begin, la.blocks, la.kind, la.smem, s);
+    }
+  }
   B.launches = launch_count() - l0;
 }
 
@@ -1157,30 +1234,27 @@ void enqueue_batch(dd_batch& B, const void* const* inputs, cudaStream_t s) {
 
 extern "C" {
 
-int dd_batch_create(dd_plan* const* plans, int32_t nplans, int32_t use_graph, dd_batch** batch) {
+int dd_batch_create(dd_plan* const* plans, int32_t nplans, int32_t flags, dd_batch** batch) {
   if (!plans || nplans < 1 || !batch) { set_error("NULL argument"); return DD_ERR_INVALID; }
   dd_batch* B = nullptr;
   const int rc = guarded([&] {
+    if (flags & ~(DD_BATCH_GRAPH | DD_BATCH_PERSISTENT)) throw Error{DD_ERR_INVALID, "unknown batch flags"};
     for (int i = 0; i < nplans; ++i) {
       if (!plans[i]) throw Error{DD_ERR_INVALID, "NULL plan"};
       if (plans[i]->device != plans[0]->device)
         throw Error{DD_ERR_INVALID, "all plans of a batch must be on one device"};
       for (int j = 0; j < i; ++j)
         if (plans[j] == plans[i]) throw Error{DD_ERR_INVALID, "a plan appears twice in the batch"};
-      if (!batchable(*plans[i]))
-        throw Error{DD_ERR_UNSUPPORTED, "plan " + std::to_string(i) +
-                                            " runs direct-load kernels (32-bit samples or offsets "
-                                            "too spread for the staged sums) and cannot be batched"};
     }
     DeviceGuard g(plans[0]->device);
     B = new dd_batch();
     B->device = plans[0]->device;
     B->plans.assign(plans, plans + nplans);
-    B->use_graph = use_graph != 0;
+    B->use_graph = (flags & DD_BATCH_GRAPH) != 0;
+    B->persistent = (flags & DD_BATCH_PERSISTENT) != 0;
     DD_CUDA_TRY(cudaStreamCreateWithFlags(&B->st, cudaStreamNonBlocking));
     DD_CUDA_TRY(cudaEventCreateWithFlags(&B->ev_in, cudaEventDisableTiming));
     DD_CUDA_TRY(cudaEventCreateWithFlags(&B->ev_out, cudaEventDisableTiming));
-    B->d_next.alloc(sizeof(unsigned long long));
     B->d_err.alloc(sizeof(int));
     DD_CUDA_TRY(cudaMemset(B->d_err.p, 0, sizeof(int)));
   });
@@ -1233,7 +1307,7 @@ int dd_batch_run(dd_batch* B, const void* const* inputs, void* const* outputs, v
         cudaGraph_t graph = nullptr;
         DD_CUDA_TRY(cudaStreamBeginCapture(B->st, cudaStreamCaptureModeThreadLocal));
         try {
-          enqueue_batch(*B, inputs, B->st);
+          enqueue_batch(*B, inputs, outputs, B->st);
         } catch (...) {
           cudaStreamEndCapture(B->st, &graph);
           if (graph) cudaGraphDestroy(graph);
@@ -1247,7 +1321,7 @@ int dd_batch_run(dd_batch* B, const void* const* inputs, void* const* outputs, v
       }
       DD_CUDA_TRY(cudaGraphLaunch(B->exec, B->st));
     } else {
-      enqueue_batch(*B, inputs, B->st);
+      enqueue_batch(*B, inputs, outputs, B->st);
     }
     DD_CUDA_TRY(cudaEventRecord(B->ev_out, B->st));
     DD_CUDA_TRY(cudaStreamWaitEvent(user, B->ev_out, 0));
@@ -1274,10 +1348,14 @@ int dd_batch_get_info(const dd_batch* B, dd_batch_info* info) {
   dd_batch_info o{};
   o.nplans = static_cast<int64_t>(B->plans.size());
   o.groups = static_cast<int64_t>(B->groups.size());
-  o.blocks = B->total;
-  o.grid = B->grid;
+  o.blocks = B->blocks;
+  o.sum_launches = static_cast<int64_t>(B->sums.size());
   o.launches = B->launches;
+  int64_t own = 0;
+  for (char c : B->own) own += c;
+  o.own_plans = own;
   o.graph = B->use_graph ? 1 : 0;
+  o.persistent = B->persistent ? 1 : 0;
   o.graph_captures = B->captures;
   *info = o;
   return DD_OK;

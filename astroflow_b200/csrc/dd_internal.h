@@ -320,10 +320,14 @@ struct SumBatchGroup {
   int pad;
 };
 constexpr int kErrWaitGroup = 3;  // a batched group gave up waiting for its inputs
-int sum_batch_blocks_per_sm();
+int sum_batch_blocks_per_sm(size_t smem);
+// Persistent launch over groups (dependent stages ordered by counters).
 void launch_sum_batch(const SumBatchGroup* d_groups, int ngroups, long long total, int* d_ctrs,
                       unsigned long long* d_next, int* d_err, size_t smem, unsigned grid,
                       cudaStream_t st);
+// Grouped launch: one grid over independent groups of one variant (`kind`).
+void launch_sum_grouped(const SumBatchGroup* d_groups, int ngroups, long long total, int kind,
+                        size_t smem, cudaStream_t st);
 
 // ---- probes (dd_probe.cu) ----
 double measure_int_add_rate(int device);

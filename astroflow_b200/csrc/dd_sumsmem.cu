@@ -564,20 +564,74 @@ __global__ void __launch_bounds__(kThreads, 2) k_sum_u32(SumLaunch L) {
   sum_u32<RB, NW>(L, blockIdx, sw, P);
 }
 
-// ------------------------------------------------------------------ batched (persistent)
-// One persistent launch over the blocks of many staged sums (the stages of many
-// plans).  Blocks are handed out in order by an atomic counter; a group whose
+// ------------------------------------------------------------------ batched launches
+// Block-to-group search: the last group whose first block is <= b.
+__device__ __forceinline__ int find_group(const SumBatchGroup* groups, int ngroups, long long b) {
+  int lo = 0, hi = ngroups - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&groups[mid].first) <= b) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// The group's launch description, once per block, into shared memory.
+__device__ __forceinline__ void load_launch(const SumBatchGroup* g, SumLaunch& s_L) {
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(&g->L);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&s_L);
+  for (int i = threadIdx.x; i < static_cast<int>(sizeof(SumLaunch) / 4); i += kThreads)
+    dst[i] = __ldg(src + i);
+}
+
+__device__ __forceinline__ uint3 group_block(long long local, unsigned gx, unsigned gy) {
+  uint3 blk;
+  blk.x = static_cast<unsigned>(local % gx);
+  local /= gx;
+  blk.y = static_cast<unsigned>(local % gy);
+  blk.z = static_cast<unsigned>(local / gy);
+  return blk;
+}
+
+template <int KIND>
+__device__ __forceinline__ void run_one(const SumLaunch& L, uint3 blk, uint32_t* sw, Pipe& P) {
+  if constexpr (KIND == kSumKindU8Out16) sum_u8<kSumRows, DD_SUM8_NW, true, false>(L, blk, sw, P);
+  else if constexpr (KIND == kSumKindU8Flush) sum_u8<kSumRows, DD_SUM8F_NW, false, true>(L, blk, sw, P);
+  else if constexpr (KIND == kSumKindU8) sum_u8<kSumRows, DD_SUM8_NW, false, false>(L, blk, sw, P);
+  else if constexpr (KIND == kSumKindU16) sum_u16<kSumRows, DD_SUM16_NW>(L, blk, sw, P);
+  else sum_u32<kSumRows, kSum32NW>(L, blk, sw, P);
+}
+
+// Grouped launch: one grid over the blocks of several staged sums of the same
+// variant (the same stage of many plans), none of which reads another's output.
+template <int KIND>
+__global__ void __launch_bounds__(kThreads, 2) k_sum_grouped(const SumBatchGroup* groups,
+                                                            int ngroups) {
+  extern __shared__ __align__(128) uint32_t sw[];
+  __shared__ Pipe P;
+  __shared__ SumLaunch s_L;
+  __shared__ int s_group;
+  const long long b = blockIdx.x;
+  if (threadIdx.x == 0) s_group = find_group(groups, ngroups, b);
+  __syncthreads();
+  const SumBatchGroup* G = groups + s_group;
+  load_launch(G, s_L);
+  __syncthreads();
+  run_one<KIND>(s_L, group_block(b - __ldg(&G->first), __ldg(&G->gx), s_L.grid_y), sw, P);
+}
+
+// Persistent launch over the blocks of many staged sums, dependent stages
+// included.  Blocks are handed out in order by an atomic counter; a group whose
 // input is produced by an earlier group waits (bounded) until that group's
-// blocks have all signalled completion.  Since every block of an earlier group
-// has already been handed to a resident block, the waits always end.
+// blocks have all signalled completion.  Every block of an earlier group has
+// already been handed to a running block, so the waits always end.
 __device__ __forceinline__ void run_kind(int kind, const SumLaunch& L, uint3 blk, uint32_t* sw,
                                          Pipe& P) {
   switch (kind) {
-    case kSumKindU8Out16: sum_u8<kSumRows, DD_SUM8_NW, true, false>(L, blk, sw, P); break;
-    case kSumKindU8Flush: sum_u8<kSumRows, DD_SUM8F_NW, false, true>(L, blk, sw, P); break;
-    case kSumKindU8: sum_u8<kSumRows, DD_SUM8_NW, false, false>(L, blk, sw, P); break;
-    case kSumKindU16: sum_u16<kSumRows, DD_SUM16_NW>(L, blk, sw, P); break;
-    default: sum_u32<kSumRows, kSum32NW>(L, blk, sw, P); break;
+    case kSumKindU8Out16: run_one<kSumKindU8Out16>(L, blk, sw, P); break;
+    case kSumKindU8Flush: run_one<kSumKindU8Flush>(L, blk, sw, P); break;
+    case kSumKindU8: run_one<kSumKindU8>(L, blk, sw, P); break;
+    case kSumKindU16: run_one<kSumKindU16>(L, blk, sw, P); break;
+    default: run_one<kSumKindU32>(L, blk, sw, P); break;
   }
 }
 
@@ -587,23 +641,25 @@ __global__ void __launch_bounds__(kThreads, 2) k_sum_batch(const SumBatchGroup* 
                                                           int* err) {
   extern __shared__ __align__(128) uint32_t sw[];
   __shared__ Pipe P;
+  __shared__ SumLaunch s_L;
   __shared__ long long s_blk;
   __shared__ int s_group, s_ok;
+  // the next block is taken while the current one runs, so the atomic's latency
+  // overlaps work (the hand-out order is unchanged)
+  long long b_next = 0;
+  if (threadIdx.x == 0) b_next = static_cast<long long>(atomicAdd(next, 1ull));
   for (;;) {
     if (threadIdx.x == 0) {
-      const long long b = static_cast<long long>(atomicAdd(next, 1ull));
+      const long long b = b_next;
       s_blk = b;
       s_ok = 1;
       if (b < total) {
-        int lo = 0, hi = ngroups - 1;  // last group whose first block <= b
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (groups[mid].first <= b) lo = mid; else hi = mid - 1;
-        }
-        s_group = lo;
-        const int wc = groups[lo].wait_ctr;
+        b_next = static_cast<long long>(atomicAdd(next, 1ull));
+        const int g = find_group(groups, ngroups, b);
+        s_group = g;
+        const int wc = groups[g].wait_ctr;
         if (wc >= 0) {
-          const int need = groups[lo].wait_need;
+          const int need = groups[g].wait_need;
           const long long t0 = clock64();
           for (;;) {
             int v;
@@ -614,7 +670,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sum_batch(const SumBatchGroup* 
               s_ok = 0;
               break;
             }
-            __nanosleep(256);
+            __nanosleep(128);
           }
           // the bulk copies that follow read what the other blocks wrote
           asm volatile("fence.proxy.async.global;\n" ::: "memory");
@@ -624,17 +680,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_sum_batch(const SumBatchGroup* 
     __syncthreads();
     const long long b = s_blk;
     if (b >= total) break;
-    const SumBatchGroup& G = groups[s_group];
-    long long local = b - G.first;
-    uint3 blk;
-    blk.x = static_cast<unsigned>(local % G.gx);
-    local /= G.gx;
-    blk.y = static_cast<unsigned>(local % G.L.grid_y);
-    blk.z = static_cast<unsigned>(local / G.L.grid_y);
-    if (s_ok) run_kind(G.kind, G.L, blk, sw, P);
+    const SumBatchGroup* G = groups + s_group;
+    load_launch(G, s_L);
+    __syncthreads();
+    if (s_ok) run_kind(G->kind, s_L, group_block(b - G->first, G->gx, s_L.grid_y), sw, P);
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) atomicAdd(ctrs + G.done_ctr, 1);
+    if (threadIdx.x == 0) atomicAdd(ctrs + G->done_ctr, 1);
   }
 }
 
@@ -721,9 +773,9 @@ unsigned sum_grid_x(const SumLaunch& L) {
   return static_cast<unsigned>((L.ncols + T - 1) / T);
 }
 
-int sum_batch_blocks_per_sm() {
+int sum_batch_blocks_per_sm(size_t smem) {
   int n = 0;
-  DD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sum_batch, kThreads, 0));
+  DD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sum_batch, kThreads, smem));
   return n;
 }
 
@@ -735,6 +787,30 @@ void launch_sum_batch(const SumBatchGroup* d_groups, int ngroups, long long tota
                                      static_cast<int>(smem)));
   k_sum_batch<<<grid, kThreads, smem, st>>>(d_groups, ngroups, total, d_ctrs, d_next, d_err);
   DD_LAUNCHED();
+}
+
+template <int KIND>
+void launch_grouped_k(const SumBatchGroup* d_groups, int ngroups, long long total, size_t smem,
+                      cudaStream_t st) {
+  if (smem > 48 * 1024)
+    DD_CUDA_TRY(cudaFuncSetAttribute(k_sum_grouped<KIND>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+  k_sum_grouped<KIND><<<static_cast<unsigned>(total), kThreads, smem, st>>>(d_groups, ngroups);
+  DD_LAUNCHED();
+}
+
+void launch_sum_grouped(const SumBatchGroup* d_groups, int ngroups, long long total, int kind,
+                        size_t smem, cudaStream_t st) {
+  if (total <= 0) return;
+  if (total >= (1LL << 31)) throw Error{DD_ERR_RUNTIME, "grouped launch too large"};
+  switch (kind) {
+    case kSumKindU8Out16: launch_grouped_k<kSumKindU8Out16>(d_groups, ngroups, total, smem, st); break;
+    case kSumKindU8Flush: launch_grouped_k<kSumKindU8Flush>(d_groups, ngroups, total, smem, st); break;
+    case kSumKindU8: launch_grouped_k<kSumKindU8>(d_groups, ngroups, total, smem, st); break;
+    case kSumKindU16: launch_grouped_k<kSumKindU16>(d_groups, ngroups, total, smem, st); break;
+    default: launch_grouped_k<kSumKindU32>(d_groups, ngroups, total, smem, st); break;
+  }
 }
 
 }  // namespace dd

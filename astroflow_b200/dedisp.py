@@ -186,18 +186,20 @@ class Plan:
 
 class Batch:
     """Many chunks of different geometries in one run (dd_batch_*): each plan's
-    RFI/layout kernels, then one persistent launch over the dedispersion sums of
-    all plans, captured in a CUDA graph and replayed while the same buffers are
-    passed.  Results equal Plan.run of each plan on its chunk."""
+    RFI/layout kernels, then the dedispersion sums of all plans batched (one
+    launch per tile, stage and kernel variant over every plan, or with
+    persistent=True one persistent launch), captured in a CUDA graph and
+    replayed while the same buffers are passed.  Results equal Plan.run of each
+    plan on its chunk."""
 
-    def __init__(self, plans: Sequence[Plan], use_graph: bool = True):
+    def __init__(self, plans: Sequence[Plan], use_graph: bool = True, persistent: bool = False):
         if not plans:
             raise ValueError("a batch needs at least one plan")
         self.plans = list(plans)
         arr = (ctypes.c_void_p * len(self.plans))(*[p._h.value for p in self.plans])
         self._h = ctypes.c_void_p()
-        _lib.check(_lib.load().dd_batch_create(arr, len(self.plans), int(bool(use_graph)),
-                                               ctypes.byref(self._h)))
+        flags = (_lib.BATCH_GRAPH if use_graph else 0) | (_lib.BATCH_PERSISTENT if persistent else 0)
+        _lib.check(_lib.load().dd_batch_create(arr, len(self.plans), flags, ctypes.byref(self._h)))
 
     def empty_outputs(self):
         return [p.empty_output() for p in self.plans]

@@ -155,3 +155,39 @@ def make_chunk_device(spec: ChunkSpec, device: int = 0):
                     blk.index_put_((rr, cc), vv, accumulate=True)
         out[r0:r1] = torch.clamp(torch.round(blk), 0, vmax).to(torch.int32).to(dt)
     return out, spec.header()
+
+
+# ---------------------------------------------------------------- heterogeneous batches
+@dataclass
+class BatchChunk:
+    """One chunk of a heterogeneous batch and its dedispersion plan."""
+    spec: ChunkSpec
+    dm_high: float
+    dm_step: float
+    time_downsample: int
+    subband_width: int
+
+
+def draw_batch(n: int = 64, seed: int = 2024, subband_width: int = 32) -> List[BatchChunk]:
+    """Seeded draw of a heterogeneous batch: nchan in {1024, 2048, 4096}, 8- or 16-bit
+    samples, nsamp log-uniform in [2^15, 2^19], band 1000-1500 or 1250-1550 MHz,
+    maximum DM in {500, 1500, 3000} with a step in {0.5, 1, 1.5, 2}, time
+    downsampling in {1, 2, 4, 8}, one dispersed pulse per chunk at a random DM."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        nchans = int(rng.choice([1024, 2048, 4096]))
+        nbits = int(rng.choice([8, 16]))
+        nsamp = int(round(2 ** rng.uniform(15, 19)))
+        f_hi, bw = ((1500.0, 500.0), (1550.0, 300.0))[int(rng.integers(2))]
+        dm_high = float(rng.choice([500.0, 1500.0, 3000.0]))
+        dm_step = float(rng.choice([0.5, 1.0, 1.5, 2.0]))
+        ds = int(rng.choice([1, 2, 4, 8]))
+        tsamp = 49.152e-6
+        dm = float(rng.uniform(0.1, 0.9) * dm_high)
+        amp = 12.0 if nbits == 8 else 1200.0
+        spec = ChunkSpec(nchans=nchans, nsamp=nsamp, nbits=nbits, f_hi=f_hi, bandwidth=bw,
+                         tsamp=tsamp, seed=seed * 1000 + i,
+                         pulses=[(dm, float(rng.uniform(0.1, 0.6)) * nsamp * tsamp, 1e-3, amp)])
+        out.append(BatchChunk(spec, dm_high, dm_step, ds, subband_width))
+    return out

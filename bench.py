@@ -64,11 +64,14 @@ WORKLOADS = {
         nchans=1024, nsamp=1 << 17, nbits=8, dm=(0.0, 1000.0, 1.0), algorithm="brute",
         subband_width=32, ds=1, rfi=None,
         chunk=dict(pulses=[(565.0, 2.0, 1e-3, 12.0)])),
+    # 64 seeded heterogeneous chunks (nchan 1024-4096, 8/16-bit, 2^15-2^19 samples,
+    # two bands, DM ranges up to 3000, downsampling 1-8), dedispersed as batches
+    "batched-64-heterogeneous-subband32": dict(kind="batch", nchunks=64, seed=2024,
+                                               subband_width=32, budget_gb=140.0),
 }
 DEFAULT_WORKLOAD = "wideband-4096ch-u8-2^20-6001dm-subband64-rfi"
 
 
-# ---------------------------------------------------------------- distributed plumbing
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
@@ -156,6 +159,123 @@ def reference_cpu_rate(x_host: np.ndarray, hdr: dict, wl: dict, target_s: float)
               f"the first {n} samples x {nchans} channels, all {ndm} DM trials, "
               f"{threads} OpenMP threads")
     return rate, threads, sample, dt
+
+
+def bench_batch(args, wl, dist, dev):
+    """Heterogeneous batch: the seeded chunks of synth.draw_batch dedispersed (a) one
+    plain call per chunk (Plan.run, back to back on one stream), (b) as a grouped
+    batch and (c) as a persistent batch (Batch, replayed from a CUDA graph).  Chunks
+    are grouped into waves that fit the HBM budget; `value` is the faster batched
+    form's throughput over all chunks."""
+    import torch
+
+    from astroflow_b200.dedisp import Batch, Plan, measure_int_add_rate
+    from astroflow_b200.synth import draw_batch, make_chunk_device
+
+    f32 = np.float32
+    chunks = draw_batch(wl["nchunks"], seed=wl["seed"] + dist.rank, subband_width=wl["subband_width"])
+    budget = wl["budget_gb"] * 1e9
+    stream = torch.cuda.current_stream(dev)
+    times = {"plain": 0.0, "grouped": 0.0, "persistent": 0.0}
+    launches = {"plain": 0, "grouped": 0, "persistent": 0}
+    units_total = adds_total = bytes_total = 0.0
+    waves = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / args.steps
+
+    clocks = ClockSampler(dev)
+    clocks.start()
+    i = 0
+    while i < len(chunks):
+        plans, xs, outs, used = [], [], [], 0.0
+        while i < len(chunks):
+            c = chunks[i]
+            hdr = c.spec.header()
+            for k in ("tsamp", "fch1", "foff"):
+                hdr[k] = float(f32(hdr[k]))
+            lo = float(f32(hdr["fch1"]))
+            hi = float(f32(f32(hdr["fch1"]) + f32(hdr["nchans"] - 1) * f32(hdr["foff"])))
+            plan = Plan(hdr, 0.0, c.dm_high, lo, hi, c.dm_step, c.time_downsample,
+                        algorithm="subband", subband_width=c.subband_width, device=dev)
+            need = (plan.info["workspace_bytes"] + plan.out_shape[0] * plan.out_shape[1] * 4 +
+                    plan.in_shape[0] * plan.in_shape[1] * plan.nbits // 8)
+            if plans and used + need > budget:
+                plan.close()
+                break
+            x, _ = make_chunk_device(c.spec, dev)
+            plans.append(plan)
+            xs.append(x)
+            outs.append(plan.empty_output())
+            used += need
+            i += 1
+        units = sum(p.out_shape[0] * p.out_shape[1] for p in plans)
+        wave = {"chunks": len(plans), "gb": round(used / 1e9, 1), "units": units}
+
+        def plain():
+            for p, x, o in zip(plans, xs, outs):
+                p.run(x, o, stream)
+        wave["plain_ms"] = timed(plain)
+        launches["plain"] += args.steps * sum(p.run_profiled(x, o, stream)["launches"]
+                                              for p, x, o in zip(plans, xs, outs))
+        for mode in ("grouped", "persistent"):
+            batch = Batch(plans, use_graph=True, persistent=(mode == "persistent"))
+            wave[mode + "_ms"] = timed(lambda: batch.run(xs, outs, stream))
+            batch.status()
+            launches[mode] += batch.info["launches"] * args.steps
+            wave[mode + "_sum_launches"] = batch.info["sum_launches"]
+            wave[mode + "_own_plans"] = batch.info["own_plans"]
+            batch.close()
+        for k in times:
+            times[k] += wave[k + "_ms"]
+        units_total += units
+        adds_total += sum(p.info["adds_per_run"] for p in plans)
+        bytes_total += sum(p.in_shape[0] * p.in_shape[1] * p.nbits / 8 + p.out_shape[0] * p.out_shape[1] * 4
+                           for p in plans)
+        waves.append(wave)
+        for p in plans:
+            p.close()
+        del xs, outs
+        torch.cuda.empty_cache()
+    clk = clocks.stop()
+    best = min(("grouped", "persistent"), key=lambda k: times[k])
+    rate = dist.job_rate(units_total, times[best] * 1e-3)
+    rates = {k: dist.job_rate(units_total, t * 1e-3) for k, t in times.items()}
+    ms = dist.max(times[best])
+    hbm_peak, peak_kind = roofline_peaks()
+    add_peak = measure_int_add_rate(dev)
+    t = times[best] * 1e-3
+    roof_s = max(bytes_total / (hbm_peak * 1e9), adds_total / add_peak)
+    if dist.rank == 0:
+        line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": dist.world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "u8/u16", "data": "synthetic (seeded draw of 64 chunks, generated on the GPU)",
+                "config": {"workload": args.workload, "chunks": len(chunks), "batched_form": best,
+                           "waves": waves, "seed": wl["seed"], "subband_width": wl["subband_width"],
+                           "hbm_budget_gb": wl["budget_gb"],
+                           "l2": "inputs larger than L2 per wave; no flush between steps",
+                           "parallelism": f"replicas x{dist.world}"},
+                "forms": {k: {"value": rates[k], "ms_per_step": times[k], "launches": launches[k]}
+                          for k in times},
+                "batched_over_plain": times["plain"] / times[best],
+                "roofline": {"bound": "hbm", "achieved": bytes_total / t / 1e9, "peak": hbm_peak,
+                             "unit": "GB/s", "frac": bytes_total / t / 1e9 / hbm_peak,
+                             "peak_kind": peak_kind, "traffic": None,
+                             "int_add": {"achieved": adds_total / t, "peak": add_peak, "unit": "adds/s",
+                                         "frac": adds_total / t / add_peak},
+                             "step_frac": roof_s / t},
+                "cpu_baseline": None, "e2e": None, "gpu_launches": launches[best], "clocks": clk}
+        print(json.dumps(line))
 
 
 def reference_gpu_arm(args, wl, spec, hdr, config, dist, dev):
@@ -320,6 +440,10 @@ def main():
     dist = Replicas("nccl", timeout_s=300.0)
     dev = dist.local
     torch.cuda.set_device(dev)
+    if wl.get("kind") == "batch":
+        bench_batch(args, wl, dist, dev)
+        dist.close()
+        return
     spec = ChunkSpec(nchans=wl["nchans"], nsamp=wl["nsamp"], nbits=wl["nbits"], seed=dist.chunk_seed(1234),
                      **wl["chunk"])
     hdr = spec.header()

@@ -247,28 +247,38 @@ int dd_iqrm_masks_noalloc(const void* input, int32_t nbits, int64_t nsamp, int32
                           const dd_iqrm_config* cfg, uint8_t* masks, uint32_t* bounds,
                           int32_t max_windows, int32_t* n_windows, void* stream);
 
-/* ---- Batches: many chunks of different geometries in one persistent launch.
+/* ---- Batches: many chunks of different geometries dedispersed together.
  * The reference dedisperses one chunk per call (gpucal::dedisperse_spec,
- * src/core/dedispered.cu:988-1304); a batch runs one chunk through each of its
- * plans: each plan's binning/RFI/layout kernels, then a single persistent
- * kernel over the dedispersion sums of all plans (blocks handed out in order,
- * dependent stages of a plan ordered by completion counters).  Results equal
- * dd_run of each plan on its chunk.  With use_graph != 0 the run is captured
- * into a CUDA graph on the batch's own stream and replayed while the same
- * buffers are passed; new buffers (or a plan whose tables were replaced) cause
- * one new capture.  Plans must stay alive and unused elsewhere while the batch
- * runs; plans with 32-bit samples are rejected (DD_ERR_UNSUPPORTED). */
+ * src/core/dedispered.cu:988-1304).  A batch runs one chunk through each of its
+ * plans: each plan's binning/RFI/layout kernels, then the dedispersion sums of
+ * all plans batched, either as one launch per (time tile, stage, kernel
+ * variant) over that stage of every plan (default), or with DD_BATCH_PERSISTENT
+ * as a single persistent launch over all of them whose blocks are handed out in
+ * order and whose dependent stages wait (bounded) on completion counters.
+ * Results equal dd_run of each plan on its chunk.  With DD_BATCH_GRAPH the run
+ * is captured into a CUDA graph on the batch's own stream and replayed while
+ * the same buffers are passed; new buffers (or a plan whose tables were
+ * replaced) cause one new capture.  Plans must stay alive and unused elsewhere
+ * while the batch runs.  Plans whose sums cannot be batched (32-bit samples,
+ * delay spreads wider than the staged windows) run their own kernels inside the
+ * same run. */
+#define DD_BATCH_GRAPH 1
+#define DD_BATCH_PERSISTENT 2
 typedef struct dd_batch dd_batch;
 typedef struct dd_batch_info {
   int64_t nplans;
-  int64_t groups;          /* staged sums in the persistent launch */
-  int64_t blocks;          /* blocks the persistent launch hands out */
-  int64_t grid;            /* resident blocks of the persistent launch */
-  int64_t launches;        /* kernels one run launches (RFI/layout per plan + 1) */
+  int64_t groups;          /* batched staged sums */
+  int64_t blocks;          /* blocks of all batched sum launches */
+  int64_t sum_launches;    /* batched sum launches per run */
+  int64_t launches;        /* kernels one run launches (all of them) */
+  int64_t own_plans;       /* plans that run their own kernels */
   int32_t graph;           /* runs replay a captured CUDA graph */
+  int32_t persistent;      /* sums in one persistent launch */
   int32_t graph_captures;  /* graphs captured so far */
+  int32_t pad;
 } dd_batch_info;
-int dd_batch_create(dd_plan* const* plans, int32_t nplans, int32_t use_graph, dd_batch** batch);
+/* flags: DD_BATCH_GRAPH | DD_BATCH_PERSISTENT. */
+int dd_batch_create(dd_plan* const* plans, int32_t nplans, int32_t flags, dd_batch** batch);
 /* inputs[i], outputs[i]: device buffers of plan i as for dd_run.  Asynchronous
  * with respect to the host; ordered after earlier work on `stream`, and later
  * work on `stream` is ordered after it. */

@@ -56,14 +56,15 @@ def make(case, seed):
     return plan, dev(x)
 
 
-@pytest.mark.parametrize("use_graph", [True, False])
-def test_batch_equals_individual_runs(use_graph):
+@pytest.mark.parametrize("use_graph,persistent", [(True, False), (False, False), (True, True),
+                                                   (False, True)])
+def test_batch_equals_individual_runs(use_graph, persistent):
     items = [make(c, 40 + i) for i, c in enumerate(CHUNKS)]
     plans = [p for p, _ in items]
     xs = [x for _, x in items]
     want = [to_np(p.run(x)) for p, x in items]
     torch.cuda.synchronize()
-    batch = Batch(plans, use_graph=use_graph)
+    batch = Batch(plans, use_graph=use_graph, persistent=persistent)
     outs = batch.empty_outputs()
     for rep in range(3):  # replays of the same buffers
         for o in outs:
@@ -74,6 +75,7 @@ def test_batch_equals_individual_runs(use_graph):
             assert np.array_equal(to_np(o), w), f"chunk {i} differs (run {rep})"
     info = batch.info
     assert info["nplans"] == len(CHUNKS) and info["graph"] == int(use_graph)
+    assert info["persistent"] == int(persistent) and info["sum_launches"] >= 1
     assert info["graph_captures"] == (1 if use_graph else 0)
     # new output buffers: one more capture, same results
     outs2 = batch.empty_outputs()
@@ -85,13 +87,22 @@ def test_batch_equals_individual_runs(use_graph):
     batch.close()
 
 
-def test_batch_rejects_32bit_plans_and_duplicates():
+@pytest.mark.parametrize("persistent", [False, True])
+def test_batch_runs_own_kernels_for_32bit_plans(persistent):
+    """A 32-bit plan (direct-load kernels) next to staged plans: all results exact."""
     rng = np.random.default_rng(0)
     hdr = dict(tsamp=1e-4, fch1=1200.0, foff=1.0, nbits=32, nchans=64, ndata=2048)
+    x32 = rng.integers(0, 1 << 20, size=(2048, 64)).astype(np.uint32)
     p32 = Plan(hdr, 0.0, 50.0, 1200.0, 1263.0, 1.0, 1, algorithm="subband")
-    with pytest.raises(RuntimeError, match="cannot be batched"):
-        Batch([p32])
-    p8, _ = make(CHUNKS[0], 1)
+    d32 = torch.from_numpy(x32.view(np.int32)).cuda().view(torch.uint32)
+    p8, x8 = make(CHUNKS[0], 1)
+    want32 = p32.run(d32).view(torch.int64).cpu().numpy()
+    want8 = to_np(p8.run(x8))
+    batch = Batch([p32, p8], persistent=persistent)
+    o32, o8 = batch.run([d32, x8])
+    batch.status()
+    assert batch.info["own_plans"] == 1
+    assert np.array_equal(o32.view(torch.int64).cpu().numpy(), want32)
+    assert np.array_equal(to_np(o8), want8)
     with pytest.raises(ValueError, match="twice"):
         Batch([p8, p8])
-    del rng
