@@ -30,6 +30,8 @@ EXPORTS = ("dd_plan_create", "dd_plan_destroy", "dd_plan_get_info", "dd_plan_get
            "dd_plan_set_delay_table", "dd_run", "dd_run_ex", "dd_run_host", "dd_run_profiled",
            "dd_measure_int_add_rate", "dd_iqrm_masks_noalloc", "dd_batch_create",
            "dd_batch_run", "dd_batch_status", "dd_batch_get_info", "dd_batch_destroy",
+           "dd_stream_open", "dd_stream_push", "dd_stream_get_info", "dd_stream_plan",
+           "dd_stream_close",
            "dd_last_error", "dd_abi_version")
 
 
@@ -73,6 +75,13 @@ class BatchInfo(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in ("nplans", "groups", "blocks", "sum_launches",
                                                "launches", "own_plans")] + \
                [(n, ctypes.c_int32) for n in ("graph", "persistent", "graph_captures", "pad")]
+
+
+class StreamInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("dm_steps", "out_cols", "chunk_samples",
+                                               "tail_samples", "pushed_samples",
+                                               "workspace_bytes")] + \
+               [("adds_per_push", ctypes.c_double)]
 
 
 BATCH_GRAPH = 1
@@ -124,6 +133,13 @@ def load():
     L.dd_batch_status.argtypes = [P]
     L.dd_batch_get_info.argtypes = [P, ctypes.POINTER(BatchInfo)]
     L.dd_batch_destroy.argtypes = [P]
+    L.dd_stream_open.argtypes = [ctypes.POINTER(Header), ctypes.POINTER(PlanParams),
+                                 ctypes.POINTER(RfiConfig), P, ctypes.c_int32, ctypes.c_int32,
+                                 ctypes.POINTER(P)]
+    L.dd_stream_push.argtypes = [P, P, P, P]
+    L.dd_stream_get_info.argtypes = [P, ctypes.POINTER(StreamInfo)]
+    L.dd_stream_plan.argtypes = [P, ctypes.POINTER(P)]
+    L.dd_stream_close.argtypes = [P]
     for name in EXPORTS:
         if name not in ("dd_last_error", "dd_abi_version"):
             getattr(L, name).restype = ctypes.c_int

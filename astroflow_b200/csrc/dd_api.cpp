@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <limits>
 #include <new>
 #include <string>
@@ -275,6 +276,7 @@ void create_subband(dd_plan& P) {
   P.ndm0 = P.p.ndm0 > 0 ? P.p.ndm0 : 32;
   const int ds = P.p.time_downsample;
   P.nbin = (P.nin + ds - 1) / ds;
+  if (P.nout <= 0 || P.nout > P.nbin) P.nout = P.nbin;
   P.dch = P.ce - P.cs + 1;
   P.nsb = (P.dch + P.sbw - 1) / P.sbw;
   P.ndm_nom = (P.dm_steps + P.ndm0 - 1) / P.ndm0;
@@ -353,7 +355,7 @@ void create_subband(dd_plan& P) {
   const int64_t R = round_up(std::max<int64_t>(P.max_res, 1), kT);
   int64_t n = 1;
   while (n * T1 - R < kT) ++n;
-  while (((n + 1) * T1 - R) * per_col <= (int64_t(1) << 30) && (n * T1 - R) < P.nbin) ++n;
+  while (((n + 1) * T1 - R) * per_col <= (int64_t(1) << 30) && (n * T1 - R) < P.nout) ++n;
   int64_t L = std::max<int64_t>(kT, n * T1 - R);
   P.tile = L;
   // Stage-2 blocks past the tile's last column read up to one block tile beyond it
@@ -368,8 +370,8 @@ void create_subband(dd_plan& P) {
   DD_CUDA_TRY(cudaMemset(P.d_inter.p, 0, P.d_inter.bytes));
   if (ds > 1 || callsite_zdm_active(P))
     P.d_binned.alloc(static_cast<size_t>(P.nbin * P.hdr.nchans) * P.elem);
-  P.adds = static_cast<double>(P.ndm_nom) * P.dch * P.nbin +
-           static_cast<double>(P.dm_steps) * P.nsb * P.nbin;
+  P.adds = static_cast<double>(P.ndm_nom) * P.dch * P.nout +
+           static_cast<double>(P.dm_steps) * P.nsb * P.nout;
 }
 
 // The staged-window sums serve 8- and 16-bit samples without downsampling (one
@@ -576,10 +578,10 @@ SumLaunch stage2_launch(const dd_plan& P, int64_t t0, void* output) {
   L.group = P.ndm0;
   L.rows_per_block = kSumRows;
   L.out = static_cast<char*>(output);
-  L.out_pitch = P.nbin * 4;
+  L.out_pitch = P.nout * 4;
   L.out_col0 = t0;
   L.out_elem = 4;
-  L.ncols = std::min<int64_t>(P.tile, P.nbin - t0);
+  L.ncols = std::min<int64_t>(P.tile, P.nout - t0);
   L.win_bytes = P.win2;
   L.src_bytes = static_cast<int>(inter_elem(P));
   L.flush = 0;
@@ -599,7 +601,7 @@ void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out
   cudaEvent_t a = pf ? pf->mark() : nullptr;
   run_rfi_and_prep(P, input, masks_out, bounds_out, prepped, st);
   if (pf) pf->prep.emplace_back(a, pf->mark());
-  for (int64_t t0 = 0; t0 < P.nbin; t0 += P.tile) {
+  for (int64_t t0 = 0; t0 < P.nout; t0 += P.tile) {
     cudaEvent_t b1 = pf ? pf->mark() : nullptr;
     if (P.win1) {
       launch_sum(stage1_launch(P, t0), st);
@@ -633,9 +635,9 @@ void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out
       s2.nsb = P.nsb;
       s2.dm_steps = P.dm_steps;
       s2.ndm0 = P.ndm0;
-      s2.ncols = std::min<int64_t>(P.tile, P.nbin - t0);
+      s2.ncols = std::min<int64_t>(P.tile, P.nout - t0);
       s2.out = output;
-      s2.out_pitch = P.nbin;
+      s2.out_pitch = P.nout;
       s2.col0 = t0;
       s2.out64 = P.nbits == 32 ? 1 : 0;
       s2.sbw = P.sbw;
@@ -810,69 +812,77 @@ int dd_abi_version(void) { return DD_ABI_VERSION; }
 
 const char* dd_last_error(void) { return g_last_error.c_str(); }
 
+}  // extern "C"
+
+namespace dd {
+namespace {
+// Builds a plan (throws on error).  nout > 0 limits a subband plan's output to
+// the first nout binned columns (the plan of a stream).
+dd_plan* make_plan(const dd_header* header, const dd_plan_params* params, const dd_rfi_config* rfi,
+                   const int32_t* bad_channels, int32_t n_bad, int32_t device, int64_t nout) {
+  if (!header || !params) throw Error{DD_ERR_INVALID, "header and params are required"};
+  if (header->nbits != 8 && header->nbits != 16 && header->nbits != 32)
+    throw Error{DD_ERR_INVALID, "nbits must be 8, 16 or 32"};
+  if (header->nchans < 2 || header->ndata < 1 || !(header->tsamp > 0))
+    throw Error{DD_ERR_INVALID, "header needs nchans >= 2, ndata >= 1 and tsamp > 0"};
+  if (params->time_downsample < 1) throw Error{DD_ERR_INVALID, "time_downsample must be >= 1"};
+  if (!(params->dm_step > 0) || params->dm_high < params->dm_low)
+    throw Error{DD_ERR_INVALID, "Invalid DM parameters"};
+  int ndev = 0;
+  DD_CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (ndev == 0) throw Error{DD_ERR_RUNTIME, "No CUDA devices found"};
+  if (device < 0 || device >= ndev) throw Error{DD_ERR_INVALID, "invalid target device"};
+  DeviceGuard g(device);
+  std::unique_ptr<dd_plan> P(new dd_plan());
+  P->hdr = *header;
+  P->p = *params;
+  if (rfi) P->rfi = *rfi;
+  if (P->p.algorithm == DD_ALGO_BRUTE) {
+    // The CPU path the brute-force mode follows has no RFI stages.
+    P->rfi.use_iqrm = P->rfi.use_mask = P->rfi.use_zero_dm = 0;
+  }
+  if (bad_channels && n_bad > 0) P->bad.assign(bad_channels, bad_channels + n_bad);
+  P->device = device;
+  P->nbits = header->nbits;
+  P->elem = header->nbits / 8;
+  P->nin = header->ndata;
+  P->nout = nout;
+  // The reference's GPU path casts sample counts to unsigned int in its RFI
+  // kernels (rfimarker.cu, iqrm.cu).
+  if (P->nin >= (int64_t(1) << 32)) throw Error{DD_ERR_INVALID, "ndata too large"};
+  // Floating-point forms of the reference's IQRM arithmetic (bit 8: std from a
+  // fused multiply-add; bit 4: threshold through the reciprocal of 1.349).
+  P->iqrm_variant = 8 | 4;
+  if (const char* v = std::getenv("ASTROFLOW_DD_IQRM_VARIANT")) P->iqrm_variant = std::atoi(v);
+  // The _dedisperse_spec path's Header carries tsamp as float.
+  P->tsamp = P->p.freq_mode == DD_FREQ_FIL ? header->tsamp
+                                            : static_cast<double>(static_cast<float>(header->tsamp));
+  P->d_err.alloc(sizeof(int));
+  DD_CUDA_TRY(cudaMemset(P->d_err.p, 0, sizeof(int)));
+  build_freq(*P);
+  build_band(*P);
+  if (P->p.algorithm == DD_ALGO_BRUTE) {
+    create_brute(*P);
+  } else if (P->p.algorithm == DD_ALGO_SUBBAND) {
+    create_subband(*P);
+    create_rfi(*P);
+  } else {
+    throw Error{DD_ERR_INVALID, "unknown algorithm"};
+  }
+  DD_CUDA_TRY(cudaDeviceSynchronize());
+  return P.release();
+}
+}  // namespace
+}  // namespace dd
+
+extern "C" {
+
 int dd_plan_create(const dd_header* header, const dd_plan_params* params,
                    const dd_rfi_config* rfi, const int32_t* bad_channels, int32_t n_bad,
                    int32_t device, dd_plan** plan) {
   if (!plan) { set_error("plan pointer is NULL"); return DD_ERR_INVALID; }
   *plan = nullptr;
-  dd_plan* P = nullptr;
-  int rc = guarded([&] {
-    if (!header || !params) throw Error{DD_ERR_INVALID, "header and params are required"};
-    if (header->nbits != 8 && header->nbits != 16 && header->nbits != 32)
-      throw Error{DD_ERR_INVALID, "nbits must be 8, 16 or 32"};
-    if (header->nchans < 2 || header->ndata < 1 || !(header->tsamp > 0))
-      throw Error{DD_ERR_INVALID, "header needs nchans >= 2, ndata >= 1 and tsamp > 0"};
-    if (params->time_downsample < 1) throw Error{DD_ERR_INVALID, "time_downsample must be >= 1"};
-    if (!(params->dm_step > 0) || params->dm_high < params->dm_low)
-      throw Error{DD_ERR_INVALID, "Invalid DM parameters"};
-    int ndev = 0;
-    DD_CUDA_TRY(cudaGetDeviceCount(&ndev));
-    if (ndev == 0) throw Error{DD_ERR_RUNTIME, "No CUDA devices found"};
-    if (device < 0 || device >= ndev) throw Error{DD_ERR_INVALID, "invalid target device"};
-    DeviceGuard g(device);
-    P = new dd_plan();
-    P->hdr = *header;
-    P->p = *params;
-    if (rfi) P->rfi = *rfi;
-    if (P->p.algorithm == DD_ALGO_BRUTE) {
-      // The CPU path the brute-force mode follows has no RFI stages.
-      P->rfi.use_iqrm = P->rfi.use_mask = P->rfi.use_zero_dm = 0;
-    }
-    if (bad_channels && n_bad > 0) P->bad.assign(bad_channels, bad_channels + n_bad);
-    P->device = device;
-    P->nbits = header->nbits;
-    P->elem = header->nbits / 8;
-    P->nin = header->ndata;
-    // The reference's GPU path casts sample counts to unsigned int in its RFI
-    // kernels (rfimarker.cu, iqrm.cu).
-    if (P->nin >= (int64_t(1) << 32)) throw Error{DD_ERR_INVALID, "ndata too large"};
-    // Floating-point forms of the reference's IQRM arithmetic (bit 8: std from a
-    // fused multiply-add; bit 4: threshold through the reciprocal of 1.349).
-    P->iqrm_variant = 8 | 4;
-    if (const char* v = std::getenv("ASTROFLOW_DD_IQRM_VARIANT")) P->iqrm_variant = std::atoi(v);
-    // The _dedisperse_spec path's Header carries tsamp as float.
-    P->tsamp = P->p.freq_mode == DD_FREQ_FIL ? header->tsamp
-                                              : static_cast<double>(static_cast<float>(header->tsamp));
-    P->d_err.alloc(sizeof(int));
-    DD_CUDA_TRY(cudaMemset(P->d_err.p, 0, sizeof(int)));
-    build_freq(*P);
-    build_band(*P);
-    if (P->p.algorithm == DD_ALGO_BRUTE) {
-      create_brute(*P);
-    } else if (P->p.algorithm == DD_ALGO_SUBBAND) {
-      create_subband(*P);
-      create_rfi(*P);
-    } else {
-      throw Error{DD_ERR_INVALID, "unknown algorithm"};
-    }
-    DD_CUDA_TRY(cudaDeviceSynchronize());
-  });
-  if (rc != DD_OK) {
-    delete P;
-    return rc;
-  }
-  *plan = P;
-  return DD_OK;
+  return guarded([&] { *plan = make_plan(header, params, rfi, bad_channels, n_bad, device, 0); });
 }
 
 int dd_plan_destroy(dd_plan* plan) {
@@ -892,7 +902,7 @@ int dd_plan_get_info(const dd_plan* P, dd_plan_info* info) {
     o.dm_steps = P->dm_steps;
     o.nsamp_in = P->nin;
     o.nsamp_binned = P->nbin;
-    o.out_cols = P->p.algorithm == DD_ALGO_BRUTE ? P->out_cols : P->nbin;
+    o.out_cols = P->p.algorithm == DD_ALGO_BRUTE ? P->out_cols : P->nout;
     o.out_elem_bytes = P->nbits == 32 ? 8 : 4;
     o.nsb = P->nsb;
     o.ndm_nom = P->ndm_nom;
@@ -1000,7 +1010,7 @@ int dd_run_host(dd_plan* P, const void* h_input, void* h_output, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t in_bytes = static_cast<size_t>(P->nin * P->hdr.nchans) * P->elem;
     const size_t out_bytes = static_cast<size_t>(P->dm_steps) *
-                             (P->p.algorithm == DD_ALGO_BRUTE ? P->out_cols : P->nbin) *
+                             (P->p.algorithm == DD_ALGO_BRUTE ? P->out_cols : P->nout) *
                              (P->nbits == 32 ? 8 : 4);
     void* d_in = nullptr;
     void* d_out = nullptr;
@@ -1113,7 +1123,7 @@ void build_groups(dd_batch& B, void* const* outputs) {
   int64_t max_tiles = 1;
   for (int p = 0; p < n; ++p)
     if (!B.own[p] && B.plans[p]->p.algorithm == DD_ALGO_SUBBAND)
-      max_tiles = std::max<int64_t>(max_tiles, (B.plans[p]->nbin + B.plans[p]->tile - 1) / B.plans[p]->tile);
+      max_tiles = std::max<int64_t>(max_tiles, (B.plans[p]->nout + B.plans[p]->tile - 1) / B.plans[p]->tile);
   // The sums of one stage of every plan, tile by tile: stage[k][0] = stage 1 of tile
   // k, stage[k][1] = stage 2 of tile k (and the brute-force sums at k = 0).
   std::vector<std::vector<std::pair<int, SumLaunch>>> stage(2 * max_tiles);
@@ -1125,7 +1135,7 @@ void build_groups(dd_batch& B, void* const* outputs) {
         if (k == 0) stage[1].emplace_back(p, brute_launch(P, outputs[p]));
         continue;
       }
-      if (k * P.tile >= P.nbin) continue;
+      if (k * P.tile >= P.nout) continue;
       stage[2 * k].emplace_back(p, stage1_launch(P, k * P.tile));
       stage[2 * k + 1].emplace_back(p, stage2_launch(P, k * P.tile, outputs[p]));
     }
@@ -1363,3 +1373,119 @@ int dd_batch_get_info(const dd_batch* B, dd_batch_info* info) {
 
 }  // extern "C"
 
+
+// ---------------------------------------------------------------- streams
+// A stream dedisperses a beam chunk by chunk.  It keeps the last `tail` input
+// samples of the beam on the device (tail = the plan's largest total delay,
+// stage-1 delay plus stage-2 shift, in input samples) and runs each push as the
+// plain call on [tail | chunk], keeping the first chunk/ds output columns: those
+// are the columns whose every delayed sample lies inside the buffer.  Push k's
+// column t is the beam's binned time (samples pushed before push k - tail)/ds + t,
+// so the first tail/ds columns of the beam come from a zero-filled tail.
+struct dd_stream {
+  dd_plan* plan = nullptr;
+  int device = 0;
+  int64_t chunk = 0, tail = 0, buf_len = 0;  // input samples
+  int64_t row_bytes = 0;                     // bytes per input sample (all channels)
+  dd::DevBuf buf[2];
+  int cur = 0;
+  int64_t pushed = 0;
+};
+
+extern "C" {
+
+int dd_stream_open(const dd_header* header, const dd_plan_params* params, const dd_rfi_config* rfi,
+                   const int32_t* bad_channels, int32_t n_bad, int32_t device, dd_stream** out) {
+  if (!out || !header || !params) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  *out = nullptr;
+  dd_stream* S = nullptr;
+  const int rc = guarded([&] {
+    if (params->algorithm != DD_ALGO_SUBBAND)
+      throw Error{DD_ERR_UNSUPPORTED, "streams run the subband algorithm"};
+    const int ds = params->time_downsample;
+    if (ds < 1 || header->ndata < 1 || header->ndata % ds != 0)
+      throw Error{DD_ERR_INVALID, "the chunk length (header ndata) must be a positive multiple "
+                                  "of time_downsample"};
+    DeviceGuard g(device);
+    // the delays set the tail: learn them from a plan over one chunk
+    std::unique_ptr<dd_plan> probe(make_plan(header, params, rfi, bad_channels, n_bad, device, 0));
+    const int64_t tail_bin = static_cast<int64_t>(probe->max_delay) + probe->max_res;
+    probe.reset();
+    S = new dd_stream();
+    S->device = device;
+    S->chunk = header->ndata;
+    S->tail = tail_bin * ds;
+    S->buf_len = S->tail + S->chunk;
+    S->row_bytes = static_cast<int64_t>(header->nchans) * (header->nbits / 8);
+    dd_header h = *header;
+    h.ndata = S->buf_len;
+    S->plan = make_plan(&h, params, rfi, bad_channels, n_bad, device, S->chunk / ds);
+    for (int b = 0; b < 2; ++b) {
+      S->buf[b].alloc(static_cast<size_t>(S->buf_len * S->row_bytes));
+      DD_CUDA_TRY(cudaMemset(S->buf[b].p, 0, S->buf[b].bytes));
+    }
+  });
+  if (rc != DD_OK) {
+    if (S) {
+      DeviceGuard g(device);
+      delete S->plan;
+      delete S;
+    }
+    return rc;
+  }
+  *out = S;
+  return DD_OK;
+}
+
+int dd_stream_push(dd_stream* S, const void* chunk, void* output, void* stream) {
+  if (!S || !chunk || !output) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  return guarded([&] {
+    DeviceGuard g(S->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    char* cur = static_cast<char*>(S->buf[S->cur].p);
+    char* nxt = static_cast<char*>(S->buf[S->cur ^ 1].p);
+    DD_CUDA_TRY(cudaMemcpyAsync(cur + S->tail * S->row_bytes, chunk,
+                                static_cast<size_t>(S->chunk * S->row_bytes),
+                                cudaMemcpyDeviceToDevice, st));
+    run_subband(*S->plan, cur, output, nullptr, nullptr, nullptr, st);
+    // the next buffer starts with this buffer's last `tail` samples
+    if (S->tail)
+      DD_CUDA_TRY(cudaMemcpyAsync(nxt, cur + S->chunk * S->row_bytes,
+                                  static_cast<size_t>(S->tail * S->row_bytes),
+                                  cudaMemcpyDeviceToDevice, st));
+    S->cur ^= 1;
+    S->pushed += S->chunk;
+  });
+}
+
+int dd_stream_get_info(const dd_stream* S, dd_stream_info* info) {
+  if (!S || !info) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  dd_stream_info o{};
+  o.dm_steps = S->plan->dm_steps;
+  o.out_cols = S->plan->nout;
+  o.chunk_samples = S->chunk;
+  o.tail_samples = S->tail;
+  o.pushed_samples = S->pushed;
+  o.workspace_bytes = workspace_of(*S->plan) + static_cast<int64_t>(S->buf[0].bytes + S->buf[1].bytes);
+  o.adds_per_push = S->plan->adds;
+  *info = o;
+  return DD_OK;
+}
+
+int dd_stream_plan(const dd_stream* S, dd_plan** plan) {
+  if (!S || !plan) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  *plan = S->plan;
+  return DD_OK;
+}
+
+int dd_stream_close(dd_stream* S) {
+  if (!S) return DD_OK;
+  return guarded([&] {
+    DeviceGuard g(S->device);
+    delete S->plan;
+    S->plan = nullptr;
+    delete S;
+  });
+}
+
+}  // extern "C"

@@ -68,6 +68,7 @@ struct dd_plan {
   int64_t dm_steps = 0;
   int64_t nin = 0;           // input samples
   int64_t nbin = 0;          // binned samples (subband) / input samples (brute)
+  int64_t nout = 0;          // subband: output columns (nbin, or fewer for a stream's plan)
   float ref_freq = 0.f;
   double tsamp = 0;          // sampling time as the reference path uses it
 

@@ -53,6 +53,34 @@ def _tdtype(bits: int):
     return {8: torch.uint8, 16: torch.uint16, 32: torch.uint32, 64: torch.uint64}[bits]
 
 
+class _FfiArgs:
+    pass
+
+
+def _ffi_args(header, dm_low, dm_high, freq_start, freq_end, dm_step, time_downsample, t_sample,
+              algorithm, subband_width, ndm0, zero_dm_mode, table_mode, freq_mode, freq_table,
+              rfi, bad_channels) -> _FfiArgs:
+    """The C structs of dd_plan_create / dd_stream_open (kept alive by the caller)."""
+    g = (lambda k: header[k]) if isinstance(header, dict) else (lambda k: getattr(header, k))
+    a = _FfiArgs()
+    a.nbits = int(g("nbits"))
+    a.nchans = int(g("nchans"))
+    a.h = _lib.Header(float(g("mjd")) if _has(header, "mjd") else 0.0, float(g("tsamp")),
+                      float(g("fch1")), float(g("foff")), a.nbits, a.nchans, int(g("ndata")))
+    a.freq_table = None if freq_table is None else np.ascontiguousarray(freq_table, np.float64)
+    a.p = _lib.PlanParams(dm_low, dm_high, dm_step, freq_start, freq_end, int(time_downsample),
+                          t_sample, _ALGOS[algorithm], int(subband_width), int(ndm0),
+                          _ZDM[zero_dm_mode], _TABLES[table_mode], _FREQ[freq_mode],
+                          None if a.freq_table is None else a.freq_table.ctypes.data)
+    r = rfi or RfiParams()
+    q = r.iqrm
+    a.r = _lib.RfiConfig(int(r.use_mask), int(r.use_zero_dm), int(r.use_iqrm),
+                         _lib.IqrmConfig(int(q.mode), q.radius_frac, q.nsigma, q.geofactor,
+                                         q.win_sec, q.hop_sec, int(bool(q.include_tail))))
+    a.bad = np.ascontiguousarray(list(bad_channels or []), np.int32)
+    return a
+
+
 class Plan:
     """One dedispersion geometry on one GPU.
 
@@ -70,29 +98,14 @@ class Plan:
                  rfi: Optional[RfiParams] = None, bad_channels: Optional[Sequence[int]] = None,
                  device: int = 0):
         L = _lib.load()
-        g = (lambda k: header[k]) if isinstance(header, dict) else (lambda k: getattr(header, k))
-        self.nbits = int(g("nbits"))
-        self.nchans = int(g("nchans"))
-        self.device = int(device)
-        h = _lib.Header(float(g("mjd")) if _has(header, "mjd") else 0.0, float(g("tsamp")),
-                        float(g("fch1")), float(g("foff")), self.nbits, self.nchans,
-                        int(g("ndata")))
-        self._freq_table = None
-        if freq_table is not None:
-            self._freq_table = np.ascontiguousarray(freq_table, np.float64)
-        p = _lib.PlanParams(dm_low, dm_high, dm_step, freq_start, freq_end, int(time_downsample),
-                            t_sample, _ALGOS[algorithm], int(subband_width), int(ndm0),
-                            _ZDM[zero_dm_mode], _TABLES[table_mode], _FREQ[freq_mode],
-                            None if self._freq_table is None else self._freq_table.ctypes.data)
-        r = rfi or RfiParams()
-        q = r.iqrm
-        rc_ = _lib.RfiConfig(int(r.use_mask), int(r.use_zero_dm), int(r.use_iqrm),
-                             _lib.IqrmConfig(int(q.mode), q.radius_frac, q.nsigma, q.geofactor,
-                                             q.win_sec, q.hop_sec, int(bool(q.include_tail))))
-        bad = np.ascontiguousarray(list(bad_channels or []), np.int32)
+        a = _ffi_args(header, dm_low, dm_high, freq_start, freq_end, dm_step, time_downsample,
+                      t_sample, algorithm, subband_width, ndm0, zero_dm_mode, table_mode,
+                      freq_mode, freq_table, rfi, bad_channels)
+        self.nbits, self.nchans, self.device = a.nbits, a.nchans, int(device)
+        self._keep = a
         self._h = ctypes.c_void_p()
-        _lib.check(L.dd_plan_create(ctypes.byref(h), ctypes.byref(p), ctypes.byref(rc_),
-                                    bad.ctypes.data if bad.size else None, int(bad.size),
+        _lib.check(L.dd_plan_create(ctypes.byref(a.h), ctypes.byref(a.p), ctypes.byref(a.r),
+                                    a.bad.ctypes.data if a.bad.size else None, int(a.bad.size),
                                     self.device, ctypes.byref(self._h)))
         info = _lib.PlanInfo()
         _lib.check(L.dd_plan_get_info(self._h, ctypes.byref(info)))
@@ -238,6 +251,69 @@ class Batch:
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:
             _lib.load().dd_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Stream:
+    """A beam dedispersed chunk by chunk (dd_stream_*): the beam's last `tail`
+    samples stay on the device and every push is the plain subband call on
+    [tail | chunk], returning its first chunk/time_downsample columns.  header
+    describes one chunk (ndata = samples per push)."""
+
+    def __init__(self, header, dm_low: float, dm_high: float, freq_start: float,
+                 freq_end: float, dm_step: float = 1.0, time_downsample: int = 1,
+                 subband_width: int = 32, ndm0: int = 32, zero_dm_mode: str = "callsite",
+                 table_mode: str = "reference", freq_mode: str = "header",
+                 freq_table: Optional[np.ndarray] = None, rfi: Optional[RfiParams] = None,
+                 bad_channels: Optional[Sequence[int]] = None, device: int = 0):
+        L = _lib.load()
+        a = _ffi_args(header, dm_low, dm_high, freq_start, freq_end, dm_step, time_downsample,
+                      0.5, "subband", subband_width, ndm0, zero_dm_mode, table_mode, freq_mode,
+                      freq_table, rfi, bad_channels)
+        self.nbits, self.nchans, self.device = a.nbits, a.nchans, int(device)
+        self._keep = a
+        self._h = ctypes.c_void_p()
+        _lib.check(L.dd_stream_open(ctypes.byref(a.h), ctypes.byref(a.p), ctypes.byref(a.r),
+                                    a.bad.ctypes.data if a.bad.size else None, int(a.bad.size),
+                                    self.device, ctypes.byref(self._h)))
+        self.out_shape = (int(self.info["dm_steps"]), int(self.info["out_cols"]))
+        self.chunk_shape = (int(self.info["chunk_samples"]), self.nchans)
+
+    @property
+    def info(self) -> dict:
+        i = _lib.StreamInfo()
+        _lib.check(_lib.load().dd_stream_get_info(self._h, ctypes.byref(i)))
+        return {n: getattr(i, n) for n, _ in _lib.StreamInfo._fields_}
+
+    def empty_output(self):
+        torch = _torch()
+        return torch.empty(self.out_shape, dtype=_tdtype(64 if self.nbits == 32 else 32),
+                           device=f"cuda:{self.device}")
+
+    def push(self, chunk, out=None, stream=None):
+        """chunk: contiguous CUDA tensor of chunk_shape samples; returns out."""
+        torch = _torch()
+        if not chunk.is_cuda or not chunk.is_contiguous() or chunk.element_size() * 8 != self.nbits:
+            raise ValueError(f"chunk must be a contiguous CUDA tensor of uint{self.nbits}")
+        if chunk.numel() != self.chunk_shape[0] * self.chunk_shape[1]:
+            raise ValueError(f"chunk must hold {self.chunk_shape} samples")
+        if out is None:
+            out = self.empty_output()
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        _lib.check(_lib.load().dd_stream_push(self._h, chunk.data_ptr(), out.data_ptr(),
+                                              ctypes.c_void_p(stream.cuda_stream)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.load().dd_stream_close(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

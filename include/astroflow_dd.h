@@ -288,6 +288,38 @@ int dd_batch_status(dd_batch* batch);
 int dd_batch_get_info(const dd_batch* batch, dd_batch_info* info);
 int dd_batch_destroy(dd_batch* batch);
 
+/* ---- Streams: a beam dedispersed chunk by chunk (no reference counterpart:
+ * the reference treats every call's chunk as standalone and drops the terms
+ * with t + delay >= N, dedispered.cu:444 and 473).  A stream keeps the beam's
+ * last `tail_samples` input samples on the device, tail = the plan's largest
+ * total delay (stage-1 delay plus stage-2 shift) in input samples, and runs each
+ * push as the plain subband call (all RFI stages included) on [tail | chunk],
+ * returning its first chunk/time_downsample output columns, the columns whose
+ * delayed samples all lie in the buffer.  Push k's column t is the beam's
+ * binned time (samples pushed before push k - tail)/time_downsample + t; the
+ * first pushes read a zero-filled tail.  header.ndata is the chunk length (a
+ * multiple of time_downsample); params must select DD_ALGO_SUBBAND.  Pushes of
+ * one stream must be ordered (one CUDA stream, or serialised). */
+typedef struct dd_stream dd_stream;
+typedef struct dd_stream_info {
+  int64_t dm_steps;        /* output rows */
+  int64_t out_cols;        /* output columns per push */
+  int64_t chunk_samples;   /* input samples per push */
+  int64_t tail_samples;    /* input samples kept between pushes */
+  int64_t pushed_samples;  /* input samples pushed so far */
+  int64_t workspace_bytes; /* device memory the stream holds */
+  double adds_per_push;    /* algorithmic integer additions per push */
+} dd_stream_info;
+int dd_stream_open(const dd_header* header, const dd_plan_params* params,
+                   const dd_rfi_config* rfi, const int32_t* bad_channels, int32_t n_bad,
+                   int32_t device, dd_stream** stream_out);
+/* chunk: device [chunk_samples][nchans]; output: device [dm_steps][out_cols]. */
+int dd_stream_push(dd_stream* s, const void* chunk, void* output, void* stream);
+int dd_stream_get_info(const dd_stream* s, dd_stream_info* info);
+/* The plan a stream runs (owned by the stream): its info and tables. */
+int dd_stream_plan(const dd_stream* s, dd_plan** plan);
+int dd_stream_close(dd_stream* s);
+
 /* Last error message of the calling thread ("" if none). */
 const char* dd_last_error(void);
 int dd_abi_version(void);
