@@ -26,7 +26,8 @@ TABLE_REFERENCE, TABLE_FP64 = 0, 1
 FREQ_HEADER, FREQ_FIL = 0, 1
 
 # Every symbol include/astroflow_dd.h declares.
-EXPORTS = ("dd_plan_create", "dd_plan_destroy", "dd_plan_get_info", "dd_plan_get_tables",
+EXPORTS = ("dd_plan_create", "dd_plan_destroy", "dd_plan_destroy_async", "dd_plan_get_info",
+           "dd_plan_get_tables",
            "dd_plan_set_delay_table", "dd_run", "dd_run_ex", "dd_run_host", "dd_run_profiled",
            "dd_measure_int_add_rate", "dd_iqrm_masks_noalloc", "dd_batch_create",
            "dd_batch_run", "dd_batch_status", "dd_batch_get_info", "dd_batch_destroy",
@@ -133,6 +134,7 @@ def load():
     L.dd_batch_status.argtypes = [P]
     L.dd_batch_get_info.argtypes = [P, ctypes.POINTER(BatchInfo)]
     L.dd_batch_destroy.argtypes = [P]
+    L.dd_plan_destroy_async.argtypes = [P, P]
     L.dd_stream_open.argtypes = [ctypes.POINTER(Header), ctypes.POINTER(PlanParams),
                                  ctypes.POINTER(RfiConfig), P, ctypes.c_int32, ctypes.c_int32,
                                  ctypes.POINTER(P)]

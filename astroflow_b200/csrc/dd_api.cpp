@@ -782,10 +782,19 @@ long long& launch_count() {
   return n;
 }
 
+// Device memory comes from the stream-ordered allocator (the device's default
+// pool), allocated on the legacy stream; callers synchronise the legacy stream
+// before other streams use it (plan creation does).  It is released either
+// after a device-wide synchronisation (dd_plan_destroy and every other path), or
+// stream-ordered on a caller's stream without stalling the device
+// (dd_plan_destroy_async sets g_free_stream for the duration of the call).
+thread_local cudaStream_t g_free_stream = nullptr;
+thread_local bool g_free_async = false;
+
 void DevBuf::alloc(size_t n) {
   release();
   if (n == 0) return;
-  cudaError_t e = cudaMalloc(&p, n);
+  cudaError_t e = cudaMallocAsync(&p, n, cudaStreamLegacy);
   if (e != cudaSuccess) {
     p = nullptr;
     cudaGetLastError();
@@ -797,7 +806,14 @@ void DevBuf::alloc(size_t n) {
 }
 
 void DevBuf::release() {
-  if (p) cudaFree(p);
+  if (p) {
+    if (g_free_async) {
+      cudaFreeAsync(p, g_free_stream);
+    } else {
+      cudaDeviceSynchronize();
+      cudaFreeAsync(p, cudaStreamLegacy);
+    }
+  }
   p = nullptr;
   bytes = 0;
 }
@@ -869,7 +885,8 @@ dd_plan* make_plan(const dd_header* header, const dd_plan_params* params, const 
   } else {
     throw Error{DD_ERR_INVALID, "unknown algorithm"};
   }
-  DD_CUDA_TRY(cudaDeviceSynchronize());
+  // plan set-up work ran on the legacy stream; other streams keep running
+  DD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
   return P.release();
 }
 }  // namespace
@@ -890,6 +907,18 @@ int dd_plan_destroy(dd_plan* plan) {
   return guarded([&] {
     DeviceGuard g(plan->device);
     delete plan;
+  });
+}
+
+int dd_plan_destroy_async(dd_plan* plan, void* stream) {
+  if (!plan) return DD_OK;
+  return guarded([&] {
+    DeviceGuard g(plan->device);
+    g_free_stream = static_cast<cudaStream_t>(stream);
+    g_free_async = true;
+    delete plan;
+    g_free_async = false;
+    g_free_stream = nullptr;
   });
 }
 
@@ -1207,6 +1236,7 @@ void build_groups(dd_batch& B, void* const* outputs) {
     B.d_ctrs.alloc(sizeof(int) * std::max(B.nctrs, 1));
     B.d_next.alloc(sizeof(unsigned long long));
   }
+  DD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
 }
 
 // Everything one run launches, on stream s.
@@ -1266,7 +1296,8 @@ int dd_batch_create(dd_plan* const* plans, int32_t nplans, int32_t flags, dd_bat
     DD_CUDA_TRY(cudaEventCreateWithFlags(&B->ev_in, cudaEventDisableTiming));
     DD_CUDA_TRY(cudaEventCreateWithFlags(&B->ev_out, cudaEventDisableTiming));
     B->d_err.alloc(sizeof(int));
-    DD_CUDA_TRY(cudaMemset(B->d_err.p, 0, sizeof(int)));
+    DD_CUDA_TRY(cudaMemsetAsync(B->d_err.p, 0, sizeof(int), cudaStreamLegacy));
+    DD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
   });
   if (rc != DD_OK) {
     delete B;
@@ -1422,8 +1453,9 @@ int dd_stream_open(const dd_header* header, const dd_plan_params* params, const 
     S->plan = make_plan(&h, params, rfi, bad_channels, n_bad, device, S->chunk / ds);
     for (int b = 0; b < 2; ++b) {
       S->buf[b].alloc(static_cast<size_t>(S->buf_len * S->row_bytes));
-      DD_CUDA_TRY(cudaMemset(S->buf[b].p, 0, S->buf[b].bytes));
+      DD_CUDA_TRY(cudaMemsetAsync(S->buf[b].p, 0, S->buf[b].bytes, cudaStreamLegacy));
     }
+    DD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
   });
   if (rc != DD_OK) {
     if (S) {

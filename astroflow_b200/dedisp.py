@@ -185,9 +185,15 @@ class Plan:
         _lib.check(_lib.load().dd_run_host(self._h, x.ctypes.data, out.ctypes.data, h))
         return out
 
-    def close(self) -> None:
+    def close(self, stream=None) -> None:
+        """Release the plan.  With `stream` (the CUDA stream all of the plan's work
+        was issued on) its memory is released stream-ordered, without waiting for
+        the rest of the device."""
         if getattr(self, "_h", None) and self._h.value:
-            _lib.load().dd_plan_destroy(self._h)
+            if stream is None:
+                _lib.load().dd_plan_destroy(self._h)
+            else:
+                _lib.load().dd_plan_destroy_async(self._h, ctypes.c_void_p(stream.cuda_stream))
             self._h = ctypes.c_void_p()
 
     def __del__(self):

@@ -68,6 +68,13 @@ WORKLOADS = {
     # two bands, DM ranges up to 3000, downsampling 1-8), dedispersed as batches
     "batched-64-heterogeneous-subband32": dict(kind="batch", nchunks=64, seed=2024,
                                                subband_width=32, budget_gb=140.0),
+    # 19 beams streaming 0.5 s chunks of 4096 ch u8 in real time (DM 0:1:3000, zero-DM +
+    # IQRM) plus Poisson file requests (2/s, 1024-4096 ch, 5-60 s) under a 150 GB budget;
+    # --steps = seconds of served time
+    "serving-19beams-4096ch-u8-3001dm-files": dict(
+        kind="serve", beams=19, nchans=4096, chunk_s=0.5, tsamp=49.152e-6, dm=(0.0, 3000.0, 1.0),
+        subband_width=64, file_rate=2.0, file_s=(5.0, 60.0), file_nchans=(1024, 2048, 4096),
+        budget_gb=150.0, seed=77),
 }
 DEFAULT_WORKLOAD = "wideband-4096ch-u8-2^20-6001dm-subband64-rfi"
 
@@ -278,6 +285,146 @@ def bench_batch(args, wl, dist, dev):
         print(json.dumps(line))
 
 
+def bench_serve(args, wl, dist, dev):
+    """Serving: beams stream chunks in real time and files arrive as a Poisson
+    process; everything goes through astroflow_b200.serve.Server.  `value` is the
+    DM-trial*samples served per second over the timed window (args.steps seconds
+    after args.warmup seconds of warm-up); latencies are arrival -> DM-time ready
+    (chunks: on the host, files: on the device)."""
+    import torch
+
+    from astroflow_b200.dedisp import IqrmParams, RfiParams, Stream
+    from astroflow_b200.serve import Server
+    from astroflow_b200.synth import ChunkSpec, make_chunk_device
+
+    f32 = np.float32
+    rng = np.random.default_rng(wl["seed"] + dist.rank)
+    nch, tsamp = wl["nchans"], wl["tsamp"]
+    chunk = int(wl["chunk_s"] / tsamp)
+    lo_dm, hi_dm, step_dm = wl["dm"]
+    rfi = RfiParams(use_zero_dm=True, use_iqrm=True,
+                    iqrm=IqrmParams(mode=1, radius_frac=0.00134, nsigma=3.0, win_sec=0.0, hop_sec=0.5))
+
+    def geometry(nchans, n):
+        spec = ChunkSpec(nchans=nchans, nsamp=n, nbits=8, tsamp=tsamp, seed=int(rng.integers(1 << 30)),
+                         rfi_frac=0.05, impulses=2,
+                         pulses=[(float(rng.uniform(100, 2500)), 0.3 * n * tsamp, 1e-3, 12.0)])
+        h = spec.header()
+        for k in ("tsamp", "fch1", "foff"):
+            h[k] = float(f32(h[k]))
+        lo = float(f32(h["fch1"]))
+        hi = float(f32(f32(h["fch1"]) + f32(nchans - 1) * f32(h["foff"])))
+        return spec, h, lo, hi
+
+    # host data: a pool of beam chunks and one long file buffer (pinned)
+    pool = []
+    for k in range(8):
+        spec, h, lo, hi = geometry(nch, chunk)
+        x, _ = make_chunk_device(spec, dev)
+        pool.append(x.cpu().pin_memory())
+    beam_hdr, beam_lo, beam_hi = dict(h, ndata=chunk), lo, hi
+    max_file = int(wl["file_s"][1] / tsamp)
+    spec, _, _, _ = geometry(4096, max_file)
+    filebuf = torch.empty((max_file, 4096), dtype=torch.uint8, pin_memory=True)
+    step_rows = 1 << 18
+    for r0 in range(0, max_file, step_rows):
+        part = ChunkSpec(nchans=4096, nsamp=min(step_rows, max_file - r0), nbits=8, tsamp=tsamp,
+                         seed=wl["seed"] + r0)
+        xp, _ = make_chunk_device(part, dev)
+        filebuf[r0:r0 + xp.shape[0]].copy_(xp)
+        del xp
+    torch.cuda.synchronize(dev)
+
+    def file_request(arrival):
+        nchans = int(rng.choice(wl["file_nchans"]))
+        n = int(rng.uniform(*wl["file_s"]) / tsamp)
+        spec, h, lo, hi = geometry(nchans, n)
+        data = filebuf.view(-1)[:n * nchans].view(n, nchans)
+        kw = dict(dm_low=lo_dm, dm_high=hi_dm, freq_start=lo, freq_end=hi, dm_step=step_dm,
+                  subband_width=wl["subband_width"] if nchans >= 2048 else 32, rfi=rfi)
+        return data, dict(h, ndata=n), kw
+
+    srv = Server(device=dev, hbm_budget_gb=wl["budget_gb"])
+    beams = [srv.open_beam(f"beam{b}", beam_hdr, lo_dm, hi_dm, beam_lo, beam_hi, step_dm,
+                           subband_width=wl["subband_width"], rfi=rfi) for b in range(wl["beams"])]
+    # the plain single call: one chunk of one beam alone on the device
+    solo = Stream(beam_hdr, lo_dm, hi_dm, beam_lo, beam_hi, step_dm,
+                  subband_width=wl["subband_width"], rfi=rfi, device=dev)
+    xs = pool[0].to(f"cuda:{dev}")
+    out = solo.empty_output()
+    host = torch.empty(solo.out_shape, dtype=torch.int32, pin_memory=True)
+    solo_ms = []
+    for _ in range(5):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        xs.copy_(pool[1], non_blocking=True)
+        solo.push(xs, out)
+        host.copy_(out.view(torch.int32), non_blocking=True)
+        torch.cuda.synchronize(dev)
+        solo_ms.append((time.perf_counter() - t0) * 1e3)
+    solo.close()
+
+    period = wl["chunk_s"]
+    phase = [b * period / len(beams) for b in range(len(beams))]
+    t_start = time.monotonic()
+    warm_end = t_start + args.warmup
+    end = warm_end + args.steps
+    next_chunk = [t_start + p for p in phase]
+    kchunk = [0] * len(beams)
+    next_file = t_start + rng.exponential(1.0 / wl["file_rate"])
+    clocks = ClockSampler(dev)
+    clocks.start()
+    files_submitted = 0
+    while True:
+        now = time.monotonic()
+        if now >= end:
+            break
+        for b, beam in enumerate(beams):
+            while next_chunk[b] <= now:
+                srv.submit_chunk(beam, pool[(b + kchunk[b]) % len(pool)], arrival=next_chunk[b])
+                kchunk[b] += 1
+                next_chunk[b] += period
+        while next_file <= now:
+            srv.submit_file(*file_request(next_file), arrival=next_file)
+            files_submitted += 1
+            next_file += rng.exponential(1.0 / wl["file_rate"])
+        srv.step()
+        time.sleep(0.0002)
+    # units served in the window: requests that arrived in it and finished
+    srv.drain(timeout=900)
+    clk = clocks.stop()
+    st = srv.stats(since=warm_end)
+    window = [t for t in srv.finished if warm_end <= t.arrival < end and not t.error]
+    t_last = max(t.done for t in window) if window else end
+    units = sum(t.units for t in window)
+    rate = units / (t_last - warm_end)
+    srv.close()
+    if dist.rank == 0:
+        chunks_lat = st["chunks"]
+        line = {"metric": METRIC, "value": dist.job_rate(units, t_last - warm_end), "unit": UNIT,
+                "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": (t_last - warm_end) * 1e3 / max(1, args.steps),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+                "data": "synthetic (seeded, generated on the GPU, pinned host buffers)",
+                "config": {"workload": args.workload, "beams": wl["beams"], "chunk_samples": chunk,
+                           "dm": wl["dm"], "subband_width": wl["subband_width"],
+                           "file_rate_per_s": wl["file_rate"], "file_seconds": wl["file_s"],
+                           "hbm_budget_gb": wl["budget_gb"], "window_s": args.steps,
+                           "step": "one second of served time",
+                           "l2": "inputs larger than L2", "parallelism": f"replicas x{dist.world}"},
+                "serving": {"chunk_latency": chunks_lat, "file_latency": st["files"],
+                            "files_submitted": files_submitted, "errors": st["errors"][:3],
+                            "plain_chunk_ms": {"p50": float(np.median(solo_ms)), "max": float(max(solo_ms))},
+                            "chunk_deadline_s": period,
+                            "p99_under_deadline": bool(chunks_lat.get("p99_s", 1e9) < period),
+                            "served_rate": rate},
+                "roofline": None, "cpu_baseline": None,
+                "e2e": {"value": rate, "unit": UNIT, "note": "requests from pinned host buffers; "
+                        "chunk results copied back to the host"},
+                "gpu_launches": None, "clocks": clk}
+        print(json.dumps(line))
+
+
 def reference_gpu_arm(args, wl, spec, hdr, config, dist, dev):
     """The reference's own plain GPU call (gpucal::dedisperse_spec from
     src/core/dedispered.cu, built for sm_100a into oracle/_ref with its AF_DEBUG
@@ -442,6 +589,10 @@ def main():
     torch.cuda.set_device(dev)
     if wl.get("kind") == "batch":
         bench_batch(args, wl, dist, dev)
+        dist.close()
+        return
+    if wl.get("kind") == "serve":
+        bench_serve(args, wl, dist, dev)
         dist.close()
         return
     spec = ChunkSpec(nchans=wl["nchans"], nsamp=wl["nsamp"], nbits=wl["nbits"], seed=dist.chunk_seed(1234),

@@ -172,6 +172,12 @@ int dd_plan_create(const dd_header* header, const dd_plan_params* params,
                    const dd_rfi_config* rfi, const int32_t* bad_channels, int32_t n_bad,
                    int32_t device, dd_plan** plan);
 int dd_plan_destroy(dd_plan* plan);
+/* Destroy a plan without a device-wide synchronisation: its device memory is
+ * released stream-ordered on `stream`, so every use of the plan must have been
+ * issued on `stream` (or be complete).  For servers that retire plans while
+ * other requests run (dd_plan_destroy waits for the whole device first, as
+ * cudaFree does). */
+int dd_plan_destroy_async(dd_plan* plan, void* stream);
 int dd_plan_get_info(const dd_plan* plan, dd_plan_info* info);
 
 /* Copy the plan's delay tables to host memory: delay is [delay_rows][delay_cols]
