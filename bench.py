@@ -497,16 +497,18 @@ def roofline_peaks():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+def ncu_traffic(kernel: str, units_launch: float):
+    """DRAM bytes (read + write) of one launch of `kernel` at this workload: the
+    committed ncu capture's bytes per DM-trial*sample times the launch's units
+    (profiles/traffic.txt: kernel, DRAM bytes of the captured launch, its units)."""
     path = os.path.join(ROOT, "profiles", "traffic.txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
         parts = line.split()
-        if len(parts) >= 2 and parts[0] == kernel:
+        if len(parts) >= 3 and parts[0] == kernel:
             try:
-                return float(parts[1])
+                return float(parts[1]) / float(parts[2]) * units_launch
             except ValueError:
                 return None
     return None
@@ -710,7 +712,7 @@ def main():
     roofline = {
         "bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
         "frac": achieved / hbm_peak, "peak_kind": peak_kind,
-        "traffic": ncu_traffic(kname),
+        "traffic": ncu_traffic(kname, units_launch),
         "bytes_per_unit": bytes_per_unit, "units_per_launch": units_launch,
         "avg_launch_ms": avg_launch_s * 1e3,
         "int_add": {"achieved": adds_rate, "peak": add_peak, "unit": "adds/s",
