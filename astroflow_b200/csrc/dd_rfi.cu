@@ -308,6 +308,69 @@ __global__ void k_prep(PrepArgs a) {
   }
 }
 
+// 8-bit samples without downsampling (the subband layout), as k_prep but four
+// channels per load and four samples per store: a block takes 64 samples x 64
+// channels, applies the masks and the zero-DM offset to whole words with
+// byte-wise SIMD operations, and transposes 4x4 byte blocks in registers.
+// Needs nchans % 4 == 0 (aligned word loads); channel words are read from
+// c0 & ~3 and channels outside [c0, c1) are not stored.
+__global__ void __launch_bounds__(256) k_prep_u8(PrepArgs a) {
+  __shared__ uint32_t tile[64][17];  // [sample][channel word], padded
+  const uint8_t* x = static_cast<const uint8_t*>(a.x);
+  const int64_t tb = static_cast<int64_t>(blockIdx.x) * 64;
+  const int64_t cb = (a.c0 & ~int64_t(3)) + static_cast<int64_t>(blockIdx.y) * 64;
+  {
+    const int w = threadIdx.x & 15;  // channel word of the tile
+    const int64_t c = cb + 4 * w;
+    const bool cvalid = c < a.nchans;
+    uint32_t drop = 0, inrange = 0;  // per byte: bad channel / zero-DM applies
+    if (cvalid) {
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int64_t ch = c + b;
+        if (a.keep && !a.keep[ch]) drop |= 0xffu << (8 * b);
+        if (a.zdm_off && ch >= a.zdm_cs && ch < a.zdm_ce) inrange |= 0xffu << (8 * b);
+      }
+    }
+    for (int r = threadIdx.x >> 4; r < 64; r += 16) {
+      const int64_t t = tb + r;
+      uint32_t v = 0;
+      if (cvalid && t < a.nsamp) {
+        v = *reinterpret_cast<const uint32_t*>(x + t * a.nchans + c);
+        if (a.segmask) {
+          const int sg = find_seg(a.seg_t0, a.nseg, t);
+          const uint32_t m = *reinterpret_cast<const uint32_t*>(
+              a.segmask + static_cast<int64_t>(sg) * a.nchans + c);
+          v &= ~__vcmpne4(m, 0u);
+        }
+        if (a.zdm_off) {
+          const uint32_t m = min(a.zdm_off[t], 255u) * 0x01010101u;
+          v = (__vsubus4(v, m) & inrange) | (v & ~inrange);
+        }
+        v &= ~drop;
+      }
+      tile[r][w] = v;
+    }
+  }
+  __syncthreads();
+  if (!a.out) return;
+  const int i = threadIdx.x & 15;  // samples 4i .. 4i+3
+  const int j = threadIdx.x >> 4;  // channel word j: channels 4j .. 4j+3
+  const uint32_t q0 = tile[4 * i][j], q1 = tile[4 * i + 1][j];
+  const uint32_t q2 = tile[4 * i + 2][j], q3 = tile[4 * i + 3][j];
+  const uint32_t lo01 = __byte_perm(q0, q1, 0x5140), hi01 = __byte_perm(q0, q1, 0x7362);
+  const uint32_t lo23 = __byte_perm(q2, q3, 0x5140), hi23 = __byte_perm(q2, q3, 0x7362);
+  const uint32_t o[4] = {__byte_perm(lo01, lo23, 0x5410), __byte_perm(lo01, lo23, 0x7632),
+                         __byte_perm(hi01, hi23, 0x5410), __byte_perm(hi01, hi23, 0x7632)};
+  uint8_t* out = static_cast<uint8_t*>(a.out);
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int64_t cc = cb + 4 * j + b;
+    if (cc >= a.c0 && cc < a.c1)
+      *reinterpret_cast<uint32_t*>(out + (cc - a.c0) * a.pitch + tb + 4 * i) = o[b];
+  }
+}
+
 // Full-layout copy of the prepared input (parity checks only): all channels.
 template <typename T>
 __global__ void k_prep_full(PrepArgs a) {
@@ -417,7 +480,13 @@ void launch_zdm_offsets(const void* x, int nbits, int64_t nsamp, int64_t nchans,
 }
 
 void launch_prep(const PrepArgs& a, cudaStream_t st) {
-  if (a.out) {
+  if (a.out && a.nbits == 8 && a.ds == 1 && a.nchans % 4 == 0 && a.pitch % 4 == 0 &&
+      reinterpret_cast<uintptr_t>(a.x) % 4 == 0 && reinterpret_cast<uintptr_t>(a.out) % 4 == 0) {
+    const int64_t cw0 = a.c0 & ~int64_t(3);
+    dim3 grid(static_cast<unsigned>((a.nsamp + 63) / 64), static_cast<unsigned>((a.c1 - cw0 + 63) / 64));
+    k_prep_u8<<<grid, 256, 0, st>>>(a);
+    DD_LAUNCHED();
+  } else if (a.out) {
     dim3 grid(static_cast<unsigned>((a.nsamp + 63) / 64), static_cast<unsigned>((a.c1 - a.c0 + 63) / 64));
     switch (a.nbits) {
       case 8: k_prep<uint8_t><<<grid, 256, 0, st>>>(a); break;
