@@ -40,7 +40,10 @@ namespace {
 
 constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
-constexpr int kMaxStages = 4;
+#ifndef DD_SUM_MAX_STAGES
+#define DD_SUM_MAX_STAGES 8
+#endif
+constexpr int kMaxStages = DD_SUM_MAX_STAGES;  // staged source pairs in flight, at most
 constexpr long long kWaitCycles = 4000000000LL;
 
 // ------------------------------------------------------------------ mbarrier helpers
