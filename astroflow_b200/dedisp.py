@@ -203,6 +203,56 @@ class Plan:
             pass
 
 
+class MultiPlan:
+    """Several DM ranges over one chunk with one upload: astroflow searches a list
+    of (DM range, time downsampling) entries by one plain call per entry, each
+    re-uploading the chunk (python/astroflow/search.py:519-534, 719-731); here the
+    chunk stays resident and one Plan per range runs on it back to back.  Each
+    range's output equals the plain call for that range.
+
+    ranges: (dm_low, dm_high, dm_step, time_downsample) per entry; the other
+    arguments are shared by every range (see Plan)."""
+
+    def __init__(self, header, ranges, freq_start: float, freq_end: float, **plan_kwargs):
+        if not ranges:
+            raise ValueError("a multi-range plan needs at least one range")
+        self.plans = []
+        try:
+            for lo, hi, step, ds in ranges:
+                self.plans.append(Plan(header, lo, hi, freq_start, freq_end, step, ds,
+                                       **plan_kwargs))
+        except Exception:
+            self.close()
+            raise
+        self.in_shape = self.plans[0].in_shape
+        self.nbits = self.plans[0].nbits
+        self.device = self.plans[0].device
+
+    @property
+    def workspace_bytes(self) -> int:
+        return int(sum(p.info["workspace_bytes"] for p in self.plans))
+
+    @property
+    def output_bytes(self) -> int:
+        return int(sum(p.out_shape[0] * p.out_shape[1] * p.out_bits // 8 for p in self.plans))
+
+    def empty_outputs(self):
+        return [p.empty_output() for p in self.plans]
+
+    def run(self, x, outs=None, stream=None):
+        """x: the resident chunk (device tensor); returns one output per range."""
+        if outs is None:
+            outs = self.empty_outputs()
+        for p, o in zip(self.plans, outs):
+            p.run(x, o, stream)
+        return outs
+
+    def close(self) -> None:
+        for p in self.plans:
+            p.close()
+        self.plans = []
+
+
 class Batch:
     """Many chunks of different geometries in one run (dd_batch_*): each plan's
     RFI/layout kernels, then the dedispersion sums of all plans batched (one

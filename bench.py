@@ -68,6 +68,17 @@ WORKLOADS = {
     # two bands, DM ranges up to 3000, downsampling 1-8), dedispersed as batches
     "batched-64-heterogeneous-subband32": dict(kind="batch", nchunks=64, seed=2024,
                                                subband_width=32, budget_gb=140.0),
+    # 8192 ch u16, 2^21 samples, three DM ranges on one resident chunk (DM 0:0.25:500 ds 1,
+    # 500:0.5:2000 ds 2, 2000:1:5000 ds 4), subband width 64 (128 subbands), IQRM + zero-DM
+    "large-8192ch-u16-2^21-multirange-subband64-rfi": dict(
+        kind="multirange", nchans=8192, nsamp=1 << 21, nbits=16, subband_width=64,
+        ranges=[(0.0, 500.0, 0.25, 1), (500.0, 2000.0, 0.5, 2), (2000.0, 5000.0, 1.0, 4)],
+        rfi=dict(use_zero_dm=True, use_iqrm=True, use_mask=False,
+                 iqrm=dict(mode=1, radius_frac=0.00067, nsigma=3.0, geofactor=1.5, win_sec=0.0,
+                           hop_sec=0.5, include_tail=True)),
+        chunk=dict(rfi_frac=0.08, rfi_amp=6000.0, impulses=20, imp_amp=5000.0,
+                   pulses=[(300.0, 20.0, 1e-3, 1200.0), (1200.0, 50.0, 1e-3, 1200.0),
+                           (3500.0, 70.0, 1e-3, 1200.0)])),
     # 19 beams streaming 0.5 s chunks of 4096 ch u8 in real time (DM 0:1:3000, zero-DM +
     # IQRM) plus Poisson file requests (2/s, 1024-4096 ch, 5-60 s) under a 150 GB budget;
     # --steps = seconds of served time
@@ -283,6 +294,104 @@ def bench_batch(args, wl, dist, dev):
                              "step_frac": roof_s / t},
                 "cpu_baseline": None, "e2e": None, "gpu_launches": launches[best], "clocks": clk}
         print(json.dumps(line))
+
+
+def bench_multirange(args, wl, dist, dev):
+    """One resident chunk searched over several (DM range, downsampling) entries
+    (MultiPlan: one upload, one plan per range).  `value` counts the output
+    DM-trial*samples of all ranges per second; `e2e` adds the chunk's upload and
+    every range's output download (pinned host buffers)."""
+    import torch
+
+    from astroflow_b200.dedisp import IqrmParams, MultiPlan, RfiParams, measure_int_add_rate
+    from astroflow_b200.synth import ChunkSpec, make_chunk_device
+
+    f32 = np.float32
+    spec = ChunkSpec(nchans=wl["nchans"], nsamp=wl["nsamp"], nbits=wl["nbits"],
+                     seed=dist.chunk_seed(4321), **wl["chunk"])
+    hdr = spec.header()
+    for k in ("tsamp", "fch1", "foff"):
+        hdr[k] = float(f32(hdr[k]))
+    lo = float(f32(hdr["fch1"]))
+    hi = float(f32(f32(hdr["fch1"]) + f32(wl["nchans"] - 1) * f32(hdr["foff"])))
+    r = wl["rfi"]
+    rfi = RfiParams(use_mask=r["use_mask"], use_zero_dm=r["use_zero_dm"], use_iqrm=r["use_iqrm"],
+                    iqrm=IqrmParams(**r["iqrm"]))
+    x, _ = make_chunk_device(spec, dev)
+    mp = MultiPlan(hdr, wl["ranges"], lo, hi, subband_width=wl["subband_width"], rfi=rfi,
+                   device=dev)
+    outs = mp.empty_outputs()
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        mp.run(x, outs, stream)
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.3)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        mp.run(x, outs, stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    clk = clocks.stop()
+    ms_rank = e0.elapsed_time(e1) / args.steps
+    units = sum(p.out_shape[0] * p.out_shape[1] for p in mp.plans)
+    value = dist.job_rate(units, ms_rank * 1e-3)
+    ms = dist.max(ms_rank)
+    stages = [p.run_profiled(x, o, stream) for p, o in zip(mp.plans, outs)]
+    adds = sum(p.info["adds_per_run"] for p in mp.plans)
+    in_bytes = wl["nsamp"] * wl["nchans"] * wl["nbits"] // 8
+    out_bytes = mp.output_bytes
+    hbm_peak, peak_kind = roofline_peaks()
+    add_peak = measure_int_add_rate(dev)
+    roof_s = max((in_bytes + out_bytes) / (hbm_peak * 1e9), adds / add_peak)
+    e2e = None
+    if args.e2e_steps > 0:
+        h_in = torch.empty(tuple(x.shape), dtype=x.dtype, pin_memory=True)
+        h_in.copy_(x)
+        h_outs = [torch.empty(tuple(o.shape), dtype=torch.int32, pin_memory=True) for o in outs]
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e2.record(stream)
+        for _ in range(args.e2e_steps):
+            x.copy_(h_in, non_blocking=True)
+            mp.run(x, outs, stream)
+            for o, h in zip(outs, h_outs):
+                h.copy_(o.view(torch.int32), non_blocking=True)
+        e3.record(stream)
+        torch.cuda.synchronize(dev)
+        e2e_ms = e2.elapsed_time(e3) / args.e2e_steps
+        e2e = {"value": dist.job_rate(units, e2e_ms * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": int(in_bytes), "d2h_bytes_per_step": int(out_bytes),
+               "ms_per_step": e2e_ms}
+    if dist.rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": f"u{wl['nbits']}", "data": "synthetic (seeded, generated on the GPU)",
+                "config": {"workload": args.workload, "nchans": wl["nchans"], "nsamp": wl["nsamp"],
+                           "ranges": wl["ranges"], "subband_width": wl["subband_width"],
+                           "rfi": "iqrm + zero-DM (reference call-site semantics)",
+                           "device_gb": round((mp.workspace_bytes + out_bytes + in_bytes) / 1e9, 1),
+                           "l2": "inputs larger than L2", "parallelism": f"replicas x{dist.world}"},
+                "ranges_ms": [{k: round(v, 2) if isinstance(v, float) else v for k, v in st.items()}
+                              for st in stages],
+                "roofline": {"bound": "hbm", "achieved": (in_bytes + out_bytes) / (ms * 1e-3) / 1e9,
+                             "peak": hbm_peak, "unit": "GB/s",
+                             "frac": (in_bytes + out_bytes) / (ms * 1e-3) / 1e9 / hbm_peak,
+                             "peak_kind": peak_kind, "traffic": None,
+                             "int_add": {"achieved": adds / (ms * 1e-3), "peak": add_peak,
+                                         "unit": "adds/s", "frac": adds / (ms * 1e-3) / add_peak},
+                             "step_frac": roof_s / (ms * 1e-3)},
+                "cpu_baseline": None, "e2e": e2e,
+                "gpu_launches": int(sum(st["launches"] for st in stages)) * args.steps,
+                "clocks": clk}
+        print(json.dumps(line))
+    mp.close()
 
 
 def bench_serve(args, wl, dist, dev):
@@ -591,6 +700,10 @@ def main():
     torch.cuda.set_device(dev)
     if wl.get("kind") == "batch":
         bench_batch(args, wl, dist, dev)
+        dist.close()
+        return
+    if wl.get("kind") == "multirange":
+        bench_multirange(args, wl, dist, dev)
         dist.close()
         return
     if wl.get("kind") == "serve":

@@ -271,3 +271,29 @@ def test_time_binning_matches_oracle():
             plan = Plan(hdr, 0.0, 10.0, 1000.0, 1095.0, 1.0, ds, algorithm="subband")
             _, _, _, prepped = run_prepped(plan, x, 96)
             assert np.array_equal(prepped, O.time_binning(x, 96, ds))
+
+
+# ------------------------------------------------------------------ multi-range plans
+def test_multi_range_plan_matches_reference_calls_per_range():
+    """One resident chunk, three (DM range, downsampling) entries as astroflow's
+    dmrange list: each range equals the reference GPU path's plain call."""
+    from astroflow_b200.dedisp import MultiPlan
+    if not O.ref_gpu_available(64):
+        pytest.skip("reference GPU build absent")
+    spec = ChunkSpec(nchans=512, nsamp=12000, nbits=16, seed=8, rfi_frac=0.08, rfi_amp=6000,
+                     impulses=4, imp_amp=5000, pulses=[(300.0, 0.2, 3e-4, 3000.0)])
+    x, _ = make_chunk(spec)
+    tsamp32, fch1_32, foff32 = float(F32(spec.tsamp)), float(F32(spec.fch1)), float(F32(spec.foff))
+    freq = O.freq_table_header(fch1_32, foff32, 512)
+    fs, fe = float(F32(freq[0])), float(F32(freq[-1]))
+    hdr = dict(tsamp=tsamp32, fch1=fch1_32, foff=foff32, nbits=16, nchans=512, ndata=12000)
+    iq = IqrmParams(mode=0, radius_frac=0.05, nsigma=3.0, win_sec=0.0, hop_sec=0.0)
+    ranges = [(0.0, 100.0, 0.25, 1), (100.0, 400.0, 0.5, 2), (400.0, 1000.0, 1.0, 4)]
+    mp = MultiPlan(hdr, ranges, fs, fe, subband_width=64,
+                   rfi=RfiParams(use_zero_dm=True, use_iqrm=True, iqrm=iq))
+    outs = mp.run(dev(x))
+    for (lo, hi, step, ds), o in zip(ranges, outs):
+        ref = O.ref_gpu_dedisperse_spec(x, 512, tsamp32, fch1_32, foff32, lo, hi, fs, fe, step, ds,
+                                        sb_width=64, use_zero_dm=True, use_iqrm=True, iq=iq)
+        assert np.array_equal(to_np(o), ref), f"range {lo}-{hi}"
+    mp.close()
