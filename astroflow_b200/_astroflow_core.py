@@ -459,15 +459,87 @@ def _dedispered_fil(filename, dm_low, dm_high, freq_start, freq_end, dm_step, ti
     return _result(imgs, dm_low, dm_high, dm_step, t_sample, fil.filename)
 
 
-def _unsupported(name):
-    def f(*args, **kwargs):
-        raise NotImplementedError(
-            f"{name}: the single-DM dedispersed spectrum for candidate plots is not part of "
-            "this library yet (include/cpucal.hpp:203-483)")
+_SPECTRA = {8: Spectrum8, 16: Spectrum16, 32: Spectrum32}
+
+
+def _single_dm(a: np.ndarray, hdr: dict, freq_mode: str, freq_table, tstart, tend, dm, freq_start,
+               freq_end, maskfile, rfi: RFIconfig, nbits_out: int) -> _Spectrum:
+    """One dd_single_dm_run on the flat array `a` ([ndata][nchans] samples), the
+    RFI-processed rows written back into `a` as the reference's in-place masking
+    leaves them."""
+    from .dedisp import single_dm_spectrum
+
+    bad = load_mask_file(maskfile)   # RfiMarkerCPU<T> reads it whether or not it is used
+    nchans, ndata = int(hdr["nchans"]), int(hdr["ndata"])
+    if a.size < nchans * ndata:
+        raise ValueError(f"data holds {a.size} samples, the header describes {ndata} x {nchans}")
+    modifies = rfi.use_iqrm or (rfi.use_mask and bool(bad))
+    x = _to_device(a, 0)
+    spec, g, rows = single_dm_spectrum(x, hdr, _f32(tstart), _f32(tend), _f32(dm), _f32(freq_start),
+                                       _f32(freq_end), freq_mode=freq_mode, freq_table=freq_table,
+                                       rfi=rfi.params(), bad_channels=bad, masked_rows=modifies)
+    out = _Spectrum.__new__(_SPECTRA[a.dtype.itemsize * 8])
+    _Spectrum.__init__(out)
+    out.data = _to_host_same(spec)
+    if modifies:
+        flat = a.reshape(-1)[: ndata * nchans].reshape(ndata, nchans)
+        flat[g["rfi_t0"]:g["rfi_t0"] + g["rfi_len"]] = _to_host_same(rows)
+    out.ntimes, out.nchans, out.nbits = int(g["ntimes"]), int(g["nchans"]), int(nbits_out)
+    out.tstart, out.tend, out.dm = _f32(tstart), _f32(g["tend"]), _f32(dm)
+    out.freq_start, out.freq_end = _f32(g["freq_start"]), _f32(g["freq_end"])
+    return out
+
+
+def _to_host_same(t) -> np.ndarray:
+    """A device tensor of uint8/16/32 samples as a numpy array of the same type."""
+    import torch
+
+    view = {torch.uint8: (torch.uint8, np.uint8), torch.uint16: (torch.int16, np.uint16),
+            torch.uint32: (torch.int32, np.uint32)}[t.dtype]
+    return t.view(view[0]).cpu().numpy().view(view[1])
+
+
+def _dedisperse_spec_with_dm(data, header, tstart, dm, tend, freq_start, freq_end, maskfile, rficfg):
+    """cpucal::dedisperse_spec_with_dm<T> (include/cpucal.hpp:341-483) through its
+    binding (src/bindpy/pyapi.cpp:330-351): the spectrum of channels
+    [freq_start, freq_end] over [tstart, tend) seconds, each channel shifted by its
+    delay at `dm`.  The binding names its 4th and 5th parameters dm and tend while
+    the C++ function takes them as tend and dm, so positionally the call is
+    (data, header, tstart, tend, dm, freq_start, freq_end, maskfile, rficfg), which
+    is how astroflow passes them (python/astroflow/dedispered.py:120-122).  Like the
+    reference, IQRM and the mask file zero samples of `data` in place (when `data`
+    is a C-contiguous uint8/16/32 array; otherwise a converted copy is masked)."""
+    tstart_, tend_, dm_ = tstart, dm, tend
+    if not isinstance(header, Header):
+        header = Header(header)
+    a = _as_spec_array(data)
+    hdr = dict(tsamp=header.tsamp, fch1=header.fch1, foff=header.foff, nbits=a.dtype.itemsize * 8,
+               nchans=header.nchans, ndata=header.ndata)
+    return _single_dm(a, hdr, "header", None, tstart_, tend_, dm_, freq_start, freq_end, maskfile,
+                      rficfg if rficfg is not None else RFIconfig(), header.nbits)
+
+
+def _fil_with_dm(bits):
+    def f(fil, tstart, tend, dm, freq_start, freq_end, maskfile, rficfg):
+        a = fil.data if isinstance(fil, Filterbank) else None
+        if a is None:
+            raise RuntimeError("Filterbank holds no data")
+        if a.dtype.itemsize * 8 != bits:
+            # the reference reads the file's samples as the function's type whatever
+            # their width, which runs past the buffer for wider types
+            raise ValueError(f"the Filterbank holds {fil.nbits}-bit samples, not uint{bits}")
+        hdr = dict(tsamp=fil.tsamp, fch1=fil.fch1, foff=fil.foff, nbits=bits, nchans=fil.nchans,
+                   ndata=fil.ndata)
+        return _single_dm(a, hdr, "fil", fil.frequency_table, tstart, tend, dm, freq_start, freq_end,
+                          maskfile, rficfg if rficfg is not None else RFIconfig(), fil.nbits)
+    f.__name__ = f"_dedispered_fil_with_dm_uint{bits}"
+    f.__doc__ = (f"cpucal::dedispered_fil_with_dm<uint{bits}_t> (include/cpucal.hpp:203-339, "
+                 "bound at src/bindpy/bindings.cpp:31-42) on a Filterbank read into memory: the "
+                 "file's frequency table and double tsamp; IQRM and the mask file zero the "
+                 "Filterbank's samples in place as the reference does.")
     return f
 
 
-_dedisperse_spec_with_dm = _unsupported("_dedisperse_spec_with_dm")
-_dedispered_fil_with_dm_uint8 = _unsupported("_dedispered_fil_with_dm_uint8")
-_dedispered_fil_with_dm_uint16 = _unsupported("_dedispered_fil_with_dm_uint16")
-_dedispered_fil_with_dm_uint32 = _unsupported("_dedispered_fil_with_dm_uint32")
+_dedispered_fil_with_dm_uint8 = _fil_with_dm(8)
+_dedispered_fil_with_dm_uint16 = _fil_with_dm(16)
+_dedispered_fil_with_dm_uint32 = _fil_with_dm(32)

@@ -32,7 +32,7 @@ EXPORTS = ("dd_plan_create", "dd_plan_destroy", "dd_plan_destroy_async", "dd_pla
            "dd_measure_int_add_rate", "dd_iqrm_masks_noalloc", "dd_batch_create",
            "dd_batch_run", "dd_batch_status", "dd_batch_get_info", "dd_batch_destroy",
            "dd_stream_open", "dd_stream_push", "dd_stream_get_info", "dd_stream_plan",
-           "dd_stream_close",
+           "dd_stream_close", "dd_single_dm_geometry", "dd_single_dm_run",
            "dd_last_error", "dd_abi_version")
 
 
@@ -85,6 +85,19 @@ class StreamInfo(ctypes.Structure):
                [("adds_per_push", ctypes.c_double)]
 
 
+class SingleDmParams(ctypes.Structure):
+    _fields_ = [("tstart", ctypes.c_float), ("tend", ctypes.c_float), ("dm", ctypes.c_float),
+                ("freq_start", ctypes.c_float), ("freq_end", ctypes.c_float),
+                ("freq_mode", ctypes.c_int32), ("freq_table", ctypes.c_void_p)]
+
+
+class SingleDmInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("t_start", "ntimes", "chan_start", "nchans",
+                                               "rfi_t0", "rfi_len")] + \
+               [("tend", ctypes.c_float), ("freq_start", ctypes.c_float),
+                ("freq_end", ctypes.c_float), ("pad", ctypes.c_int32)]
+
+
 BATCH_GRAPH = 1
 BATCH_PERSISTENT = 2
 
@@ -135,6 +148,10 @@ def load():
     L.dd_batch_get_info.argtypes = [P, ctypes.POINTER(BatchInfo)]
     L.dd_batch_destroy.argtypes = [P]
     L.dd_plan_destroy_async.argtypes = [P, P]
+    L.dd_single_dm_geometry.argtypes = [ctypes.POINTER(Header), ctypes.POINTER(SingleDmParams),
+                                        ctypes.POINTER(SingleDmInfo)]
+    L.dd_single_dm_run.argtypes = [ctypes.POINTER(Header), ctypes.POINTER(SingleDmParams),
+                                   ctypes.POINTER(RfiConfig), P, ctypes.c_int32, P, P, P, P]
     L.dd_stream_open.argtypes = [ctypes.POINTER(Header), ctypes.POINTER(PlanParams),
                                  ctypes.POINTER(RfiConfig), P, ctypes.c_int32, ctypes.c_int32,
                                  ctypes.POINTER(P)]

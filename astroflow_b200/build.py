@@ -37,6 +37,7 @@ UNITS = [
     ("dd_probe.cu", []),
     ("dd_sumsmem.cu", []),
     ("dd_noalloc.cu", []),
+    ("dd_single.cu", ["-Xcompiler", "-fno-fast-math"]),
 ]
 HOST = ["dd_api.cpp"]
 HEADERS = ["dd_internal.h", os.path.join("..", "..", "include", "astroflow_dd.h")]

@@ -379,6 +379,41 @@ class Stream:
             pass
 
 
+def single_dm_spectrum(x, header, tstart: float, tend: float, dm: float, freq_start: float,
+                       freq_end: float, freq_mode: str = "header",
+                       freq_table: Optional[np.ndarray] = None, rfi: Optional[RfiParams] = None,
+                       bad_channels: Optional[Sequence[int]] = None, masked_rows: bool = False,
+                       stream=None):
+    """Dedispersed spectrum at one DM over [tstart, tend) (dd_single_dm_run): the
+    selected channels, each shifted by its delay.  x: device tensor [ndata, nchans].
+    Returns (spectrum [ntimes, nsel] device tensor, geometry dict, the RFI-processed
+    rows [rfi_len, nchans] or None)."""
+    torch = _torch()
+    L = _lib.load()
+    a = _ffi_args(header, 0.0, 1.0, freq_start, freq_end, 1.0, 1, 0.5, "subband", 32, 32,
+                  "callsite", "reference", freq_mode, freq_table, rfi, bad_channels)
+    q = _lib.SingleDmParams(tstart, tend, dm, freq_start, freq_end, _FREQ[freq_mode],
+                            None if a.freq_table is None else a.freq_table.ctypes.data)
+    info = _lib.SingleDmInfo()
+    _lib.check(L.dd_single_dm_geometry(ctypes.byref(a.h), ctypes.byref(q), ctypes.byref(info)))
+    g = {n: getattr(info, n) for n, _ in _lib.SingleDmInfo._fields_}
+    if not x.is_cuda or not x.is_contiguous() or x.element_size() * 8 != a.nbits:
+        raise ValueError(f"x must be a contiguous CUDA tensor of uint{a.nbits}")
+    if x.numel() < int(a.h.ndata) * a.nchans:
+        raise ValueError("x holds fewer than ndata * nchans samples")
+    dt = _tdtype(a.nbits)
+    out = torch.empty((g["ntimes"], g["nchans"]), dtype=dt, device=x.device)
+    rows = torch.empty((g["rfi_len"], a.nchans), dtype=dt, device=x.device) if masked_rows else None
+    if stream is None:
+        stream = torch.cuda.current_stream(x.device)
+    _lib.check(L.dd_single_dm_run(ctypes.byref(a.h), ctypes.byref(q), ctypes.byref(a.r),
+                                  a.bad.ctypes.data if a.bad.size else None, int(a.bad.size),
+                                  x.data_ptr(), out.data_ptr(),
+                                  None if rows is None else rows.data_ptr(),
+                                  ctypes.c_void_p(stream.cuda_stream)))
+    return out, g, rows
+
+
 def iqrm_masks_noalloc(x, nchans: int, chan_start: int, chan_end: int, tsamp: float,
                        iqrm: IqrmParams, masks, bounds, stream=None) -> int:
     """IQRM window masks through dd_iqrm_masks_noalloc: no device memory is

@@ -253,6 +253,45 @@ int dd_iqrm_masks_noalloc(const void* input, int32_t nbits, int64_t nsamp, int32
                           const dd_iqrm_config* cfg, uint8_t* masks, uint32_t* bounds,
                           int32_t max_windows, int32_t* n_windows, void* stream);
 
+/* ---- Single-DM dedispersed spectrum of a time window (candidate plots):
+ * cpucal::dedisperse_spec_with_dm (include/cpucal.hpp:341-483) with
+ * freq_mode DD_FREQ_HEADER, cpucal::dedispered_fil_with_dm (cpucal.hpp:203-339)
+ * with DD_FREQ_FIL.  Channels [chan_start, chan_start + nchans) selected by the
+ * reference's linear frequency map; out[t][c] = x[t_start + t + delay(c)][chan_start + c],
+ * delay(c) = lround(4148.808*dm*(1/f_c^2 - 1/f_high^2)/tsamp) in float.  IQRM and
+ * the mask file (rfi->use_iqrm, rfi->use_mask) run first on the rows
+ * [rfi_t0, rfi_t0 + rfi_len) as the reference does; the reference zeroes those
+ * rows of the caller's array, here they are left untouched and, when
+ * masked_rows is not NULL, written there instead ([rfi_len][nchans]). */
+typedef struct dd_single_dm_params {
+  float tstart;              /* seconds from the chunk's first sample */
+  float tend;
+  float dm;
+  float freq_start;          /* MHz */
+  float freq_end;
+  int32_t freq_mode;         /* dd_freq_mode: Header (float) or Filterbank (double) arithmetic */
+  const double* freq_table;  /* DD_FREQ_FIL: the file's channel frequencies, or NULL */
+} dd_single_dm_params;
+typedef struct dd_single_dm_info {
+  int64_t t_start;           /* input sample of output row 0 */
+  int64_t ntimes;            /* output rows */
+  int64_t chan_start;        /* first selected channel */
+  int64_t nchans;            /* selected channels = output columns */
+  int64_t rfi_t0;            /* first input row of the RFI slice */
+  int64_t rfi_len;           /* rows of the RFI slice */
+  float tend;                /* tstart + ntimes * tsamp */
+  float freq_start;          /* lowest selected frequency */
+  float freq_end;            /* highest selected frequency */
+  int32_t pad;
+} dd_single_dm_info;
+/* Host-only: validate and report the output geometry. */
+int dd_single_dm_geometry(const dd_header* header, const dd_single_dm_params* params,
+                          dd_single_dm_info* info);
+/* input: device [ndata][nchans]; output: device [ntimes][nchans (selected)]. */
+int dd_single_dm_run(const dd_header* header, const dd_single_dm_params* params,
+                     const dd_rfi_config* rfi, const int32_t* bad_channels, int32_t n_bad,
+                     const void* input, void* output, void* masked_rows, void* stream);
+
 /* ---- Batches: many chunks of different geometries dedispersed together.
  * The reference dedisperses one chunk per call (gpucal::dedisperse_spec,
  * src/core/dedispered.cu:988-1304).  A batch runs one chunk through each of its

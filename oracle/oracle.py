@@ -280,6 +280,150 @@ def mark_channels(data: np.ndarray, nchans, bad):
                             _ptr(bad), len(bad))
 
 
+# ---------------------------------------------------------------- single-DM spectrum
+@dataclass
+class SingleDmGeometry:
+    t_start: int
+    ntimes: int
+    chan_start: int
+    nchans: int
+    rfi_t0: int
+    rfi_len: int
+    tend: float
+    freq_start: float
+    freq_end: float
+    delay: np.ndarray          # per selected channel, samples
+
+
+def _lround(x: float) -> int:
+    """C lround: nearest integer, halves away from zero."""
+    a = abs(float(x))
+    r = np.floor(a)
+    r = r + 1.0 if a - r >= 0.5 else r
+    return int(r if x >= 0 else -r)
+
+
+def _fma_f32(a, b, c) -> np.float32:
+    """fmaf(a, b, c): a*b + c rounded once to float (the reference build's -ffast-math
+    contracts a*b + c into an FMA)."""
+    from fractions import Fraction
+    v = Fraction(float(a)) * Fraction(float(b)) + Fraction(float(c))
+    f = np.float32(float(v))
+    best = None
+    for cand in (np.nextafter(f, np.float32(-np.inf)), f, np.nextafter(f, np.float32(np.inf))):
+        err = abs(Fraction(float(cand)) - v)
+        key = (err, int(np.array(cand).view(np.uint32)) & 1)   # ties to even
+        if best is None or key < best[0]:
+            best = (key, cand)
+    return np.float32(best[1])
+
+
+def _fma_f64(a, b, c) -> float:
+    """fma(a, b, c) in double, rounded once."""
+    from fractions import Fraction
+    return float(Fraction(float(a)) * Fraction(float(b)) + Fraction(float(c)))
+
+
+def single_dm_geometry(nchans, ndata, tsamp, fch1, foff, tstart, tend, dm, freq_start, freq_end,
+                       fil=False, freq_table=None) -> SingleDmGeometry:
+    """Window, channel selection and delays of cpucal::dedisperse_spec_with_dm
+    (include/cpucal.hpp:341-427; fil=False: float tsamp/fch1/foff of a Header) and
+    cpucal::dedispered_fil_with_dm (cpucal.hpp:203-286; fil=True: the file's double
+    frequency table and double tsamp), in IEEE arithmetic with the two products
+    followed by a sum that the reference build (-ffast-math -mfma) contracts into
+    FMAs: the Header frequency table fch1 + i*foff (cpucal.hpp:374-376) and
+    tend = tstart + t_len*tsamp (cpucal.hpp:459, 306).  Raises ValueError with the
+    reference's message where the reference throws."""
+    F = np.float32
+    tstart, tend, dm, fs, fe = F(tstart), F(tend), F(dm), F(freq_start), F(freq_end)
+    if not tend > tstart:
+        raise ValueError("tend must be > tstart")
+    if fil:
+        tbl = (np.asarray(freq_table, np.float64) if freq_table is not None
+               else fch1 + np.arange(nchans, dtype=np.float64) * foff)
+        freq = tbl.astype(np.float32)
+        t0, t1 = int(float(tstart) / tsamp), int(float(tend) / tsamp)
+    else:
+        tsamp = F(tsamp)
+        freq = np.array([_fma_f32(F(i), F(foff), F(fch1)) for i in range(nchans)], np.float32)
+        t0, t1 = int(tstart / tsamp), int(tend / tsamp)
+    t_len_req = t1 - t0 if t1 > t0 else 0
+    if t_len_req == 0 or t0 >= ndata:
+        raise ValueError("Invalid time window for this file.")
+    if not fil:
+        if fs >= fe:
+            raise ValueError("freq_end must be > freq_start")
+        if dm < 0:
+            raise ValueError("dm must be >= 0")
+        if F(foff) < 0:
+            raise ValueError("frequency channels are in descending order, which is not supported yet.")
+    f0, fN = freq[0], freq[-1]
+    fmin, fmax = min(f0, fN), max(f0, fN)
+    if fs < fmin or fe > fmax or fe <= fs:
+        raise ValueError("Frequency range out of file range")
+
+    def index(f):
+        raw = float(F(f - f0)) / float(F(fN - f0)) * float(nchans - 1)
+        raw = min(max(raw, 0.0), float(nchans - 1))
+        return int(np.floor(raw + 1e-9))
+
+    cs, ce_incl = index(fs), index(fe)
+    if ce_incl < cs:
+        cs, ce_incl = ce_incl, cs
+    ce = min(ce_incl + 1, nchans)
+    nsel = ce - cs if ce > cs else 0
+    if nsel == 0:
+        raise ValueError("Empty channel selection.")
+    f_high = max(freq[cs], freq[ce - 1])
+    delay = np.zeros(nsel, np.int64)
+    for c in range(cs, ce):
+        d = F(F(F(4148.808) * dm) * F(F(1) / F(freq[c] * freq[c]) - F(1) / F(f_high * f_high)))
+        delay[c - cs] = _lround(float(d) / tsamp) if fil else _lround(F(d / tsamp))
+    if delay.min() < 0:
+        raise ValueError("dm must be >= 0")
+    dmax = int(delay.max())
+    cap = ndata - t0 if ndata > t0 else 0
+    t_len = min(t_len_req, cap - dmax) if cap > dmax else 0
+    if t_len == 0:
+        raise ValueError("Time window too short for this DM and band.")
+    rfi_t0 = t0 - dmax if t0 > dmax else 0
+    rfi_len = min(t_len + (t0 - rfi_t0) + 2 * dmax, ndata - rfi_t0)
+    if fil:
+        t_end = float(F(_fma_f64(F(t_len), tsamp, tstart)))
+    else:
+        t_end = float(_fma_f32(F(t_len), tsamp, tstart))
+    return SingleDmGeometry(t0, t_len, cs, nsel, rfi_t0, rfi_len, t_end,
+                            float(min(freq[cs], freq[ce - 1])), float(max(freq[cs], freq[ce - 1])),
+                            delay)
+
+
+def single_dm_spectrum(data: np.ndarray, nchans: int, g: SingleDmGeometry) -> np.ndarray:
+    """The gather of cpucal.hpp:318-336 / 462-480: out[t][c] =
+    data[t_start + t + delay[c]][chan_start + c]."""
+    x = data.reshape(-1)[: (data.size // nchans) * nchans].reshape(-1, nchans)
+    rows = g.t_start + np.arange(g.ntimes)[:, None] + g.delay[None, :]
+    cols = g.chan_start + np.arange(g.nchans)[None, :]
+    return x[rows, cols]
+
+
+def single_dm_with_rfi(data: np.ndarray, nchans: int, g: SingleDmGeometry, tsamp: float,
+                       use_mask=False, bad=(), iq=None):
+    """The whole call on a copy of `data`: IQRM window masks over the RFI slice
+    [rfi_t0, rfi_t0 + rfi_len) for the selected channels (cpucal.hpp:440-448,
+    tsamp as the call passes it), then the mask file's channels zeroed on the same
+    slice (:449-451), then the gather.  Returns (spectrum, the array after the call)."""
+    x = np.ascontiguousarray(data).copy()
+    flat = x.reshape(-1)[: (x.size // nchans) * nchans].reshape(-1, nchans)
+    sl = flat[g.rfi_t0:g.rfi_t0 + g.rfi_len].copy()
+    if iq is not None:
+        t0, t1, masks = iqrm_masks(sl, nchans, g.chan_start, g.chan_start + g.nchans, tsamp, iq)
+        apply_window_masks(sl, nchans, t0, t1, masks)
+    if use_mask and len(bad):
+        mark_channels(sl, nchans, list(bad))
+    flat[g.rfi_t0:g.rfi_t0 + g.rfi_len] = sl
+    return single_dm_spectrum(x, nchans, g), x
+
+
 # ---------------------------------------------------------------- reference builds
 _ref_cpu = None
 
@@ -504,6 +648,55 @@ def ref_gpu_dedispered_fil(filename, dm_low, dm_high, freq_start, freq_end, dm_s
     if rc:
         raise ValueError(f"reference GPU call failed: {err.value.decode()}")
     return out[:rows.value * cols.value].reshape(rows.value, cols.value)
+
+
+def ref_gpu_spec_with_dm(data, nchans, tsamp, fch1, foff, tstart, tend, dm, freq_start, freq_end,
+                         mask_file="", use_mask=False, use_iqrm=False, iq=None, sb_width=32):
+    """The reference's cpucal::dedisperse_spec_with_dm on a copy of `data`; returns
+    (spectrum [ntimes, nsel], (tstart, tend, freq_start, freq_end), the copy after the
+    call (the reference zeroes the RFI-masked samples of its input in place))."""
+    data = np.ascontiguousarray(data).copy()
+    nbits = data.dtype.itemsize * 8
+    L = ref_gpu(sb_width)
+    L.ref_gpu_spec_with_dm.restype = _c_int
+    L.ref_gpu_spec_with_dm.argtypes = [_c_int, _P, _c_float, _c_float, _c_float, _c_int, _c_long,
+                                       _c_float, _c_float, _c_float, _c_float, _c_float,
+                                       ctypes.c_char_p, _P, _P, _c_long, _P, _P, _P,
+                                       ctypes.c_char_p, _c_int]
+    r = _tap_rfi(use_mask, False, use_iqrm, iq)
+    cap = data.size
+    raw = np.zeros(cap, data.dtype)
+    nt, ns = _c_long(), _c_long()
+    meta = np.zeros(4, np.float32)
+    err = ctypes.create_string_buffer(512)
+    rc = L.ref_gpu_spec_with_dm(nbits, _ptr(data), tsamp, fch1, foff, nchans, data.size // nchans,
+                                tstart, tend, dm, freq_start, freq_end, mask_file.encode(),
+                                ctypes.byref(r), _ptr(raw), cap, ctypes.byref(nt), ctypes.byref(ns),
+                                _ptr(meta), err, 512)
+    if rc:
+        raise ValueError(err.value.decode())
+    return raw[:nt.value * ns.value].reshape(nt.value, ns.value), tuple(meta), data
+
+
+def ref_gpu_fil_with_dm(filename, nbits, tstart, tend, dm, freq_start, freq_end, mask_file="",
+                        use_mask=False, use_iqrm=False, iq=None, cap=1 << 26, sb_width=32):
+    """The reference's Filterbank + cpucal::dedispered_fil_with_dm."""
+    L = ref_gpu(sb_width)
+    L.ref_gpu_fil_with_dm.restype = _c_int
+    L.ref_gpu_fil_with_dm.argtypes = [ctypes.c_char_p, _c_float, _c_float, _c_float, _c_float,
+                                      _c_float, ctypes.c_char_p, _P, _P, _c_long, _P, _P, _P,
+                                      ctypes.c_char_p, _c_int]
+    r = _tap_rfi(use_mask, False, use_iqrm, iq)
+    raw = np.zeros(cap, {8: np.uint8, 16: np.uint16, 32: np.uint32}[nbits])
+    nt, ns = _c_long(), _c_long()
+    meta = np.zeros(4, np.float32)
+    err = ctypes.create_string_buffer(512)
+    rc = L.ref_gpu_fil_with_dm(str(filename).encode(), tstart, tend, dm, freq_start, freq_end,
+                               mask_file.encode(), ctypes.byref(r), _ptr(raw), cap, ctypes.byref(nt),
+                               ctypes.byref(ns), _ptr(meta), err, 512)
+    if rc:
+        raise ValueError(err.value.decode())
+    return raw[:nt.value * ns.value].reshape(nt.value, ns.value), tuple(meta)
 
 
 def ref_gpu_tables(nchans, ndata, tsamp, fch1, foff, dm_low, dm_high, freq_start, freq_end,

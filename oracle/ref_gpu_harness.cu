@@ -325,3 +325,78 @@ extern "C" int ref_gpu_dedispered_fil(const char* filename, float dm_low, float 
   *cols = static_cast<long>(cap.cols);
   return 0;
 }
+
+// ---- single-DM spectra: cpucal::dedisperse_spec_with_dm (include/cpucal.hpp:341-483)
+// and cpucal::dedispered_fil_with_dm (:203-339).  Both zero the RFI-masked samples of
+// their input in place, so `data` (a copy owned by the caller) shows that mutation.
+#include "cpucal.hpp"
+
+namespace {
+template <typename T>
+int copy_spectrum(const Spectrum<T>& s, void* out, long out_cap, long* ntimes, long* nsel,
+                  float* meta, char* err, int errlen) {
+  if (static_cast<long>(s.ntimes * s.nchans) > out_cap) {
+    std::snprintf(err, errlen, "output capacity too small");
+    return 3;
+  }
+  std::memcpy(out, s.data.get(), s.ntimes * s.nchans * sizeof(T));
+  *ntimes = static_cast<long>(s.ntimes);
+  *nsel = static_cast<long>(s.nchans);
+  meta[0] = s.tstart;
+  meta[1] = s.tend;
+  meta[2] = s.freq_start;
+  meta[3] = s.freq_end;
+  return 0;
+}
+
+template <typename T>
+int spec_with_dm(void* data, const Header& hdr, float tstart, float tend, float dm, float fs,
+                 float fe, const char* mask_file, const TapRfi* r, void* out, long out_cap,
+                 long* ntimes, long* nsel, float* meta, char* err, int errlen) {
+  try {
+    Spectrum<T> s = cpucal::dedisperse_spec_with_dm<T>(static_cast<T*>(data), hdr, dm, tstart,
+                                                       tend, fs, fe, std::string(mask_file),
+                                                       make_rfi(r));
+    return copy_spectrum(s, out, out_cap, ntimes, nsel, meta, err, errlen);
+  } catch (const std::exception& e) {
+    std::snprintf(err, errlen, "%s", e.what());
+    return 2;
+  }
+}
+}  // namespace
+
+extern "C" int ref_gpu_spec_with_dm(int nbits, void* data, float tsamp, float fch1, float foff,
+                                    int nchans, long ndata, float tstart, float tend, float dm,
+                                    float fs, float fe, const char* mask_file, const void* rfi,
+                                    void* out, long out_cap, long* ntimes, long* nsel,
+                                    float* meta, char* err, int errlen) {
+  Header hdr(0.0f, tsamp, fch1, foff, nbits, nchans, ndata, "tap");
+  const TapRfi* r = static_cast<const TapRfi*>(rfi);
+  switch (nbits) {
+    case 8: return spec_with_dm<uint8_t>(data, hdr, tstart, tend, dm, fs, fe, mask_file, r, out, out_cap, ntimes, nsel, meta, err, errlen);
+    case 16: return spec_with_dm<uint16_t>(data, hdr, tstart, tend, dm, fs, fe, mask_file, r, out, out_cap, ntimes, nsel, meta, err, errlen);
+    case 32: return spec_with_dm<uint32_t>(data, hdr, tstart, tend, dm, fs, fe, mask_file, r, out, out_cap, ntimes, nsel, meta, err, errlen);
+  }
+  std::snprintf(err, errlen, "unsupported nbits");
+  return 5;
+}
+
+extern "C" int ref_gpu_fil_with_dm(const char* filename, float tstart, float tend, float dm,
+                                   float fs, float fe, const char* mask_file, const void* rfi,
+                                   void* out, long out_cap, long* ntimes, long* nsel, float* meta,
+                                   char* err, int errlen) {
+  const TapRfi* r = static_cast<const TapRfi*>(rfi);
+  try {
+    Filterbank fil{std::string(filename)};
+    switch (fil.nbits) {
+      case 8: return copy_spectrum(cpucal::dedispered_fil_with_dm<uint8_t>(&fil, tstart, tend, dm, fs, fe, std::string(mask_file), make_rfi(r)), out, out_cap, ntimes, nsel, meta, err, errlen);
+      case 16: return copy_spectrum(cpucal::dedispered_fil_with_dm<uint16_t>(&fil, tstart, tend, dm, fs, fe, std::string(mask_file), make_rfi(r)), out, out_cap, ntimes, nsel, meta, err, errlen);
+      case 32: return copy_spectrum(cpucal::dedispered_fil_with_dm<uint32_t>(&fil, tstart, tend, dm, fs, fe, std::string(mask_file), make_rfi(r)), out, out_cap, ntimes, nsel, meta, err, errlen);
+    }
+  } catch (const std::exception& e) {
+    std::snprintf(err, errlen, "%s", e.what());
+    return 2;
+  }
+  std::snprintf(err, errlen, "unsupported nbits");
+  return 5;
+}

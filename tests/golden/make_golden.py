@@ -2,6 +2,8 @@
 
   python tests/golden/make_golden.py cpu   # reference CPU brute force (any x86-64 host)
   python tests/golden/make_golden.py gpu   # reference GPU path (needs a B200)
+  python tests/golden/make_golden.py single        # single-DM spectra (any x86-64 host)
+  python tests/golden/make_golden.py single_iqrm   # single-DM spectra with IQRM (needs a B200)
 
 Both need the reference builds under oracle/_ref/ (made by `make -C oracle ref`
 from the reference sources).  Each fixture is a compressed .npz holding the
@@ -14,7 +16,10 @@ seeded input, the call's parameters and what the reference returned:
                   the RFI stages off: coarse delays, residuals and the raw sums;
   ref_gpu_rfi_*   the RFI stages of the same call (binning, IQRM window masks,
                   zero-DM, mask file; dedispered.cu:1057-1122): window bounds,
-                  masks and the processed input.
+                  masks and the processed input;
+  ref_single_*    cpucal::dedisperse_spec_with_dm / dedispered_fil_with_dm
+                  (include/cpucal.hpp:203-483): the spectrum, its tstart/tend/band,
+                  and for Header input the samples of the caller's array it zeroed.
 
 The CPU tests check the oracle against these files, so the oracle stays pinned
 to the reference where the reference tree and a GPU are absent.
@@ -140,13 +145,83 @@ def make_gpu(out_dir):
         print(path, os.path.getsize(path))
 
 
+SINGLE_CASES = [
+    # name, fil, nbits, nchans, N, tsamp, fch1, foff, tstart, tend, dm, band fractions,
+    # mask, IQRM (mode, radius_frac, nsigma, win_sec, hop_sec) or None
+    ("hdr_u8", False, 8, 32, 1500, 64e-6, 1200.0, 9.375, 0.02, 0.07, 30.0, (0.1, 0.9), False, None),
+    ("hdr_u16_mask", False, 16, 24, 1500, 1e-4, 1100.0, 6.0, 0.02, 0.09, 25.0, (0.0, 1.0), True,
+     None),
+    ("fil_u32", True, 32, 16, 1000, 49.152e-6, 1300.0, 8.5, 0.01, 0.035, 20.0, (0.2, 0.8), False,
+     None),
+    ("fil_u8_desc_mask", True, 8, 40, 1500, 64e-6, 1500.0, -7.0, 0.0, 0.06, 40.0, (0.0, 1.0), True,
+     None),
+    ("hdr_u8_iqrm", False, 8, 64, 2500, 64e-6, 1200.0, 4.6875, 0.03, 0.1, 40.0, (0.0, 1.0), True,
+     (0, 0.1, 3.0, 0.03, 0.02)),
+    ("fil_u16_iqrm", True, 16, 48, 2000, 1e-4, 1150.0, 6.25, 0.02, 0.12, 50.0, (0.1, 0.95), False,
+     (1, 0.08, 2.5, 0.0, 0.0)),
+]
+
+
+def make_single(out_dir, iqrm):
+    """cpucal::dedisperse_spec_with_dm / dedispered_fil_with_dm (include/cpucal.hpp:203-483).
+    The IQRM cases run the reference's GPU IQRM and need a B200 (iqrm=True)."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    from sigproc_writer import write_fil
+    if not O.ref_gpu_available(32):
+        raise SystemExit("oracle/_ref/libref_gpu_sb32.so missing")
+    for k, (name, fil, nbits, nchans, n, tsamp, fch1, foff, ts, te, dm, band, use_mask,
+            iqp) in enumerate(SINGLE_CASES):
+        if (iqp is not None) != iqrm:
+            continue
+        rng = np.random.default_rng(400 + k)
+        if nbits == 32:
+            x = rng.integers(0, 1 << 20, size=(n, nchans)).astype(np.uint32)
+        else:
+            x = _data(rng, n, nchans, nbits)
+        lo_f, hi_f = (fch1, fch1 + (nchans - 1) * foff) if foff > 0 else \
+            (fch1 + (nchans - 1) * foff, fch1)
+        fs = float(F32(lo_f + band[0] * (hi_f - lo_f)))
+        fe = float(F32(lo_f + band[1] * (hi_f - lo_f)))
+        bad = sorted(int(c) for c in rng.choice(nchans, size=4, replace=False))
+        iq = _Iq(*iqp) if iqp is not None else None
+        with tempfile.TemporaryDirectory() as td:
+            mask_file = os.path.join(td, "mask.txt")
+            with open(mask_file, "w") as fh:
+                fh.write(" ".join(map(str, bad)) + "\n")
+            if fil:
+                path = os.path.join(td, "a.fil")
+                write_fil(path, x, tsamp, fch1, foff)
+                spec, meta = O.ref_gpu_fil_with_dm(path, nbits, ts, te, dm, fs, fe, mask_file,
+                                                   use_mask=use_mask, use_iqrm=iqp is not None,
+                                                   iq=iq)
+                after = None
+            else:
+                tsamp, fch1, foff = float(F32(tsamp)), float(F32(fch1)), float(F32(foff))
+                spec, meta, after = O.ref_gpu_spec_with_dm(x, nchans, tsamp, fch1, foff, ts, te, dm,
+                                                           fs, fe, mask_file, use_mask=use_mask,
+                                                           use_iqrm=iqp is not None, iq=iq)
+        path = os.path.join(out_dir, f"ref_single_{name}.npz")
+        # the caller's array after the call, as the flat indices the reference zeroed
+        extra = {} if after is None else {
+            "zeroed": np.flatnonzero(after.reshape(-1) != x.reshape(-1)).astype(np.int32)}
+        np.savez_compressed(path, data=x, fil=fil, nchans=nchans, tsamp=tsamp, fch1=fch1, foff=foff,
+                            tstart=ts, tend=te, dm=dm, freq_start=fs, freq_end=fe,
+                            use_mask=use_mask, bad=np.array(bad, np.int32),
+                            iq=np.array(iqp if iqp is not None else (), np.float64),
+                            spec=spec, meta=np.array(meta, np.float32), **extra)
+        print(path, os.path.getsize(path))
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("which", choices=["cpu", "gpu"])
+    ap.add_argument("which", choices=["cpu", "gpu", "single", "single_iqrm"])
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
-    (make_cpu if a.which == "cpu" else make_gpu)(a.out)
+    if a.which.startswith("single"):
+        make_single(a.out, a.which == "single_iqrm")
+    else:
+        (make_cpu if a.which == "cpu" else make_gpu)(a.out)
 
 
 if __name__ == "__main__":

@@ -53,7 +53,8 @@ def test_struct_layouts_match_c():
         "dd_header": _lib.Header, "dd_iqrm_config": _lib.IqrmConfig, "dd_rfi_config": _lib.RfiConfig,
         "dd_plan_params": _lib.PlanParams, "dd_plan_info": _lib.PlanInfo,
         "dd_run_stats": _lib.RunStats, "dd_batch_info": _lib.BatchInfo,
-        "dd_stream_info": _lib.StreamInfo,
+        "dd_stream_info": _lib.StreamInfo, "dd_single_dm_params": _lib.SingleDmParams,
+        "dd_single_dm_info": _lib.SingleDmInfo,
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for cname, py in structs.items():

@@ -149,6 +149,12 @@ def test_dedisperse_spec_arguments_are_positional_like_the_reference():
     names = list(inspect.signature(C._dedispered_fil).parameters)
     assert names == ["filename", "dm_low", "dm_high", "freq_start", "freq_end", "dm_step",
                      "time_downsample", "t_sample", "target", "target_id", "maskfile", "rficfg"]
+    # bindings.cpp:59-61 names the 4th and 5th parameters dm, tend (positionally tend, dm)
+    names = list(inspect.signature(C._dedisperse_spec_with_dm).parameters)
+    assert names == ["data", "header", "tstart", "dm", "tend", "freq_start", "freq_end",
+                     "maskfile", "rficfg"]
+    names = list(inspect.signature(C._dedispered_fil_with_dm_uint16).parameters)
+    assert names == ["fil", "tstart", "tend", "dm", "freq_start", "freq_end", "maskfile", "rficfg"]
 
 
 def test_dedispered_fil_unknown_target_raises_like_the_reference(tmp_path):
@@ -158,6 +164,14 @@ def test_dedispered_fil_unknown_target_raises_like_the_reference(tmp_path):
         C._dedispered_fil(str(p), 0, 10, 1100.0, 1101.5, 1, 1, 0.001, target=7)
 
 
-def test_single_dm_entry_points_say_they_are_missing():
-    with pytest.raises(NotImplementedError):
-        C._dedisperse_spec_with_dm(None, None, 0, 0, 0, 0, 0, "", None)
+def test_single_dm_fil_entry_points_check_the_sample_width(tmp_path):
+    """_dedispered_fil_with_dm_uint{8,16,32} read the Filterbank's samples as their
+    own type; a file of another width is refused before any device work."""
+    p = tmp_path / "a.fil"
+    write_fil(str(p), np.zeros((64, 8), np.uint8), 1e-3, 1000.0, 1.0)
+    fb = C.Filterbank(str(p))
+    for f in (C._dedispered_fil_with_dm_uint16, C._dedispered_fil_with_dm_uint32):
+        with pytest.raises(ValueError):
+            f(fb, 0.0, 0.01, 1.0, 1000.0, 1007.0, "", C.RFIconfig())
+    with pytest.raises(RuntimeError):
+        C._dedispered_fil_with_dm_uint8(None, 0.0, 0.01, 1.0, 1000.0, 1007.0, "", C.RFIconfig())
