@@ -361,14 +361,6 @@ def _to_device(a: np.ndarray, device: int):
     return t.view({np.uint8: torch.uint8, np.uint16: torch.uint16, np.uint32: torch.uint32}[a.dtype.type])
 
 
-def _to_host(t) -> np.ndarray:
-    import torch
-
-    if t.dtype == torch.uint32:
-        return t.view(torch.int32).cpu().numpy().view(np.uint32)
-    return t.view(torch.int64).cpu().numpy().view(np.uint64)
-
-
 def _result(images, dm_low, dm_high, dm_step, tsample, filname) -> DedispersedDataUint8:
     r = DedispersedDataUint8()
     r._dm_times = list(images)
@@ -408,9 +400,8 @@ def _dedisperse_spec(data, header, dm_low, dm_high, freq_start, dm_step=1, ref_f
         subband_width=SUBBAND_WIDTH, ndm0=NDM0, zero_dm_mode=ZERO_DM_MODE, freq_mode="header",
         rfi=rfi.params(), bad_channels=bad, device=int(target_id)))
     out = plan.run(_to_device(a, int(target_id)))
-    raw = _to_host(out)
     tsamp_out = _f32(header.tsamp * np.float32(ds)) if ds > 1 else header.tsamp
-    imgs = postprocess.slice_images(raw, tsamp_out, 1, t_sample)
+    imgs = postprocess.device_slice_images(out, tsamp_out, 1, t_sample)
     return _result(imgs, dm_low, dm_high, dm_step_, t_sample, header.filename)
 
 
@@ -434,28 +425,31 @@ def _dedispered_fil(filename, dm_low, dm_high, freq_start, freq_end, dm_step, ti
                     algorithm="subband", subband_width=SUBBAND_WIDTH, ndm0=NDM0,
                     zero_dm_mode=ZERO_DM_MODE, freq_mode="fil", freq_table=fil.frequency_table,
                     rfi=rfi.params(), bad_channels=bad, device=int(target_id))
-        raw = _to_host(plan.run(_to_device(a, int(target_id))))
+        out = plan.run(_to_device(a, int(target_id)))
         ds = int(time_downsample)
         tsamp_out = _f32(fil.tsamp * ds) if ds > 1 else _f32(fil.tsamp)
-        imgs = postprocess.slice_images(raw, tsamp_out, 1, t_sample)
+        imgs = postprocess.device_slice_images(out, tsamp_out, 1, t_sample)
+        del out
         plan.close()
         return _result(imgs, dm_low, dm_high, dm_step, t_sample, fil.filename)
     plan = Plan(hdr, dm_low, dm_high, freq_start, freq_end, dm_step, int(time_downsample), t_sample,
                 algorithm="brute", freq_mode="fil", freq_table=fil.frequency_table,
                 device=int(target_id))
-    raw = _to_host(plan.run(_to_device(a, int(target_id))))
-    plan.close()
+    out = plan.run(_to_device(a, int(target_id)))
     # slices of std::round(t_sample / tsamp) samples, each ceil(len / ds) columns,
     # concatenated along time (include/cpucal.hpp:141-160).  The last, shorter slice
     # gets its own width; the reference reads it with the first slice's width.
     sps = int(np.floor(float(np.float32(t_sample)) / fil.tsamp + 0.5))
     ds = int(time_downsample)
-    blocks, off = [], 0
+    starts, counts, off = [], [], 0
     for start in range(0, fil.ndata, sps):
         cols = (min(start + sps, fil.ndata) - start + ds - 1) // ds
-        blocks.append(raw[:, off:off + cols])
+        starts.append(off)
+        counts.append(cols)
         off += cols
-    imgs = postprocess.images(blocks)
+    imgs = postprocess.to_host_images(postprocess.device_images(out, starts, counts))
+    del out
+    plan.close()
     return _result(imgs, dm_low, dm_high, dm_step, t_sample, fil.filename)
 
 

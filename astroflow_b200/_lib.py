@@ -33,6 +33,7 @@ EXPORTS = ("dd_plan_create", "dd_plan_destroy", "dd_plan_destroy_async", "dd_pla
            "dd_batch_run", "dd_batch_status", "dd_batch_get_info", "dd_batch_destroy",
            "dd_stream_open", "dd_stream_push", "dd_stream_get_info", "dd_stream_plan",
            "dd_stream_close", "dd_single_dm_geometry", "dd_single_dm_run",
+           "dd_images",
            "dd_last_error", "dd_abi_version")
 
 
@@ -152,6 +153,8 @@ def load():
                                         ctypes.POINTER(SingleDmInfo)]
     L.dd_single_dm_run.argtypes = [ctypes.POINTER(Header), ctypes.POINTER(SingleDmParams),
                                    ctypes.POINTER(RfiConfig), P, ctypes.c_int32, P, P, P, P]
+    L.dd_images.argtypes = [P, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, P, P,
+                            ctypes.c_int32, P, P, P, P]
     L.dd_stream_open.argtypes = [ctypes.POINTER(Header), ctypes.POINTER(PlanParams),
                                  ctypes.POINTER(RfiConfig), P, ctypes.c_int32, ctypes.c_int32,
                                  ctypes.POINTER(P)]

@@ -38,6 +38,7 @@ UNITS = [
     ("dd_sumsmem.cu", []),
     ("dd_noalloc.cu", []),
     ("dd_single.cu", ["-Xcompiler", "-fno-fast-math"]),
+    ("dd_image.cu", ["-Xcompiler", "-fno-fast-math"]),
 ]
 HOST = ["dd_api.cpp"]
 HEADERS = ["dd_internal.h", os.path.join("..", "..", "include", "astroflow_dd.h")]

@@ -711,9 +711,14 @@ size_t sum_smem_bytes(int win_bytes, int stages) {
   return static_cast<size_t>(2 * stages + 1) * win_bytes;
 }
 
+#ifndef DD_SUM_SMEM_KB
+#define DD_SUM_SMEM_KB 100
+#endif
+// Staged source pairs for a window size: as many as fit DD_SUM_SMEM_KB of shared
+// memory (two blocks per SM at the default), at least two.
 int sum_stages(int win_bytes) {
   int s = kMaxStages;
-  while (s > 2 && sum_smem_bytes(win_bytes, s) > 100 * 1024) --s;
+  while (s > 2 && sum_smem_bytes(win_bytes, s) > DD_SUM_SMEM_KB * 1024) --s;
   return s;
 }
 

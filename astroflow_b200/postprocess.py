@@ -6,12 +6,14 @@ slices of t_sample seconds) and include/data.h:299-369 (the CPU path: one image
 per slice it already produced).  Each image is: uint sums -> float32, resize to
 512x512 (INTER_AREA when both dimensions exceed 512, else INTER_LANCZOS4),
 min-max normalise to uint8, gray -> RGB, COLORMAP_VIRIDIS.  This module does the
-same with OpenCV's Python binding on the host.
+same with OpenCV's Python binding on the host (slice_images, images) and on the
+GPU through dd_images (device_slice_images, device_images): the GPU form resizes,
+normalises and colors in device memory and copies only the images to the host.
 """
 from __future__ import annotations
 
 from concurrent.futures import ThreadPoolExecutor
-from typing import List, Sequence
+from typing import List, Optional, Sequence
 
 import numpy as np
 
@@ -53,3 +55,79 @@ def images(blocks: Sequence[np.ndarray], threads: int = 16) -> List[np.ndarray]:
     """One image per block (include/data.h:299-369)."""
     with ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
         return list(ex.map(_image, blocks))
+
+
+_LUT: Optional[np.ndarray] = None
+
+
+def viridis_lut() -> np.ndarray:
+    """The 256 BGR colors OpenCV's COLORMAP_VIRIDIS gives a gray ramp converted to
+    RGB (the reference's cvtColor + applyColorMap), as a [256, 3] uint8 table."""
+    global _LUT
+    if _LUT is None:
+        import cv2
+
+        ramp = np.arange(256, dtype=np.uint8).reshape(16, 16)
+        rgb = cv2.cvtColor(ramp, cv2.COLOR_GRAY2RGB)
+        _LUT = np.ascontiguousarray(cv2.applyColorMap(rgb, cv2.COLORMAP_VIRIDIS).reshape(256, 3))
+    return _LUT
+
+
+def device_images(out, col_start: Sequence[int], col_count: Sequence[int], target: int = TARGET,
+                  stream=None, resized: bool = False):
+    """Images of column slices of a device DM-time tensor out [rows, cols] (uint32
+    or uint64), made on the GPU (dd_images).  Returns the device tensor
+    [n, target, target, 3] uint8, or with resized=True the float images
+    [n, target, target] before normalisation."""
+    import ctypes
+
+    import torch
+
+    from . import _lib
+
+    L = _lib.load()
+    if not out.is_cuda or out.dim() != 2 or out.element_size() not in (4, 8):
+        raise ValueError("out must be a 2-D CUDA tensor of uint32 or uint64 sums")
+    if out.stride(1) != 1:
+        raise ValueError("out rows must be contiguous")
+    c0 = np.ascontiguousarray(col_start, np.int64)
+    cn = np.ascontiguousarray(col_count, np.int64)
+    n = int(c0.size)
+    dev = out.device
+    if stream is None:
+        stream = torch.cuda.current_stream(dev)
+    img = f32 = None
+    if resized:
+        f32 = torch.empty((n, target, target), dtype=torch.float32, device=dev)
+    else:
+        img = torch.empty((n, target, target, 3), dtype=torch.uint8, device=dev)
+    lut = viridis_lut()
+    _lib.check(L.dd_images(ctypes.c_void_p(out.data_ptr()), out.element_size(), out.shape[0],
+                           out.stride(0), n, c0.ctypes.data, cn.ctypes.data, target,
+                           lut.ctypes.data, None if img is None else img.data_ptr(),
+                           None if f32 is None else f32.data_ptr(),
+                           ctypes.c_void_p(stream.cuda_stream)))
+    return f32 if resized else img
+
+
+def slice_bounds(cols: int, sps: int):
+    """Column starts and widths of the t_sample slices (include/data.h:644-691)."""
+    n = (cols + sps - 1) // sps
+    starts = [i * sps for i in range(n)]
+    return starts, [min(sps, cols - s) for s in starts]
+
+
+def to_host_images(dev_imgs) -> List[np.ndarray]:
+    """One device-to-host copy of [n, t, t, 3] images, returned as n arrays."""
+    host = dev_imgs.cpu().numpy()
+    return [host[i] for i in range(host.shape[0])]
+
+
+def device_slice_images(out, tsamp: float, time_downsample: int,
+                        slice_duration: float) -> List[np.ndarray]:
+    """slice_images on the GPU: the same images from the device DM-time tensor."""
+    sps = samples_per_slice(tsamp, time_downsample, slice_duration)
+    if sps <= 0:
+        raise ValueError("t_sample is shorter than one (downsampled) sample")
+    starts, counts = slice_bounds(out.shape[1], sps)
+    return to_host_images(device_images(out, starts, counts))

@@ -292,6 +292,23 @@ int dd_single_dm_run(const dd_header* header, const dd_single_dm_params* params,
                      const dd_rfi_config* rfi, const int32_t* bad_channels, int32_t n_bad,
                      const void* input, void* output, void* masked_rows, void* stream);
 
+/* ---- DM-time images: the image step of the reference's GPU path
+ * (preprocess_typed_dedisperseddata_with_slicing, include/data.h:620-727) and of
+ * its CPU path (preprocess_dedisperseddata, data.h:299-369), on the GPU.  Each
+ * slice (columns [col_start[i], col_start[i] + col_count[i]) of every row) is
+ * converted to float, resized to target x target (INTER_AREA when both of its
+ * dimensions exceed target, else INTER_LANCZOS4, with OpenCV's float rounding),
+ * min-max normalised to uint8 and colored through lut_bgr (256 BGR triples, e.g.
+ * OpenCV's COLORMAP_VIRIDIS of a gray ramp).  dm_time: device [nrows][row_pitch]
+ * of uint32 (elem_bytes 4) or uint64 (8).  Outputs (device, either may be NULL
+ * but not both): images [nslices][target][target][3] uint8 (B, G, R) and
+ * resized [nslices][target][target] float.  col_start, col_count and lut_bgr are
+ * host arrays.  target <= 1024. */
+int dd_images(const void* dm_time, int32_t elem_bytes, int64_t nrows, int64_t row_pitch,
+              int32_t nslices, const int64_t* col_start, const int64_t* col_count,
+              int32_t target, const uint8_t* lut_bgr, uint8_t* images, float* resized,
+              void* stream);
+
 /* ---- Batches: many chunks of different geometries dedispersed together.
  * The reference dedisperses one chunk per call (gpucal::dedisperse_spec,
  * src/core/dedispered.cu:988-1304).  A batch runs one chunk through each of its

@@ -175,3 +175,13 @@ def test_single_dm_fil_entry_points_check_the_sample_width(tmp_path):
             f(fb, 0.0, 0.01, 1.0, 1000.0, 1007.0, "", C.RFIconfig())
     with pytest.raises(RuntimeError):
         C._dedispered_fil_with_dm_uint8(None, 0.0, 0.01, 1.0, 1000.0, 1007.0, "", C.RFIconfig())
+
+
+def test_viridis_table_is_the_reference_colormap():
+    """The GPU image step colors through a 256-entry table; it must equal
+    cvtColor(GRAY2RGB) + applyColorMap(VIRIDIS) (include/data.h:703-705)."""
+    cv2 = pytest.importorskip("cv2")
+    lut = postprocess.viridis_lut()
+    g = np.random.default_rng(3).integers(0, 256, (64, 80), dtype=np.uint8)
+    want = cv2.applyColorMap(cv2.cvtColor(g, cv2.COLOR_GRAY2RGB), cv2.COLORMAP_VIRIDIS)
+    assert lut.shape == (256, 3) and np.array_equal(lut[g], want)
