@@ -14,7 +14,10 @@ RFI channels, broadband impulses and three dispersed pulses injected.
 Prints one JSON line (rank 0).  `value` is DM-trial*samples per second over all
 ranks (weak scaling: every rank dedisperses its own chunk; the path has no
 exchange between GPUs).  `e2e` is the same metric through the C ABI with host
-buffers (dd_run_host: host->device copy, run, device->host copy per step).
+buffers (dd_run_host: host->device copy, run, device->host copy per step);
+`e2e_dropin` the same through the drop-in _astroflow_core._dedisperse_spec (host
+numpy chunk in, the 512x512x3 images of every t_sample slice out, made on the
+GPU).
 `--impl reference` times the reference's own CPU implementation of the path
 (include/cpucal.hpp, built from source into oracle/_ref) on this host's cores;
 `--impl reference-gpu` times the reference's own GPU path (src/core/dedispered.cu
@@ -676,6 +679,51 @@ def e2e_run(plan, x, out, units, dist, dev, stream, steps):
     return e2e, same
 
 
+def e2e_dropin_run(wl, hdr, x, units, dist, dev, steps, t_sample=0.5):
+    """The workload's metric through the drop-in call the reference's users make,
+    _astroflow_core._dedisperse_spec: a host numpy chunk in, the t_sample-second
+    512x512x3 viridis images out (what the reference returns), every copy and the
+    image step inside the timed region."""
+    import torch
+
+    from astroflow_b200 import _astroflow_core as C
+
+    x_host = x.cpu().numpy()
+    if wl["nbits"] == 16:
+        x_host = x_host.view(np.uint16)
+    header = C.Header(0.0, hdr["tsamp"], hdr["fch1"], hdr["foff"], wl["nbits"], wl["nchans"],
+                      wl["nsamp"], "bench")
+    r = wl["rfi"]
+    rfi = C.RFIconfig()
+    if r:
+        q = r["iqrm"]
+        rfi = C.RFIconfig(r["use_mask"], r["use_zero_dm"], r["use_iqrm"],
+                          C.IQRMconfig(q["mode"], q["radius_frac"], q["nsigma"], q["geofactor"],
+                                       q["win_sec"], q["hop_sec"], q["include_tail"]))
+    C.SUBBAND_WIDTH = wl["subband_width"]
+    lo, hi, step = wl["dm"]
+    f32 = np.float32
+    fs = float(f32(hdr["fch1"]))
+    fe = float(f32(f32(hdr["fch1"]) + f32(wl["nchans"] - 1) * f32(hdr["foff"])))
+    args = (x_host, header, lo, hi, fs, fe, step, wl["ds"], t_sample, dev, "", rfi)
+    res = C._dedisperse_spec(*args)  # builds and caches the plan
+    stream = torch.cuda.current_stream(dev)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        res = C._dedisperse_spec(*args)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_rank = e0.elapsed_time(e1) / steps
+    n = len(res.dm_times)
+    return {"value": dist.job_rate(units, ms_rank * 1e-3), "unit": UNIT,
+            "h2d_bytes_per_step": int(x_host.nbytes), "d2h_bytes_per_step": int(n * 512 * 512 * 3),
+            "ms_per_step": dist.max(ms_rank), "images": n, "t_sample": t_sample,
+            "api": "_astroflow_core._dedisperse_spec: host numpy chunk in, images out"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -841,6 +889,11 @@ def main():
     if args.e2e_steps > 0:
         e2e, same = e2e_run(plan, x, out, units, dist, dev, stream, args.e2e_steps)
 
+    e2e_dropin = None
+    if args.e2e_steps > 0 and wl["algorithm"] == "subband":
+        del out
+        e2e_dropin = e2e_dropin_run(wl, hdr, x, units, dist, dev, args.e2e_steps)
+
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
@@ -857,7 +910,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": f"u{wl['nbits']}", "data": "synthetic (seeded, generated on the GPU)",
                 "config": config, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches, "clocks": clk,
+                "e2e_dropin": e2e_dropin, "gpu_launches": launches, "clocks": clk,
                 "host_path_matches_device": same}
         print(json.dumps(line))
     dist.close()
