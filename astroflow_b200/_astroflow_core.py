@@ -33,7 +33,7 @@ from typing import List, Optional
 
 import numpy as np
 
-from . import postprocess
+from . import ingest, postprocess
 from .dedisp import IqrmParams, Plan, RfiParams
 
 REF_FREQ_END = 1
@@ -412,45 +412,53 @@ def _dedispered_fil(filename, dm_low, dm_high, freq_start, freq_end, dm_step, ti
     cpucal::dedispered_fil_omp (include/cpucal.hpp:75-201), here as the brute-force
     kernel with the CPU path's semantics."""
     rfi = rficfg if rficfg is not None else RFIconfig()
-    fil = Filterbank(filename)
-    if fil.nbits not in (8, 16, 32) or target not in (CPU_TARGET, GPU_TARGET):
+    try:
+        fh, table = ingest.fil_header(filename)
+    except ValueError as e:  # the reference's reader raises these as RuntimeError
+        raise RuntimeError(str(e)) from None
+    if target not in (CPU_TARGET, GPU_TARGET):
         # the reference's switch falls through to its default for any other target
-        raise RuntimeError(f"Unsupported nbits value: {fil.nbits}")
-    a = fil.data.reshape(fil.ndata, -1)
-    hdr = dict(tsamp=fil.tsamp, fch1=fil.fch1, foff=fil.foff, nbits=fil.nbits,
-               nchans=fil.nchans, ndata=fil.ndata)
+        raise RuntimeError(f"Unsupported nbits value: {fh['nbits']}")
+    if fh["nifs"] == 1:
+        # straight from the file into device memory (pinned staging, flip on the GPU)
+        x = ingest.read_filterbank(filename, device=int(target_id))[0].view(-1)
+    else:
+        fil = Filterbank(filename)
+        x = _to_device(fil.data.reshape(fil.ndata, -1), int(target_id))
+    ndata, tsamp = fh["ndata"], fh["tsamp"]
+    hdr = dict(tsamp=tsamp, fch1=fh["fch1"], foff=fh["foff"], nbits=fh["nbits"],
+               nchans=fh["nchans"], ndata=ndata)
     bad = load_mask_file(maskfile)
     if target == GPU_TARGET:
         plan = Plan(hdr, dm_low, dm_high, freq_start, freq_end, dm_step, int(time_downsample),
                     algorithm="subband", subband_width=SUBBAND_WIDTH, ndm0=NDM0,
-                    zero_dm_mode=ZERO_DM_MODE, freq_mode="fil", freq_table=fil.frequency_table,
+                    zero_dm_mode=ZERO_DM_MODE, freq_mode="fil", freq_table=table,
                     rfi=rfi.params(), bad_channels=bad, device=int(target_id))
-        out = plan.run(_to_device(a, int(target_id)))
+        out = plan.run(x)
         ds = int(time_downsample)
-        tsamp_out = _f32(fil.tsamp * ds) if ds > 1 else _f32(fil.tsamp)
+        tsamp_out = _f32(tsamp * ds) if ds > 1 else _f32(tsamp)
         imgs = postprocess.device_slice_images(out, tsamp_out, 1, t_sample)
         del out
         plan.close()
-        return _result(imgs, dm_low, dm_high, dm_step, t_sample, fil.filename)
+        return _result(imgs, dm_low, dm_high, dm_step, t_sample, str(filename))
     plan = Plan(hdr, dm_low, dm_high, freq_start, freq_end, dm_step, int(time_downsample), t_sample,
-                algorithm="brute", freq_mode="fil", freq_table=fil.frequency_table,
-                device=int(target_id))
-    out = plan.run(_to_device(a, int(target_id)))
+                algorithm="brute", freq_mode="fil", freq_table=table, device=int(target_id))
+    out = plan.run(x)
     # slices of std::round(t_sample / tsamp) samples, each ceil(len / ds) columns,
     # concatenated along time (include/cpucal.hpp:141-160).  The last, shorter slice
     # gets its own width; the reference reads it with the first slice's width.
-    sps = int(np.floor(float(np.float32(t_sample)) / fil.tsamp + 0.5))
+    sps = int(np.floor(float(np.float32(t_sample)) / tsamp + 0.5))
     ds = int(time_downsample)
     starts, counts, off = [], [], 0
-    for start in range(0, fil.ndata, sps):
-        cols = (min(start + sps, fil.ndata) - start + ds - 1) // ds
+    for start in range(0, ndata, sps):
+        cols = (min(start + sps, ndata) - start + ds - 1) // ds
         starts.append(off)
         counts.append(cols)
         off += cols
     imgs = postprocess.to_host_images(postprocess.device_images(out, starts, counts))
     del out
     plan.close()
-    return _result(imgs, dm_low, dm_high, dm_step, t_sample, fil.filename)
+    return _result(imgs, dm_low, dm_high, dm_step, t_sample, str(filename))
 
 
 _SPECTRA = {8: Spectrum8, 16: Spectrum16, 32: Spectrum32}

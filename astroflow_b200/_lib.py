@@ -33,7 +33,7 @@ EXPORTS = ("dd_plan_create", "dd_plan_destroy", "dd_plan_destroy_async", "dd_pla
            "dd_batch_run", "dd_batch_status", "dd_batch_get_info", "dd_batch_destroy",
            "dd_stream_open", "dd_stream_push", "dd_stream_get_info", "dd_stream_plan",
            "dd_stream_close", "dd_single_dm_geometry", "dd_single_dm_run",
-           "dd_images",
+           "dd_images", "dd_fil_read_header", "dd_fil_read", "dd_ingest_host",
            "dd_last_error", "dd_abi_version")
 
 

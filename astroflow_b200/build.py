@@ -39,6 +39,7 @@ UNITS = [
     ("dd_noalloc.cu", []),
     ("dd_single.cu", ["-Xcompiler", "-fno-fast-math"]),
     ("dd_image.cu", ["-Xcompiler", "-fno-fast-math"]),
+    ("dd_ingest.cu", []),
 ]
 HOST = ["dd_api.cpp"]
 HEADERS = ["dd_internal.h", os.path.join("..", "..", "include", "astroflow_dd.h")]

@@ -309,6 +309,42 @@ int dd_images(const void* dm_time, int32_t elem_bytes, int64_t nrows, int64_t ro
               int32_t target, const uint8_t* lut_bgr, uint8_t* images, float* resized,
               void* stream);
 
+/* ---- Ingest: data into device memory in the plans' layout ([time][channel],
+ * ascending frequency), through pinned staging blocks that worker threads fill
+ * while earlier blocks are copied and transformed on the device.
+ *
+ * dd_fil_read_header parses a SIGPROC header as the reference's Filterbank does
+ * (src/data/filterbank.cpp:319-452: keywords, FREQUENCY_START/fchannel tables,
+ * sample count from the file size) and reports it after the reference's channel
+ * flip (filterbank.cpp:793-842: foff < 0 -> ascending order, fch1 = lowest
+ * frequency, foff = |foff|; a file with a frequency table keeps fch1 = foff = 0);
+ * freq_table (optional, cap entries) receives the frequency table in that order.
+ * dd_fil_read streams samples [t0, t0 + nsamp) of a single-IF file into
+ * device_out ([nsamp][nchans], nbits/8 bytes per sample), flipping the channel
+ * order on the device when the file's foff < 0.  dd_ingest_host does the same
+ * from a host array [nsamp][npol][nchans]: npol 1 copies (DD_INGEST_FLIP
+ * reverses the channels), npol >= 2 averages polarisations 0 and 1 as the
+ * reference's PSRFITS reader does (python/astroflow/io/psrfits.py:44-51:
+ * ((a + b) / 2).astype(dtype), the sum wrapping in the sample type, the
+ * halving truncating toward zero; DD_INGEST_SIGNED for signed samples), then
+ * flips if asked.  Both return when the copies are done; work queued on
+ * `stream` afterwards sees the data. */
+typedef struct dd_fil_header {
+  double tsamp, fch1, foff, tstart;
+  int64_t ndata;          /* samples in the file */
+  int64_t header_bytes;
+  int32_t nbits, nchans, nifs;
+  int32_t flipped;        /* the file's channels run downwards; reads reverse them */
+  int32_t has_freq_table;
+  int32_t pad;
+} dd_fil_header;
+#define DD_INGEST_FLIP 1
+#define DD_INGEST_SIGNED 2
+int dd_fil_read_header(const char* path, dd_fil_header* out, double* freq_table, int32_t cap);
+int dd_fil_read(const char* path, int64_t t0, int64_t nsamp, void* device_out, void* stream);
+int dd_ingest_host(const void* host, int64_t nsamp, int32_t npol, int32_t nchans,
+                   int32_t elem_bytes, int32_t flags, void* device_out, void* stream);
+
 /* ---- Batches: many chunks of different geometries dedispersed together.
  * The reference dedisperses one chunk per call (gpucal::dedisperse_spec,
  * src/core/dedispered.cu:988-1304).  A batch runs one chunk through each of its
