@@ -354,11 +354,11 @@ def _as_spec_array(data) -> np.ndarray:
 
 
 def _to_device(a: np.ndarray, device: int):
-    import torch
-
-    view = {np.uint8: a, np.uint16: a.view(np.int16), np.uint32: a.view(np.int32)}[a.dtype.type]
-    t = torch.from_numpy(view.reshape(-1)).to(f"cuda:{device}")
-    return t.view({np.uint8: torch.uint8, np.uint16: torch.uint16, np.uint32: torch.uint32}[a.dtype.type])
+    """A C-contiguous host array as a flat device tensor of the same samples, copied
+    through the library's pinned staging (dd_ingest_host: about four times the
+    rate of a copy from pageable memory)."""
+    rows = a.reshape(-1, a.shape[-1] if a.ndim > 1 and a.shape[-1] > 0 else 1)
+    return ingest.to_device(rows, device=device).view(-1)
 
 
 def _result(images, dm_low, dm_high, dm_step, tsample, filname) -> DedispersedDataUint8:

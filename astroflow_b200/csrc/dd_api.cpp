@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -596,8 +597,13 @@ SumLaunch stage2_launch(const dd_plan& P, int64_t t0, void* output) {
   return L;
 }
 
+// after_tile(t0, cols): called once the work producing output columns
+// [t0, t0 + cols) of every DM row has been queued on the stream.
+using TileHook = std::function<void(int64_t, int64_t)>;
+
 void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out,
-                 uint32_t* bounds_out, void* prepped, cudaStream_t st, Prof* pf = nullptr) {
+                 uint32_t* bounds_out, void* prepped, cudaStream_t st, Prof* pf = nullptr,
+                 const TileHook& after_tile = TileHook()) {
   cudaEvent_t a = pf ? pf->mark() : nullptr;
   run_rfi_and_prep(P, input, masks_out, bounds_out, prepped, st);
   if (pf) pf->prep.emplace_back(a, pf->mark());
@@ -645,6 +651,7 @@ void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out
       launch_stage2(s2, st);
     }
     if (pf) pf->s2.emplace_back(b2, pf->mark());
+    if (after_tile) after_tile(t0, std::min<int64_t>(P.tile, P.nout - t0));
   }
 }
 
@@ -1038,23 +1045,60 @@ int dd_run_host(dd_plan* P, const void* h_input, void* h_output, void* stream) {
     DeviceGuard g(P->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t in_bytes = static_cast<size_t>(P->nin * P->hdr.nchans) * P->elem;
-    const size_t out_bytes = static_cast<size_t>(P->dm_steps) *
-                             (P->p.algorithm == DD_ALGO_BRUTE ? P->out_cols : P->nout) *
-                             (P->nbits == 32 ? 8 : 4);
-    void* d_in = nullptr;
-    void* d_out = nullptr;
-    DD_CUDA_TRY(cudaMallocAsync(&d_in, in_bytes, st));
-    cudaError_t e = cudaMallocAsync(&d_out, out_bytes, st);
-    if (e != cudaSuccess) {
-      cudaFreeAsync(d_in, st);
-      throw Error{DD_ERR_NOMEM, std::string("output allocation failed: ") + cudaGetErrorString(e)};
+    const int64_t cols = P->p.algorithm == DD_ALGO_BRUTE ? P->out_cols : P->nout;
+    const size_t oelem = P->nbits == 32 ? 8 : 4;
+    const size_t out_bytes = static_cast<size_t>(P->dm_steps) * cols * oelem;
+    // device buffers of the host path, kept by the plan across calls
+    if (P->d_host_in.bytes < in_bytes) P->d_host_in.alloc(in_bytes);
+    if (P->d_host_out.bytes < out_bytes) {
+      P->d_host_out.release();
+      try {
+        P->d_host_out.alloc(out_bytes);
+      } catch (const Error& er) {
+        throw Error{DD_ERR_NOMEM, "output allocation failed: " + er.msg};
+      }
     }
-    DD_CUDA_TRY(cudaMemcpyAsync(d_in, h_input, in_bytes, cudaMemcpyHostToDevice, st));
-    if (P->p.algorithm == DD_ALGO_BRUTE) run_brute(*P, d_in, d_out, nullptr, st);
-    else run_subband(*P, d_in, d_out, nullptr, nullptr, nullptr, st);
-    DD_CUDA_TRY(cudaMemcpyAsync(h_output, d_out, out_bytes, cudaMemcpyDeviceToHost, st));
-    DD_CUDA_TRY(cudaFreeAsync(d_in, st));
-    DD_CUDA_TRY(cudaFreeAsync(d_out, st));
+    // buffers are allocated stream-ordered on the legacy stream: make them visible to `st`
+    DD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
+    char* d_out = P->d_host_out.as<char>();
+    DD_CUDA_TRY(cudaMemcpyAsync(P->d_host_in.p, h_input, in_bytes, cudaMemcpyHostToDevice, st));
+    if (P->p.algorithm == DD_ALGO_BRUTE) {
+      run_brute(*P, P->d_host_in.p, d_out, nullptr, st);
+      DD_CUDA_TRY(cudaMemcpyAsync(h_output, d_out, out_bytes, cudaMemcpyDeviceToHost, st));
+    } else {
+      // each time tile's output columns go to the host on a second stream while
+      // the next tile is summed
+      if (!P->copy_stream) DD_CUDA_TRY(cudaStreamCreateWithFlags(&P->copy_stream, cudaStreamNonBlocking));
+      std::vector<cudaEvent_t> evs;
+      auto cleanup = [&]() {
+        for (cudaEvent_t ev : evs) cudaEventDestroy(ev);
+      };
+      try {
+        run_subband(*P, P->d_host_in.p, d_out, nullptr, nullptr, nullptr, st, nullptr,
+                    [&](int64_t t0, int64_t n) {
+                      cudaEvent_t ev;
+                      DD_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+                      evs.push_back(ev);
+                      DD_CUDA_TRY(cudaEventRecord(ev, st));
+                      DD_CUDA_TRY(cudaStreamWaitEvent(P->copy_stream, ev, 0));
+                      const size_t pitch = static_cast<size_t>(cols) * oelem;
+                      DD_CUDA_TRY(cudaMemcpy2DAsync(static_cast<char*>(h_output) + t0 * oelem, pitch,
+                                                    d_out + t0 * oelem, pitch, n * oelem,
+                                                    static_cast<size_t>(P->dm_steps),
+                                                    cudaMemcpyDeviceToHost, P->copy_stream));
+                    });
+        cudaEvent_t done;
+        DD_CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        evs.push_back(done);
+        DD_CUDA_TRY(cudaEventRecord(done, P->copy_stream));
+        DD_CUDA_TRY(cudaStreamWaitEvent(st, done, 0));
+      } catch (...) {
+        cudaStreamSynchronize(P->copy_stream);
+        cleanup();
+        throw;
+      }
+      cleanup();
+    }
     DD_CUDA_TRY(cudaStreamSynchronize(st));
     check_device_error(*P, st);
   });

@@ -109,6 +109,8 @@ struct dd_plan {
   dd::DevBuf d_delay, d_res, d_lags, d_bad_keep, d_win, d_seg_t0;
   dd::DevBuf d_binned;   // binned / working copy of the input [nbin][nchans]
   dd::DevBuf d_x;        // prepared channel-major input
+  dd::DevBuf d_host_in, d_host_out;  // device side of dd_run_host (kept across calls)
+  cudaStream_t copy_stream = nullptr; // dd_run_host: output copies overlapping the sums
   dd::DevBuf d_inter;    // stage-1 tile
   dd::DevBuf d_stats;    // IQRM sums [nwin][2][csub] uint64
   dd::DevBuf d_iqrm_scratch;
@@ -122,6 +124,10 @@ struct dd_plan {
   std::vector<cudaEvent_t> events;  // timing events of dd_run_profiled
   ~dd_plan() {
     for (cudaEvent_t e : events) cudaEventDestroy(e);
+    if (copy_stream) {
+      cudaStreamSynchronize(copy_stream);
+      cudaStreamDestroy(copy_stream);
+    }
   }
 };
 

@@ -118,9 +118,14 @@ def slice_bounds(cols: int, sps: int):
 
 
 def to_host_images(dev_imgs) -> List[np.ndarray]:
-    """One device-to-host copy of [n, t, t, 3] images, returned as n arrays."""
-    host = dev_imgs.cpu().numpy()
-    return [host[i] for i in range(host.shape[0])]
+    """One device-to-host copy of [n, t, t, 3] images into pinned memory, returned
+    as n arrays (views that keep the pinned block alive)."""
+    import torch
+
+    host = torch.empty(tuple(dev_imgs.shape), dtype=dev_imgs.dtype, pin_memory=True)
+    host.copy_(dev_imgs)
+    h = host.numpy()
+    return [h[i] for i in range(h.shape[0])]
 
 
 def device_slice_images(out, tsamp: float, time_downsample: int,

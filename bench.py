@@ -889,9 +889,12 @@ def main():
     if args.e2e_steps > 0:
         e2e, same = e2e_run(plan, x, out, units, dist, dev, stream, args.e2e_steps)
 
+    # and through the drop-in call (its own plan and output; ours released first)
     e2e_dropin = None
     if args.e2e_steps > 0 and wl["algorithm"] == "subband":
         del out
+        plan.close()
+        torch.cuda.empty_cache()
         e2e_dropin = e2e_dropin_run(wl, hdr, x, units, dist, dev, args.e2e_steps)
 
     cpu = None

@@ -202,7 +202,10 @@ int dd_run_ex(dd_plan* plan, const void* input, void* output, uint8_t* iqrm_mask
               uint32_t* iqrm_bounds, void* prepped, void* stream);
 
 /* dd_run from host memory: copies input in, runs, copies the output back and
- * synchronises the stream.  Host buffers may be pageable or pinned. */
+ * synchronises the stream.  Host buffers may be pageable or pinned (pinned
+ * buffers let the output of each time tile travel while the next tile is
+ * summed).  The device-side input and output buffers are kept by the plan for
+ * later calls and released with it. */
 int dd_run_host(dd_plan* plan, const void* h_input, void* h_output, void* stream);
 
 /* Device-time breakdown of one run, measured with CUDA events on the run's
