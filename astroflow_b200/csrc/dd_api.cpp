@@ -49,6 +49,9 @@ int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 // Bytes of one stage-1 sum: uint16 for 8-bit input in narrow subbands, else the
 // reference's accumulator type (uint32, or uint64 for 32-bit samples).
 int64_t inter_elem(const dd_plan& P) { return P.inter16 ? 2 : (P.nbits == 32 ? 8 : 4); }
+// Stage 1 of 8-bit samples into 32-bit sums widens its 16-bit lanes every 256
+// sources only when a subband holds more than 257 channels (257 x 255 fits).
+bool stage1_flush(const dd_plan& P) { return P.nbits == 8 && !P.inter16 && P.sbw > 257; }
 
 // ---- frequency table and band (dedispered.cu:1003-1031, cpucal.hpp:85-116)
 void build_freq(dd_plan& P) {
@@ -328,9 +331,12 @@ void create_subband(dd_plan& P) {
   for (int v : P.h_res) { P.max_res = std::max(P.max_res, v); minr = std::min(minr, v); }
   if (mind < 0 || minr < 0)
     throw invalid("negative dispersion delays (DM below zero or band order) are not supported");
-  P.inter16 = (P.nbits == 8 && P.sbw <= 257) ? 1 : 0;
+#ifndef DD_INTER32
+#define DD_INTER32 1
+#endif
+  P.inter16 = (P.nbits == 8 && P.sbw <= 257 && !DD_INTER32) ? 1 : 0;
   if (P.nbits <= 16) {
-    const int T1 = sum_variant_tile(P.elem, P.nbits == 8 && !P.inter16);
+    const int T1 = sum_variant_tile(P.elem, stage1_flush(P));
     P.win1 = window_bytes(table_spread(P.h_delay, P.ndm_nom, P.dch, kSumRows, 0), T1, P.elem);
   }
   if (P.nbits <= 16) {
@@ -352,11 +358,14 @@ void create_subband(dd_plan& P) {
   // tiles T1: L = n*T1 - R with R the halo rounded to the base tile.  n grows
   // while one tile of subband sums stays within 1 GiB and the tile is not
   // longer than the chunk.
-  const int64_t T1 = P.win1 ? sum_variant_tile(P.elem, P.nbits == 8 && !P.inter16) : kT;
+  const int64_t T1 = P.win1 ? sum_variant_tile(P.elem, stage1_flush(P)) : kT;
   const int64_t R = round_up(std::max<int64_t>(P.max_res, 1), kT);
   int64_t n = 1;
   while (n * T1 - R < kT) ++n;
-  while (((n + 1) * T1 - R) * per_col <= (int64_t(1) << 30) && (n * T1 - R) < P.nout) ++n;
+#ifndef DD_INTER_MB
+#define DD_INTER_MB 2048
+#endif
+  while (((n + 1) * T1 - R) * per_col <= (int64_t(DD_INTER_MB) << 20) && (n * T1 - R) < P.nout) ++n;
   int64_t L = std::max<int64_t>(kT, n * T1 - R);
   P.tile = L;
   // Stage-2 blocks past the tile's last column read up to one block tile beyond it
@@ -554,7 +563,7 @@ SumLaunch stage1_launch(const dd_plan& P, int64_t t0) {
   L.ncols = P.tile + P.max_res;
   L.win_bytes = P.win1;
   L.src_bytes = P.elem;
-  L.flush = (P.nbits == 8 && !P.inter16) ? 1 : 0;
+  L.flush = stage1_flush(P) ? 1 : 0;
   L.lane_per = 1;
   L.grid_y = static_cast<unsigned>((P.ndm_nom + kSumRows - 1) / kSumRows);
   L.grid_z = static_cast<unsigned>(P.nsb);

@@ -291,7 +291,7 @@ constexpr int kErrWaitEmpty = 2;  // the producer gave up waiting for a free sta
 #define DD_SUM16_NW 4
 #endif
 #ifndef DD_SUM8_NW
-#define DD_SUM8_NW 4
+#define DD_SUM8_NW 5
 #endif
 #ifndef DD_SUM8F_NW
 #define DD_SUM8F_NW 2
@@ -303,7 +303,13 @@ constexpr int kErrWaitEmpty = 2;  // the producer gave up waiting for a free sta
 #ifndef DD_SUM8_MINB
 #define DD_SUM8_MINB 2
 #endif
-constexpr int kSum32NW = 8;  // words per lane of the 32-bit staged sum
+#ifndef DD_SUM32_NW
+#define DD_SUM32_NW 8
+#endif
+#ifndef DD_SUM32_MINB
+#define DD_SUM32_MINB 2
+#endif
+constexpr int kSum32NW = DD_SUM32_NW;  // words per lane of the 32-bit staged sum
 inline int sum_variant_tile(int src_bytes, bool flush) {
   return sum_tile_samples(src_bytes, src_bytes == 4   ? kSum32NW
                                      : src_bytes == 2 ? DD_SUM16_NW

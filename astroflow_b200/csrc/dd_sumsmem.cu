@@ -561,7 +561,7 @@ __global__ void __launch_bounds__(kThreads, DD_SUM16_MINB) k_sum_u16(SumLaunch L
   sum_u16<RB, NW>(L, blockIdx, sw, P);
 }
 template <int RB, int NW>
-__global__ void __launch_bounds__(kThreads, 2) k_sum_u32(SumLaunch L) {
+__global__ void __launch_bounds__(kThreads, DD_SUM32_MINB) k_sum_u32(SumLaunch L) {
   extern __shared__ __align__(128) uint32_t sw[];
   __shared__ Pipe P;
   sum_u32<RB, NW>(L, blockIdx, sw, P);
