@@ -371,6 +371,75 @@ __global__ void __launch_bounds__(256) k_prep_u8(PrepArgs a) {
   }
 }
 
+// 16-bit samples without downsampling, as k_prep_u8 with 16-bit lanes: a block
+// takes 64 samples x 64 channels, loads four channels per 8-byte word pair,
+// applies the masks and the zero-DM offset lane-wise, and transposes 4x4 blocks
+// of 16-bit samples in registers into 8-byte stores of four samples per
+// channel.  Needs nchans % 4 == 0; channel words are read from c0 & ~3 and
+// channels outside [c0, c1) are not stored.
+__global__ void __launch_bounds__(256) k_prep_u16(PrepArgs a) {
+  __shared__ uint2 tile[64][17];  // [sample][four-channel group], padded
+  const uint16_t* x = static_cast<const uint16_t*>(a.x);
+  const int64_t tb = static_cast<int64_t>(blockIdx.x) * 64;
+  const int64_t cb = (a.c0 & ~int64_t(3)) + static_cast<int64_t>(blockIdx.y) * 64;
+  {
+    const int w = threadIdx.x & 15;  // four-channel group of the tile
+    const int64_t c = cb + 4 * w;
+    const bool cvalid = c < a.nchans;
+    uint2 drop = make_uint2(0, 0), inrange = make_uint2(0, 0);  // per 16-bit lane
+    if (cvalid) {
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int64_t ch = c + b;
+        const uint32_t lane = 0xffffu << (16 * (b & 1));
+        if (a.keep && !a.keep[ch]) (b < 2 ? drop.x : drop.y) |= lane;
+        if (a.zdm_off && ch >= a.zdm_cs && ch < a.zdm_ce) (b < 2 ? inrange.x : inrange.y) |= lane;
+      }
+    }
+    for (int r = threadIdx.x >> 4; r < 64; r += 16) {
+      const int64_t t = tb + r;
+      uint2 v = make_uint2(0, 0);
+      if (cvalid && t < a.nsamp) {
+        v = *reinterpret_cast<const uint2*>(x + t * a.nchans + c);
+        if (a.segmask) {
+          const int sg = find_seg(a.seg_t0, a.nseg, t);
+          const uint32_t k = __vcmpne4(*reinterpret_cast<const uint32_t*>(
+                                           a.segmask + static_cast<int64_t>(sg) * a.nchans + c),
+                                       0u);
+          v.x &= ~__byte_perm(k, 0u, 0x1100);
+          v.y &= ~__byte_perm(k, 0u, 0x3322);
+        }
+        if (a.zdm_off) {
+          const uint32_t m = min(a.zdm_off[t], 65535u) * 0x00010001u;
+          v.x = (__vsubus2(v.x, m) & inrange.x) | (v.x & ~inrange.x);
+          v.y = (__vsubus2(v.y, m) & inrange.y) | (v.y & ~inrange.y);
+        }
+        v.x &= ~drop.x;
+        v.y &= ~drop.y;
+      }
+      tile[r][w] = v;
+    }
+  }
+  __syncthreads();
+  if (!a.out) return;
+  const int i = threadIdx.x & 15;  // samples 4i .. 4i+3
+  const int j = threadIdx.x >> 4;  // channels 4j .. 4j+3
+  const uint2 q0 = tile[4 * i][j], q1 = tile[4 * i + 1][j];
+  const uint2 q2 = tile[4 * i + 2][j], q3 = tile[4 * i + 3][j];
+  const uint2 o[4] = {
+      make_uint2(__byte_perm(q0.x, q1.x, 0x5410), __byte_perm(q2.x, q3.x, 0x5410)),
+      make_uint2(__byte_perm(q0.x, q1.x, 0x7632), __byte_perm(q2.x, q3.x, 0x7632)),
+      make_uint2(__byte_perm(q0.y, q1.y, 0x5410), __byte_perm(q2.y, q3.y, 0x5410)),
+      make_uint2(__byte_perm(q0.y, q1.y, 0x7632), __byte_perm(q2.y, q3.y, 0x7632))};
+  uint16_t* out = static_cast<uint16_t*>(a.out);
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int64_t cc = cb + 4 * j + b;
+    if (cc >= a.c0 && cc < a.c1)
+      *reinterpret_cast<uint2*>(out + (cc - a.c0) * a.pitch + tb + 4 * i) = o[b];
+  }
+}
+
 // Full-layout copy of the prepared input (parity checks only): all channels.
 template <typename T>
 __global__ void k_prep_full(PrepArgs a) {
@@ -485,6 +554,12 @@ void launch_prep(const PrepArgs& a, cudaStream_t st) {
     const int64_t cw0 = a.c0 & ~int64_t(3);
     dim3 grid(static_cast<unsigned>((a.nsamp + 63) / 64), static_cast<unsigned>((a.c1 - cw0 + 63) / 64));
     k_prep_u8<<<grid, 256, 0, st>>>(a);
+    DD_LAUNCHED();
+  } else if (a.out && a.nbits == 16 && a.ds == 1 && a.nchans % 4 == 0 && a.pitch % 4 == 0 &&
+             reinterpret_cast<uintptr_t>(a.x) % 8 == 0 && reinterpret_cast<uintptr_t>(a.out) % 8 == 0) {
+    const int64_t cw0 = a.c0 & ~int64_t(3);
+    dim3 grid(static_cast<unsigned>((a.nsamp + 63) / 64), static_cast<unsigned>((a.c1 - cw0 + 63) / 64));
+    k_prep_u16<<<grid, 256, 0, st>>>(a);
     DD_LAUNCHED();
   } else if (a.out) {
     dim3 grid(static_cast<unsigned>((a.nsamp + 63) / 64), static_cast<unsigned>((a.c1 - a.c0 + 63) / 64));
