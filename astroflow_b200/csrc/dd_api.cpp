@@ -51,7 +51,10 @@ int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 int64_t inter_elem(const dd_plan& P) { return P.inter16 ? 2 : (P.nbits == 32 ? 8 : 4); }
 // Stage 1 of 8-bit samples into 32-bit sums widens its 16-bit lanes every 256
 // sources only when a subband holds more than 257 channels (257 x 255 fits).
-bool stage1_flush(const dd_plan& P) { return P.nbits == 8 && !P.inter16 && P.sbw > 257; }
+// 16-bit samples are always summed into 32-bit lanes (the "wide" variant).
+bool stage1_flush(const dd_plan& P) {
+  return (P.nbits == 8 && !P.inter16 && P.sbw > 257) || P.nbits == 16;
+}
 
 // ---- frequency table and band (dedispered.cu:1003-1031, cpucal.hpp:85-116)
 void build_freq(dd_plan& P) {
@@ -389,7 +392,7 @@ void create_subband(dd_plan& P) {
 void set_brute_window(dd_plan& P) {
   P.winb = 0;
   if (P.p.time_downsample == 1 && P.nbits <= 16) {
-    const int T = sum_variant_tile(P.elem, P.nbits == 8);
+    const int T = sum_variant_tile(P.elem, P.nbits == 8 || P.nbits == 16);
     P.winb = window_bytes(table_spread(P.h_delay, P.dm_steps, P.nc, kSumRows, 0), T, P.elem);
   }
   if (P.winb) upload_desc(P.d_descb, build_sum_desc(P.h_delay, P.dm_steps, P.nc, 0));
@@ -683,7 +686,7 @@ SumLaunch brute_launch(const dd_plan& P, void* output) {
   L.ncols = P.out_cols;
   L.win_bytes = P.winb;
   L.src_bytes = P.elem;
-  L.flush = P.nbits == 8 ? 1 : 0;
+  L.flush = (P.nbits == 8 || P.nbits == 16) ? 1 : 0;  // 8-bit: widened lanes; 16-bit: 32-bit sums
   L.lane_per = 1;
   L.grid_y = static_cast<unsigned>((P.dm_steps + kSumRows - 1) / kSumRows);
   L.grid_z = 1;
@@ -1260,7 +1263,7 @@ void build_groups(dd_batch& B, void* const* outputs) {
     for (auto& list : stage) {
       // one launch per kernel variant; windows too wide for two blocks per SM get
       // their own launch so they do not lower the others' occupancy
-      for (int kind = 0; kind <= kSumKindU32; ++kind)
+      for (int kind = 0; kind < kSumKinds; ++kind)
         for (int wide = 0; wide < 2; ++wide) {
           dd_batch::Launch la;
           la.begin = static_cast<int>(B.groups.size());

@@ -310,15 +310,21 @@ constexpr int kErrWaitEmpty = 2;  // the producer gave up waiting for a free sta
 #define DD_SUM32_MINB 2
 #endif
 constexpr int kSum32NW = DD_SUM32_NW;  // words per lane of the 32-bit staged sum
+#ifndef DD_SUM16W_NW
+#define DD_SUM16W_NW 5
+#endif
+// flush: 8-bit sources widened every 256 sources; 16-bit sources summed into
+// 32-bit lanes (the k_sum_u16w variant).
 inline int sum_variant_tile(int src_bytes, bool flush) {
   return sum_tile_samples(src_bytes, src_bytes == 4   ? kSum32NW
-                                     : src_bytes == 2 ? DD_SUM16_NW
+                                     : src_bytes == 2 ? (flush ? DD_SUM16W_NW : DD_SUM16_NW)
                                                       : (flush ? DD_SUM8F_NW : DD_SUM8_NW));
 }
 // Kernel variant of a staged sum: 8-bit sources into 16-bit sums, 8-bit sources
 // widened to 32 bits (many sources), 8-bit, 16-bit and 32-bit sources.
 enum SumKind { kSumKindU8Out16 = 0, kSumKindU8Flush = 1, kSumKindU8 = 2, kSumKindU16 = 3,
-               kSumKindU32 = 4 };
+               kSumKindU32 = 4, kSumKindU16Wide = 5 };
+constexpr int kSumKinds = 6;
 int sum_kind(const SumLaunch& L);
 unsigned sum_grid_x(const SumLaunch& L);
 // One group of a batched (persistent) launch: all blocks of one staged sum.

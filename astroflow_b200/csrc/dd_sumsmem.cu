@@ -510,6 +510,77 @@ __device__ __forceinline__ void sum_u16(const SumLaunch& L, uint3 blk, uint32_t*
   }
 }
 
+// 16-bit samples into 32-bit sums (stage 1 and brute force of 16-bit input).
+// A 16-bit sample sits in the low or high half of a window word, so no funnel
+// shift is needed: for output word k (samples 2k, 2k+1 of the block) a source
+// whose offset is word-aligned gives (w[k] & 0xffff, w[k] >> 16) and one offset
+// by a sample gives (w[k] >> 16, w[k+1] & 0xffff).  The high halves are taken
+// with a multiply-high on the FMA pipe, the low ones with a mask on the integer
+// pipe, and two sources are added per three-input add.
+template <int RB, int NW>
+__device__ __forceinline__ void sum_u16_wide(const SumLaunch& L, uint3 blk, uint32_t* sw, Pipe& P) {
+  constexpr int T = kWarps * 32 * NW * 2;
+  const Geo g = make_geo(L, T, blk);
+  if (g.nrows <= 0) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr bool kConsec = (NW & 1) != 0;  // lane layout as in k_sum_u8
+  constexpr int kStride = kConsec ? 1 : 32;
+  const int wbase = kConsec ? warp * 32 * NW + lane * NW : warp * 32 * NW + lane;
+  uint32_t lo32[RB][NW], hi32[RB][NW];
+#pragma unroll
+  for (int r = 0; r < RB; ++r)
+#pragma unroll
+    for (int k = 0; k < NW; ++k) lo32[r][k] = hi32[r][k] = 0;
+  run_pipeline<2>(L, g, P, sw, 2 * T, [&](int s, const uint32_t* win) {
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+      const int4 rw = P.row[s][r];
+      const uint32_t* w0 = win + rw.x + wbase;
+      const uint32_t* w1 = win + rw.z + wbase;
+      uint32_t va[NW + 1], vb[NW + 1];
+#pragma unroll
+      for (int i = 0; i <= NW; ++i) {
+        if (kConsec || i < NW) {
+          va[i] = w0[kStride * i];
+          vb[i] = w1[kStride * i];
+        } else {  // interleaved lanes: the word after the last one
+          va[i] = w0[kStride * (NW - 1) + 1];
+          vb[i] = w1[kStride * (NW - 1) + 1];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        const uint32_t an = kConsec ? va[k + 1] : w0[kStride * k + 1];
+        const uint32_t bn = kConsec ? vb[k + 1] : w1[kStride * k + 1];
+        // rw.y / rw.w: 0 (word-aligned) or 16 (one sample in)
+        const uint32_t alo = rw.y ? __umulhi(va[k], 0x10000u) : (va[k] & 0xffffu);
+        const uint32_t ahi = rw.y ? (an & 0xffffu) : __umulhi(va[k], 0x10000u);
+        const uint32_t blo = rw.w ? __umulhi(vb[k], 0x10000u) : (vb[k] & 0xffffu);
+        const uint32_t bhi = rw.w ? (bn & 0xffffu) : __umulhi(vb[k], 0x10000u);
+        lo32[r][k] += alo + blo;
+        hi32[r][k] += ahi + bhi;
+      }
+    }
+  });
+  if (P.failed) return;
+#pragma unroll
+  for (int r = 0; r < RB; ++r) {
+    if (r >= g.nrows) break;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      const int64_t t = static_cast<int64_t>(wbase + kStride * k) * 2;
+      if (t >= g.valid) continue;
+      uint32_t* dst = reinterpret_cast<uint32_t*>(g.out + r * g.out_pitch) + t;
+      if (t + 2 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
+        *reinterpret_cast<uint2*>(dst) = make_uint2(lo32[r][k], hi32[r][k]);
+      } else {
+        dst[0] = lo32[r][k];
+        if (t + 1 < g.valid) dst[1] = hi32[r][k];
+      }
+    }
+  }
+}
+
 // ------------------------------------------------------------------ 32-bit samples
 // Sources of 32-bit words (stage-1 sums stored as uint32): every sample is a whole
 // word, so no shifts; sums wrap modulo 2^32 like the reference's uint32 accumulators.
@@ -561,6 +632,12 @@ __global__ void __launch_bounds__(kThreads, DD_SUM16_MINB) k_sum_u16(SumLaunch L
   sum_u16<RB, NW>(L, blockIdx, sw, P);
 }
 template <int RB, int NW>
+__global__ void __launch_bounds__(kThreads, 2) k_sum_u16w(SumLaunch L) {
+  extern __shared__ __align__(128) uint32_t sw[];
+  __shared__ Pipe P;
+  sum_u16_wide<RB, NW>(L, blockIdx, sw, P);
+}
+template <int RB, int NW>
 __global__ void __launch_bounds__(kThreads, DD_SUM32_MINB) k_sum_u32(SumLaunch L) {
   extern __shared__ __align__(128) uint32_t sw[];
   __shared__ Pipe P;
@@ -601,6 +678,7 @@ __device__ __forceinline__ void run_one(const SumLaunch& L, uint3 blk, uint32_t*
   else if constexpr (KIND == kSumKindU8Flush) sum_u8<kSumRows, DD_SUM8F_NW, false, true>(L, blk, sw, P);
   else if constexpr (KIND == kSumKindU8) sum_u8<kSumRows, DD_SUM8_NW, false, false>(L, blk, sw, P);
   else if constexpr (KIND == kSumKindU16) sum_u16<kSumRows, DD_SUM16_NW>(L, blk, sw, P);
+  else if constexpr (KIND == kSumKindU16Wide) sum_u16_wide<kSumRows, DD_SUM16W_NW>(L, blk, sw, P);
   else sum_u32<kSumRows, kSum32NW>(L, blk, sw, P);
 }
 
@@ -634,6 +712,7 @@ __device__ __forceinline__ void run_kind(int kind, const SumLaunch& L, uint3 blk
     case kSumKindU8Flush: run_one<kSumKindU8Flush>(L, blk, sw, P); break;
     case kSumKindU8: run_one<kSumKindU8>(L, blk, sw, P); break;
     case kSumKindU16: run_one<kSumKindU16>(L, blk, sw, P); break;
+    case kSumKindU16Wide: run_one<kSumKindU16Wide>(L, blk, sw, P); break;
     default: run_one<kSumKindU32>(L, blk, sw, P); break;
   }
 }
@@ -764,6 +843,7 @@ void launch_sum(const SumLaunch& L, cudaStream_t st) {
     case kSumKindU8Flush: launch_k(k_sum_u8<kSumRows, DD_SUM8F_NW, false, true>, grid, smem, L, st); break;
     case kSumKindU8: launch_k(k_sum_u8<kSumRows, DD_SUM8_NW, false, false>, grid, smem, L, st); break;
     case kSumKindU16: launch_k(k_sum_u16<kSumRows, DD_SUM16_NW>, grid, smem, L, st); break;
+    case kSumKindU16Wide: launch_k(k_sum_u16w<kSumRows, DD_SUM16W_NW>, grid, smem, L, st); break;
     default: launch_k(k_sum_u32<kSumRows, kSum32NW>, grid, smem, L, st); break;
   }
 }
@@ -773,7 +853,8 @@ int sum_kind(const SumLaunch& L) {
     if (L.out_elem == 2) return kSumKindU8Out16;
     return L.flush ? kSumKindU8Flush : kSumKindU8;
   }
-  return L.src_bytes == 2 ? kSumKindU16 : kSumKindU32;
+  if (L.src_bytes == 2) return L.flush ? kSumKindU16Wide : kSumKindU16;
+  return kSumKindU32;
 }
 
 unsigned sum_grid_x(const SumLaunch& L) {
@@ -817,6 +898,7 @@ void launch_sum_grouped(const SumBatchGroup* d_groups, int ngroups, long long to
     case kSumKindU8Flush: launch_grouped_k<kSumKindU8Flush>(d_groups, ngroups, total, smem, st); break;
     case kSumKindU8: launch_grouped_k<kSumKindU8>(d_groups, ngroups, total, smem, st); break;
     case kSumKindU16: launch_grouped_k<kSumKindU16>(d_groups, ngroups, total, smem, st); break;
+    case kSumKindU16Wide: launch_grouped_k<kSumKindU16Wide>(d_groups, ngroups, total, smem, st); break;
     default: launch_grouped_k<kSumKindU32>(d_groups, ngroups, total, smem, st); break;
   }
 }
