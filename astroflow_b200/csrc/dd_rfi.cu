@@ -15,7 +15,9 @@
 // multiply-add contraction changes it.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
+#include <cmath>
 #include <cstdint>
 
 #include "dd_internal.h"
@@ -29,23 +31,28 @@ template <> struct Lim<uint16_t> { static constexpr uint64_t vmax = 65535u; };
 template <> struct Lim<uint32_t> { static constexpr uint64_t vmax = 4294967295u; };
 
 // ---------------------------------------------------------------- binning
+// One thread per channel and output sample (grid: channel blocks x output rows,
+// rows strided by gridDim.y); smax_full = sqrt(vmax * ds) of the full bins,
+// evaluated on the host with the same IEEE square root.
 template <typename T>
 __global__ void k_time_binning(const T* __restrict__ in, T* __restrict__ out, int64_t nchans,
-                               int64_t ndata, int ds, int64_t nout) {
-  int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (idx >= nchans * nout) return;
-  int64_t c = idx % nchans;
-  int64_t k = idx / nchans;
-  int64_t t0 = k * ds;
-  int64_t t1 = t0 + ds < ndata ? t0 + ds : ndata;
-  uint64_t sum = 0;
-  for (int64_t t = t0; t < t1; ++t) sum += static_cast<uint64_t>(in[c + t * nchans]);
+                               int64_t ndata, int ds, int64_t nout, double smax_full) {
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= nchans) return;
   const uint64_t vmax = Lim<T>::vmax;
-  uint64_t cnt = static_cast<uint64_t>(t1 - t0);
-  double s = sqrt(static_cast<double>(sum));
-  double smax = sqrt(static_cast<double>(vmax * (cnt ? cnt : 1)));
-  double v = __dmul_rn(__ddiv_rn(s, smax > 0.0 ? smax : 1.0), static_cast<double>(vmax));
-  out[c + k * nchans] = static_cast<T>(v < static_cast<double>(vmax) ? v : static_cast<double>(vmax));
+  for (int64_t k = blockIdx.y; k < nout; k += gridDim.y) {
+    const int64_t t0 = k * ds;
+    const int64_t t1 = t0 + ds < ndata ? t0 + ds : ndata;
+    uint64_t sum = 0;
+    for (int64_t t = t0; t < t1; ++t) sum += static_cast<uint64_t>(in[c + t * nchans]);
+    const uint64_t cnt = static_cast<uint64_t>(t1 - t0);
+    const double s = sqrt(static_cast<double>(sum));
+    const double smax = cnt == static_cast<uint64_t>(ds)
+                            ? smax_full
+                            : sqrt(static_cast<double>(vmax * (cnt ? cnt : 1)));
+    const double v = __dmul_rn(__ddiv_rn(s, smax > 0.0 ? smax : 1.0), static_cast<double>(vmax));
+    out[c + k * nchans] = static_cast<T>(v < static_cast<double>(vmax) ? v : static_cast<double>(vmax));
+  }
 }
 
 // ---------------------------------------------------------------- IQRM sums
@@ -467,12 +474,14 @@ __global__ void k_prep_full(PrepArgs a) {
 void launch_time_binning(const void* in, void* out, int nbits, int64_t ndata, int64_t nchans,
                          int ds, cudaStream_t st) {
   const int64_t nout = (ndata + ds - 1) / ds;
-  const int64_t total = nout * nchans;
-  const unsigned blocks = static_cast<unsigned>((total + 255) / 256);
+  const dim3 grid(static_cast<unsigned>((nchans + 255) / 256),
+                  static_cast<unsigned>(std::min<int64_t>(nout, 65535)));
+  const uint64_t vmax = nbits == 8 ? 255u : nbits == 16 ? 65535u : 4294967295u;
+  const double smax_full = std::sqrt(static_cast<double>(vmax * static_cast<uint64_t>(ds)));
   switch (nbits) {
-    case 8: k_time_binning<uint8_t><<<blocks, 256, 0, st>>>(static_cast<const uint8_t*>(in), static_cast<uint8_t*>(out), nchans, ndata, ds, nout); break;
-    case 16: k_time_binning<uint16_t><<<blocks, 256, 0, st>>>(static_cast<const uint16_t*>(in), static_cast<uint16_t*>(out), nchans, ndata, ds, nout); break;
-    default: k_time_binning<uint32_t><<<blocks, 256, 0, st>>>(static_cast<const uint32_t*>(in), static_cast<uint32_t*>(out), nchans, ndata, ds, nout); break;
+    case 8: k_time_binning<uint8_t><<<grid, 256, 0, st>>>(static_cast<const uint8_t*>(in), static_cast<uint8_t*>(out), nchans, ndata, ds, nout, smax_full); break;
+    case 16: k_time_binning<uint16_t><<<grid, 256, 0, st>>>(static_cast<const uint16_t*>(in), static_cast<uint16_t*>(out), nchans, ndata, ds, nout, smax_full); break;
+    default: k_time_binning<uint32_t><<<grid, 256, 0, st>>>(static_cast<const uint32_t*>(in), static_cast<uint32_t*>(out), nchans, ndata, ds, nout, smax_full); break;
   }
   DD_LAUNCHED();
 }
