@@ -33,7 +33,7 @@ EXPORTS = ("dd_plan_create", "dd_plan_destroy", "dd_plan_destroy_async", "dd_pla
            "dd_batch_run", "dd_batch_status", "dd_batch_get_info", "dd_batch_destroy",
            "dd_stream_open", "dd_stream_push", "dd_stream_get_info", "dd_stream_plan",
            "dd_stream_close", "dd_single_dm_geometry", "dd_single_dm_run",
-           "dd_images", "dd_fil_read_header", "dd_fil_read", "dd_ingest_host",
+           "dd_images", "dd_fil_read_header", "dd_fil_read", "dd_ingest_host", "dd_launch_count",
            "dd_last_error", "dd_abi_version")
 
 
@@ -153,6 +153,7 @@ def load():
                                         ctypes.POINTER(SingleDmInfo)]
     L.dd_single_dm_run.argtypes = [ctypes.POINTER(Header), ctypes.POINTER(SingleDmParams),
                                    ctypes.POINTER(RfiConfig), P, ctypes.c_int32, P, P, P, P]
+    L.dd_launch_count.argtypes = [ctypes.POINTER(ctypes.c_int64)]
     L.dd_images.argtypes = [P, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, P, P,
                             ctypes.c_int32, P, P, P, P]
     L.dd_stream_open.argtypes = [ctypes.POINTER(Header), ctypes.POINTER(PlanParams),
@@ -179,3 +180,10 @@ def check(rc: int) -> None:
     if rc == DD_ERR_NOMEM:
         raise MemoryError(msg)
     raise RuntimeError(msg)
+
+
+def launch_count() -> int:
+    """Kernels the library has launched from the calling thread."""
+    n = ctypes.c_int64()
+    check(load().dd_launch_count(ctypes.byref(n)))
+    return n.value

@@ -379,7 +379,11 @@ void create_subband(dd_plan& P) {
   P.xpitch = round_up(ntiles * L + round_up(L + P.max_res, 8192) + P.max_delay + 8192, 64);
   P.d_x.alloc(static_cast<size_t>(P.dch * P.xpitch) * P.elem);
   DD_CUDA_TRY(cudaMemset(P.d_x.p, 0, P.d_x.bytes));
-  P.d_inter.alloc(static_cast<size_t>(P.ndm_nom * P.nsb * P.tile_pitch) * inter_elem(P));
+#ifndef DD_PAIR_STAGES
+#define DD_PAIR_STAGES 0
+#endif
+  P.inter_bytes = P.ndm_nom * P.nsb * P.tile_pitch * inter_elem(P);
+  P.d_inter.alloc(static_cast<size_t>((DD_PAIR_STAGES ? 2 : 1) * P.inter_bytes));
   DD_CUDA_TRY(cudaMemset(P.d_inter.p, 0, P.d_inter.bytes));
   if (ds > 1 || callsite_zdm_active(P))
     P.d_binned.alloc(static_cast<size_t>(P.nbin * P.hdr.nchans) * P.elem);
@@ -546,7 +550,7 @@ void run_rfi_and_prep(dd_plan& P, const void* input, uint8_t* masks_out, uint32_
 
 // Staged-sum launches of one subband time tile starting at t0 (stage 1: the
 // prepared input into the tile of subband sums; stage 2: the tile into the output).
-SumLaunch stage1_launch(const dd_plan& P, int64_t t0) {
+SumLaunch stage1_launch(const dd_plan& P, int64_t t0, int buf = 0) {
   SumLaunch L{};
   L.mode = SumLaunch::kStage1;
   L.src = static_cast<const char*>(P.d_x.p);
@@ -559,7 +563,7 @@ SumLaunch stage1_launch(const dd_plan& P, int64_t t0) {
   L.group = P.sbw;
   L.rows_per_block = kSumRows;
   L.nsb_out = P.nsb;
-  L.out = static_cast<char*>(P.d_inter.p);
+  L.out = static_cast<char*>(P.d_inter.p) + buf * P.inter_bytes;
   L.out_pitch = P.tile_pitch * inter_elem(P);
   L.out_col0 = 0;
   L.out_elem = static_cast<int>(inter_elem(P));
@@ -578,10 +582,10 @@ SumLaunch stage1_launch(const dd_plan& P, int64_t t0) {
   return L;
 }
 
-SumLaunch stage2_launch(const dd_plan& P, int64_t t0, void* output) {
+SumLaunch stage2_launch(const dd_plan& P, int64_t t0, void* output, int buf = 0) {
   SumLaunch L{};
   L.mode = SumLaunch::kStage2;
-  L.src = static_cast<const char*>(P.d_inter.p);
+  L.src = static_cast<const char*>(P.d_inter.p) + buf * P.inter_bytes;
   L.src_pitch = P.tile_pitch * inter_elem(P);
   L.off = P.d_res.as<int32_t>();
   L.off_pitch = P.nsb;
@@ -619,6 +623,31 @@ void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out
   cudaEvent_t a = pf ? pf->mark() : nullptr;
   run_rfi_and_prep(P, input, masks_out, bounds_out, prepped, st);
   if (pf) pf->prep.emplace_back(a, pf->mark());
+  // With DD_PAIR_STAGES, stage 1 of tile k+1 shares a launch with stage 2 of tile
+  // k (alternating subband-sum buffers).  Measured on B200 at the headline size it
+  // is no faster than running the stages one after another (148.6 vs 145.8 ms per
+  // step), so the default build keeps them apart.
+  if (DD_PAIR_STAGES && !pf && P.win1 && P.win2 && P.nout > P.tile) {
+    const int64_t ntiles = (P.nout + P.tile - 1) / P.tile;
+    launch_sum(stage1_launch(P, 0, 0), st);
+    bool paired = true;
+    for (int64_t k = 1; k <= ntiles; ++k) {
+      const int64_t tprev = (k - 1) * P.tile;
+      const SumLaunch s2 = stage2_launch(P, tprev, output, static_cast<int>((k - 1) & 1));
+      if (k < ntiles) {
+        const SumLaunch s1 = stage1_launch(P, k * P.tile, static_cast<int>(k & 1));
+        if (!(paired = launch_sum_pair(s1, s2, st))) {
+          launch_sum(s2, st);
+          launch_sum(s1, st);
+        }
+      } else {
+        launch_sum(s2, st);
+      }
+      if (after_tile) after_tile(tprev, std::min<int64_t>(P.tile, P.nout - tprev));
+    }
+    (void)paired;
+    return;
+  }
   for (int64_t t0 = 0; t0 < P.nout; t0 += P.tile) {
     cudaEvent_t b1 = pf ? pf->mark() : nullptr;
     if (P.win1) {
@@ -1013,6 +1042,12 @@ int dd_run_ex(dd_plan* P, const void* input, void* output, uint8_t* iqrm_masks,
 
 int dd_run(dd_plan* P, const void* input, void* output, void* stream) {
   return dd_run_ex(P, input, output, nullptr, nullptr, nullptr, stream);
+}
+
+int dd_launch_count(int64_t* count) {
+  if (!count) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  *count = launch_count();
+  return DD_OK;
 }
 
 int dd_run_profiled(dd_plan* P, const void* input, void* output, void* stream,

@@ -111,7 +111,8 @@ struct dd_plan {
   dd::DevBuf d_x;        // prepared channel-major input
   dd::DevBuf d_host_in, d_host_out;  // device side of dd_run_host (kept across calls)
   cudaStream_t copy_stream = nullptr; // dd_run_host: output copies overlapping the sums
-  dd::DevBuf d_inter;    // stage-1 tile
+  dd::DevBuf d_inter;    // stage-1 tile (two buffers in a DD_PAIR_STAGES build)
+  int64_t inter_bytes = 0; // bytes of one buffer
   dd::DevBuf d_stats;    // IQRM sums [nwin][2][csub] uint64
   dd::DevBuf d_iqrm_scratch;
   dd::DevBuf d_masks;    // IQRM window masks [nwin][nchans]
@@ -326,6 +327,9 @@ enum SumKind { kSumKindU8Out16 = 0, kSumKindU8Flush = 1, kSumKindU8 = 2, kSumKin
                kSumKindU32 = 4, kSumKindU16Wide = 5 };
 constexpr int kSumKinds = 6;
 int sum_kind(const SumLaunch& L);
+// Stage 1 of one tile and stage 2 of another in one launch (false: no paired
+// kernel for these variants; nothing launched).
+bool launch_sum_pair(const SumLaunch& L1, const SumLaunch& L2, cudaStream_t st);
 unsigned sum_grid_x(const SumLaunch& L);
 // One group of a batched (persistent) launch: all blocks of one staged sum.
 struct SumBatchGroup {

@@ -892,6 +892,62 @@ void launch_grouped_k(const SumBatchGroup* d_groups, int ngroups, long long tota
   DD_LAUNCHED();
 }
 
+// Two independent staged sums in one launch: stage 1 of time tile k+1 and
+// stage 2 of tile k (different subband-sum buffers).  Stage 1 of 8-bit input is
+// bound by the integer pipe and stage 2 by shared-memory loads; with the blocks
+// of the two interleaved, each SM runs one of each and both units stay busy.
+// Blocks 0, 2, 4, ... take the first sum's blocks in order, 1, 3, 5, ... the
+// second's, and the tail of the longer one follows.
+template <int K1, int K2>
+__global__ void __launch_bounds__(kThreads, 2) k_sum_pair(SumLaunch L1, SumLaunch L2,
+                                                          long long n1, long long n2, unsigned gx1,
+                                                          unsigned gx2) {
+  extern __shared__ __align__(128) uint32_t sw[];
+  __shared__ Pipe P;
+  const long long b = blockIdx.x;
+  const long long m = n1 < n2 ? n1 : n2;
+  int role;
+  long long local;
+  if (b < 2 * m) {
+    role = static_cast<int>(b & 1);
+    local = b >> 1;
+  } else {
+    role = n1 > n2 ? 0 : 1;
+    local = m + (b - 2 * m);
+  }
+  if (role == 0) run_one<K1>(L1, group_block(local, gx1, L1.grid_y), sw, P);
+  else run_one<K2>(L2, group_block(local, gx2, L2.grid_y), sw, P);
+}
+
+template <int K1, int K2>
+void launch_pair_k(const SumLaunch& L1, const SumLaunch& L2, cudaStream_t st) {
+  const unsigned gx1 = sum_grid_x(L1), gx2 = sum_grid_x(L2);
+  const long long n1 = static_cast<long long>(gx1) * L1.grid_y * L1.grid_z;
+  const long long n2 = static_cast<long long>(gx2) * L2.grid_y * L2.grid_z;
+  const size_t smem = std::max(sum_smem_bytes(L1.win_bytes, L1.stages),
+                               sum_smem_bytes(L2.win_bytes, L2.stages));
+  if (n1 + n2 >= (1LL << 31)) throw Error{DD_ERR_RUNTIME, "paired launch too large"};
+  if (smem > 48 * 1024)
+    DD_CUDA_TRY(cudaFuncSetAttribute(k_sum_pair<K1, K2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+  k_sum_pair<K1, K2><<<static_cast<unsigned>(n1 + n2), kThreads, smem, st>>>(L1, L2, n1, n2, gx1, gx2);
+  DD_LAUNCHED();
+}
+
+bool launch_sum_pair(const SumLaunch& L1, const SumLaunch& L2, cudaStream_t st) {
+  for (const SumLaunch* L : {&L1, &L2}) {
+    if (L->stages < 2 || L->stages > kMaxStages || !L->desc || !L->err ||
+        L->rows_per_block != kSumRows)
+      throw Error{DD_ERR_RUNTIME, "bad staged-sum launch"};
+  }
+  const int k1 = sum_kind(L1), k2 = sum_kind(L2);
+  if (k1 == kSumKindU8 && k2 == kSumKindU32) launch_pair_k<kSumKindU8, kSumKindU32>(L1, L2, st);
+  else if (k1 == kSumKindU16Wide && k2 == kSumKindU32) launch_pair_k<kSumKindU16Wide, kSumKindU32>(L1, L2, st);
+  else if (k1 == kSumKindU8Flush && k2 == kSumKindU32) launch_pair_k<kSumKindU8Flush, kSumKindU32>(L1, L2, st);
+  else return false;
+  return true;
+}
+
 void launch_sum_grouped(const SumBatchGroup* d_groups, int ngroups, long long total, int kind,
                         size_t smem, cudaStream_t st) {
   if (total <= 0) return;

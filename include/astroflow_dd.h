@@ -221,6 +221,9 @@ typedef struct dd_run_stats {
   int32_t stage2_launches;
 } dd_run_stats;
 
+/* Kernels this library has launched from the calling thread (monotonic). */
+int dd_launch_count(int64_t* count);
+
 /* dd_run that also fills `stats`; synchronises the stream before returning. */
 int dd_run_profiled(dd_plan* plan, const void* input, void* output, void* stream,
                     dd_run_stats* stats);
