@@ -62,6 +62,16 @@ WORKLOADS = {
         chunk=dict(rfi_frac=0.05, rfi_amp=60.0, impulses=20, imp_amp=50.0,
                    pulses=[(120.0, 0.5, 1e-3, 12.0), (780.0, 1.5, 1e-3, 12.0),
                            (2400.0, 2.5, 1e-3, 12.0)])),
+    # the first range of the 8192-channel 16-bit configuration on 2^18 samples (ncu
+    # captures of the 16-bit stage 1: a few GB on the device)
+    "large-8192ch-u16-2^18-2001dm-subband64-rfi": dict(
+        nchans=8192, nsamp=1 << 18, nbits=16, dm=(0.0, 500.0, 0.25), algorithm="subband",
+        subband_width=64, ds=1, rfi=dict(use_zero_dm=True, use_iqrm=True, use_mask=False,
+                                         iqrm=dict(mode=0, radius_frac=0.1, nsigma=3.0,
+                                                   geofactor=1.5, win_sec=0.0, hop_sec=0.5,
+                                                   include_tail=True)),
+        chunk=dict(rfi_frac=0.08, rfi_amp=6000.0, impulses=20, imp_amp=5000.0,
+                   pulses=[(120.0, 1.0, 1e-3, 1200.0), (400.0, 2.0, 1e-3, 1200.0)])),
     # 1024 ch u8, 2^17 samples, DM 0:1:1000, brute force (the CPU path's semantics)
     "plain-1024ch-u8-2^17-1001dm-brute": dict(
         nchans=1024, nsamp=1 << 17, nbits=8, dm=(0.0, 1000.0, 1.0), algorithm="brute",
