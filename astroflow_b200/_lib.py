@@ -34,6 +34,7 @@ EXPORTS = ("dd_plan_create", "dd_plan_destroy", "dd_plan_destroy_async", "dd_pla
            "dd_stream_open", "dd_stream_push", "dd_stream_get_info", "dd_stream_plan",
            "dd_stream_close", "dd_single_dm_geometry", "dd_single_dm_run",
            "dd_images", "dd_fil_read_header", "dd_fil_read", "dd_ingest_host", "dd_launch_count",
+           "dd_plan_autotune",
            "dd_last_error", "dd_abi_version")
 
 
@@ -99,6 +100,13 @@ class SingleDmInfo(ctypes.Structure):
                 ("freq_end", ctypes.c_float), ("pad", ctypes.c_int32)]
 
 
+class TuneReport(ctypes.Structure):
+    _fields_ = [("candidates", ctypes.c_int64), ("best_budget_bytes", ctypes.c_int64),
+                ("best_tile_samples", ctypes.c_int64), ("best_stages", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("best_ms", ctypes.c_double),
+                ("default_ms", ctypes.c_double)]
+
+
 BATCH_GRAPH = 1
 BATCH_PERSISTENT = 2
 
@@ -154,6 +162,7 @@ def load():
     L.dd_single_dm_run.argtypes = [ctypes.POINTER(Header), ctypes.POINTER(SingleDmParams),
                                    ctypes.POINTER(RfiConfig), P, ctypes.c_int32, P, P, P, P]
     L.dd_launch_count.argtypes = [ctypes.POINTER(ctypes.c_int64)]
+    L.dd_plan_autotune.argtypes = [P, P, P, ctypes.c_int32, P, ctypes.POINTER(TuneReport)]
     L.dd_images.argtypes = [P, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, P, P,
                             ctypes.c_int32, P, P, P, P]
     L.dd_stream_open.argtypes = [ctypes.POINTER(Header), ctypes.POINTER(PlanParams),

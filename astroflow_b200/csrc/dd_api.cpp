@@ -278,6 +278,46 @@ void upload(DevBuf& b, const void* h, size_t bytes) {
   if (bytes) DD_CUDA_TRY(cudaMemcpy(b.p, h, bytes, cudaMemcpyHostToDevice));
 }
 
+
+#ifndef DD_INTER_MB
+#define DD_INTER_MB 2048
+#endif
+#ifndef DD_PAIR_STAGES
+#define DD_PAIR_STAGES 0
+#endif
+// Time tiling of the subband path for a subband-sum budget (bytes per tile): the
+// tile length, the pitches, and the prepared-input and subband-sum buffers
+// (reallocated, zeroed).  Results do not depend on the tiling.
+void set_tiling(dd_plan& P, int64_t budget) {
+  const int64_t kT = tile_samples();
+  // Subband sums: 32-bit words (uint64 for 32-bit samples; uint16 in builds with
+  // DD_INTER32=0).  Tile length L plus the stage-2 halo (max_res) should fill
+  // whole stage-1 block tiles T1: L = n*T1 - R with R the halo rounded to the
+  // base tile; n grows while one tile of subband sums stays within the budget and
+  // the tile is not longer than the chunk.
+  const int64_t per_col = P.ndm_nom * P.nsb * inter_elem(P);
+  const int64_t T1 = P.win1 ? sum_variant_tile(P.elem, stage1_flush(P)) : kT;
+  const int64_t R = round_up(std::max<int64_t>(P.max_res, 1), kT);
+  int64_t n = 1;
+  while (n * T1 - R < kT) ++n;
+  while (((n + 1) * T1 - R) * per_col <= budget && (n * T1 - R) < P.nout) ++n;
+  const int64_t L = std::max<int64_t>(kT, n * T1 - R);
+  P.tile = L;
+  P.inter_budget = budget;
+  // Stage-2 blocks past the tile's last column read up to one block tile beyond it
+  // (their columns are not stored).
+  const int64_t T2 = P.win2 ? sum_variant_tile(static_cast<int>(inter_elem(P)), false) : kT;
+  P.tile_pitch = round_up(round_up(L + P.max_res, kT) + T2 + 64, 64);
+  const int64_t ntiles = (P.nbin + L - 1) / L;
+  P.xpitch = round_up(ntiles * L + round_up(L + P.max_res, 8192) + P.max_delay + 8192, 64);
+  P.d_x.alloc(static_cast<size_t>(P.dch * P.xpitch) * P.elem);
+  DD_CUDA_TRY(cudaMemsetAsync(P.d_x.p, 0, P.d_x.bytes, cudaStreamLegacy));
+  P.inter_bytes = P.ndm_nom * P.nsb * P.tile_pitch * inter_elem(P);
+  P.d_inter.alloc(static_cast<size_t>((DD_PAIR_STAGES ? 2 : 1) * P.inter_bytes));
+  DD_CUDA_TRY(cudaMemsetAsync(P.d_inter.p, 0, P.d_inter.bytes, cudaStreamLegacy));
+  DD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
+}
+
 void create_subband(dd_plan& P) {
   P.sbw = P.p.subband_width > 0 ? P.p.subband_width : 32;
   P.ndm0 = P.p.ndm0 > 0 ? P.p.ndm0 : 32;
@@ -350,41 +390,7 @@ void create_subband(dd_plan& P) {
   }
   if (P.win1) upload_desc(P.d_desc1, build_sum_desc(P.h_delay, P.ndm_nom, P.dch, 0));
   if (P.win2) upload_desc(P.d_desc2, build_sum_desc(P.h_res, P.dm_steps, P.nsb, P.ndm0));
-  const int64_t kT = tile_samples();
-  // Time tile of the stage-1 -> stage-2 pipeline: long enough that the stage-1
-  // halo (max_res extra samples per tile) stays small, short enough that one
-  // tile of subband sums stays below ~1 GiB.
-  // Subband sums: uint16 for 8-bit samples in narrow subbands, else the
-  // reference's accumulator type (uint32, or uint64 for 32-bit samples).
-  const int64_t per_col = P.ndm_nom * P.nsb * inter_elem(P);
-  // Tile length L plus the stage-2 halo (max_res) should fill whole stage-1 block
-  // tiles T1: L = n*T1 - R with R the halo rounded to the base tile.  n grows
-  // while one tile of subband sums stays within 1 GiB and the tile is not
-  // longer than the chunk.
-  const int64_t T1 = P.win1 ? sum_variant_tile(P.elem, stage1_flush(P)) : kT;
-  const int64_t R = round_up(std::max<int64_t>(P.max_res, 1), kT);
-  int64_t n = 1;
-  while (n * T1 - R < kT) ++n;
-#ifndef DD_INTER_MB
-#define DD_INTER_MB 2048
-#endif
-  while (((n + 1) * T1 - R) * per_col <= (int64_t(DD_INTER_MB) << 20) && (n * T1 - R) < P.nout) ++n;
-  int64_t L = std::max<int64_t>(kT, n * T1 - R);
-  P.tile = L;
-  // Stage-2 blocks past the tile's last column read up to one block tile beyond it
-  // (their columns are not stored).
-  const int64_t T2 = P.win2 ? sum_variant_tile(static_cast<int>(inter_elem(P)), false) : kT;
-  P.tile_pitch = round_up(round_up(L + P.max_res, kT) + T2 + 64, 64);
-  const int64_t ntiles = (P.nbin + L - 1) / L;
-  P.xpitch = round_up(ntiles * L + round_up(L + P.max_res, 8192) + P.max_delay + 8192, 64);
-  P.d_x.alloc(static_cast<size_t>(P.dch * P.xpitch) * P.elem);
-  DD_CUDA_TRY(cudaMemset(P.d_x.p, 0, P.d_x.bytes));
-#ifndef DD_PAIR_STAGES
-#define DD_PAIR_STAGES 0
-#endif
-  P.inter_bytes = P.ndm_nom * P.nsb * P.tile_pitch * inter_elem(P);
-  P.d_inter.alloc(static_cast<size_t>((DD_PAIR_STAGES ? 2 : 1) * P.inter_bytes));
-  DD_CUDA_TRY(cudaMemset(P.d_inter.p, 0, P.d_inter.bytes));
+  set_tiling(P, int64_t(DD_INTER_MB) << 20);
   if (ds > 1 || callsite_zdm_active(P))
     P.d_binned.alloc(static_cast<size_t>(P.nbin * P.hdr.nchans) * P.elem);
   P.adds = static_cast<double>(P.ndm_nom) * P.dch * P.nout +
@@ -576,7 +582,7 @@ SumLaunch stage1_launch(const dd_plan& P, int64_t t0, int buf = 0) {
   L.grid_z = static_cast<unsigned>(P.nsb);
   L.desc = P.d_desc1.as<SumDesc>();
   L.desc_pitch = P.dch;
-  L.stages = sum_stages(P.win1);
+  L.stages = P.stages_override ? P.stages_override : sum_stages(P.win1);
   L.err = P.d_err.as<int>();
   L.one = 1;
   return L;
@@ -607,7 +613,7 @@ SumLaunch stage2_launch(const dd_plan& P, int64_t t0, void* output, int buf = 0)
   L.grid_z = 1;
   L.desc = P.d_desc2.as<SumDesc>();
   L.desc_pitch = P.nsb;
-  L.stages = sum_stages(P.win2);
+  L.stages = P.stages_override ? P.stages_override : sum_stages(P.win2);
   L.err = P.d_err.as<int>();
   L.one = 1;
   return L;
@@ -1042,6 +1048,77 @@ int dd_run_ex(dd_plan* P, const void* input, void* output, uint8_t* iqrm_masks,
 
 int dd_run(dd_plan* P, const void* input, void* output, void* stream) {
   return dd_run_ex(P, input, output, nullptr, nullptr, nullptr, stream);
+}
+
+int dd_plan_autotune(dd_plan* P, const void* input, void* output, int32_t reps, void* stream,
+                     dd_tune_report* report) {
+  if (!P || !input || !output || !report) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  return guarded([&] {
+    DeviceGuard g(P->device);
+    if (P->p.algorithm != DD_ALGO_SUBBAND || !P->win1 || !P->win2)
+      throw Error{DD_ERR_UNSUPPORTED, "autotuning covers the staged subband path"};
+    if (reps < 1) throw Error{DD_ERR_INVALID, "reps must be >= 1"};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaEvent_t e0, e1;
+    DD_CUDA_TRY(cudaEventCreate(&e0));
+    DD_CUDA_TRY(cudaEventCreate(&e1));
+    auto time_shape = [&]() -> double {
+      run_subband(*P, input, output, nullptr, nullptr, nullptr, st);  // warm-up
+      DD_CUDA_TRY(cudaEventRecord(e0, st));
+      for (int i = 0; i < reps; ++i) run_subband(*P, input, output, nullptr, nullptr, nullptr, st);
+      DD_CUDA_TRY(cudaEventRecord(e1, st));
+      DD_CUDA_TRY(cudaEventSynchronize(e1));
+      float ms = 0;
+      DD_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+      check_device_error(*P, st);
+      return static_cast<double>(ms) / reps;
+    };
+    // stage counts that keep two blocks per SM for both stages
+    auto fits = [&](int S) {
+      return S >= 2 && S <= kSumMaxStages &&
+             sum_smem_bytes(P->win1, S) <= 113 * 1024 && sum_smem_bytes(P->win2, S) <= 113 * 1024;
+    };
+    const int64_t budget0 = P->inter_budget;
+    const int stages0 = P->stages_override;
+    dd_tune_report rep{};
+    rep.default_ms = time_shape();
+    rep.best_ms = rep.default_ms;
+    rep.best_budget_bytes = budget0;
+    rep.best_tile_samples = P->tile;
+    rep.best_stages = stages0;
+    rep.candidates = 1;
+    std::vector<int64_t> tiles_seen;
+    for (int64_t budget : {int64_t(512) << 20, int64_t(1) << 30, int64_t(2) << 30, int64_t(4) << 30}) {
+      try {
+        set_tiling(*P, budget);
+      } catch (const Error& e) {
+        if (e.code != DD_ERR_NOMEM) throw;
+        continue;  // does not fit: skip
+      }
+      if (std::find(tiles_seen.begin(), tiles_seen.end(), P->tile) != tiles_seen.end()) continue;
+      tiles_seen.push_back(P->tile);
+      for (int S : {0, 4, 6, 8}) {
+        if (S && !fits(S)) continue;
+        if (budget == budget0 && S == stages0) continue;  // the default, timed already
+        P->stages_override = S;
+        const double ms = time_shape();
+        ++rep.candidates;
+        if (ms < rep.best_ms) {
+          rep.best_ms = ms;
+          rep.best_budget_bytes = budget;
+          rep.best_tile_samples = P->tile;
+          rep.best_stages = S;
+        }
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // keep the fastest shape
+    P->stages_override = rep.best_stages;
+    set_tiling(*P, rep.best_budget_bytes);
+    ++P->generation;
+    *report = rep;
+  });
 }
 
 int dd_launch_count(int64_t* count) {

@@ -113,6 +113,8 @@ struct dd_plan {
   cudaStream_t copy_stream = nullptr; // dd_run_host: output copies overlapping the sums
   dd::DevBuf d_inter;    // stage-1 tile (two buffers in a DD_PAIR_STAGES build)
   int64_t inter_bytes = 0; // bytes of one buffer
+  int64_t inter_budget = 0; // subband-sum bytes per time tile the tiling was set for
+  int stages_override = 0;  // staged source pairs in flight (0: as many as fit)
   dd::DevBuf d_stats;    // IQRM sums [nwin][2][csub] uint64
   dd::DevBuf d_iqrm_scratch;
   dd::DevBuf d_masks;    // IQRM window masks [nwin][nchans]
@@ -271,6 +273,10 @@ struct SumLaunch {
   int* err;                // device error word: set when a bounded wait gives up
   unsigned one;            // 1 (a multiplier the compiler cannot fold)
 };
+#ifndef DD_SUM_MAX_STAGES
+#define DD_SUM_MAX_STAGES 8
+#endif
+constexpr int kSumMaxStages = DD_SUM_MAX_STAGES;  // staged source pairs in flight, at most
 void launch_sum(const SumLaunch& L, cudaStream_t st);
 int sum_tile_samples(int src_bytes, int nw);
 // Shared memory of a staged sum with `stages` pairs in flight.

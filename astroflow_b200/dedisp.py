@@ -159,6 +159,23 @@ class Plan:
                                          ctypes.c_void_p(stream.cuda_stream)))
         return out
 
+    def autotune(self, x, out=None, reps: int = 2, stream=None) -> dict:
+        """Choose the launch shape (time tile, staging depth) of the subband path
+        by timing dd_run on this chunk (dd_plan_autotune); results are unchanged."""
+        torch = _torch()
+        if out is None:
+            out = self.empty_output()
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        rep = _lib.TuneReport()
+        L = _lib.load()
+        _lib.check(L.dd_plan_autotune(self._h, x.data_ptr(), out.data_ptr(), int(reps),
+                                      ctypes.c_void_p(stream.cuda_stream), ctypes.byref(rep)))
+        info = _lib.PlanInfo()
+        _lib.check(L.dd_plan_get_info(self._h, ctypes.byref(info)))
+        self.info = {n: getattr(info, n) for n, _ in _lib.PlanInfo._fields_}
+        return {n: getattr(rep, n) for n, _ in _lib.TuneReport._fields_ if n != "pad"}
+
     def run_profiled(self, x, out=None, stream=None) -> dict:
         """Run once and return the device-time breakdown (ms) and launch counts."""
         torch = _torch()

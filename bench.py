@@ -747,6 +747,8 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the plan's default launch shape")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     wl = WORKLOADS[args.workload]
@@ -836,6 +838,10 @@ def main():
     out = plan.empty_output()
     stream = torch.cuda.current_stream(dev)
     units = plan.out_shape[0] * plan.out_shape[1]
+    # launch shape chosen by the library's autotuner on this chunk (untimed; results
+    # do not depend on it)
+    tune = plan.autotune(x, out, reps=1, stream=stream) if (
+        args.autotune and wl["algorithm"] == "subband") else None
     for _ in range(args.warmup):
         plan.run(x, out)
     torch.cuda.synchronize(dev)
@@ -932,6 +938,7 @@ def main():
                 "dtype": f"u{wl['nbits']}", "data": "synthetic (seeded, generated on the GPU)",
                 "config": config, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "e2e_dropin": e2e_dropin, "gpu_launches": launches, "clocks": clk,
+                "autotune": tune,
                 "host_path_matches_device": same}
         print(json.dumps(line))
     dist.close()

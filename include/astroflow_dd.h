@@ -221,6 +221,28 @@ typedef struct dd_run_stats {
   int32_t stage2_launches;
 } dd_run_stats;
 
+/* Autotuner of the subband path's launch shape.  Results do not depend on it:
+ * the time tiling and the staging depth only change how the same sums are
+ * scheduled.  dd_plan_autotune times dd_run of `plan` on the caller's chunk
+ * (device `input`, `output` overwritten) for each candidate pair of subband-sum
+ * budget per time tile (0.5, 1, 2 and 4 GiB, candidates giving the same tile
+ * length skipped) and staged source pairs in flight (4, 6, 8, and as many as
+ * fit; at most what leaves two blocks per SM), `reps` timed runs each after one
+ * warm-up, keeps the fastest and reports it.  Candidates whose buffers do not
+ * fit in device memory are skipped.  Synchronises the stream.  Batches built
+ * from the plan earlier pick the new shape up at their next run. */
+typedef struct dd_tune_report {
+  int64_t candidates;       /* shapes timed */
+  int64_t best_budget_bytes;
+  int64_t best_tile_samples;
+  int32_t best_stages;      /* 0: as many as fit */
+  int32_t pad;
+  double best_ms;           /* mean dd_run time of the chosen shape */
+  double default_ms;        /* mean dd_run time of the shape the plan was built with */
+} dd_tune_report;
+int dd_plan_autotune(dd_plan* plan, const void* input, void* output, int32_t reps, void* stream,
+                     dd_tune_report* report);
+
 /* Kernels this library has launched from the calling thread (monotonic). */
 int dd_launch_count(int64_t* count);
 

@@ -54,7 +54,7 @@ def test_struct_layouts_match_c():
         "dd_plan_params": _lib.PlanParams, "dd_plan_info": _lib.PlanInfo,
         "dd_run_stats": _lib.RunStats, "dd_batch_info": _lib.BatchInfo,
         "dd_stream_info": _lib.StreamInfo, "dd_single_dm_params": _lib.SingleDmParams,
-        "dd_single_dm_info": _lib.SingleDmInfo,
+        "dd_single_dm_info": _lib.SingleDmInfo, "dd_tune_report": _lib.TuneReport,
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for cname, py in structs.items():
