@@ -244,9 +244,16 @@ def bench_batch(args, wl, dist, dev):
                 plan.close()
                 break
             x, _ = make_chunk_device(c.spec, dev)
+            o = plan.empty_output()
+            if args.autotune:  # per-plan launch shape on its own chunk (untimed)
+                try:
+                    plan.autotune(x, o, reps=1, stream=stream)
+                except RuntimeError:  # plans on the direct kernels have no staged shape
+                    pass
+                need += plan.info["workspace_bytes"] - (need - o.numel() * 4 - x.numel() * x.element_size())
             plans.append(plan)
             xs.append(x)
-            outs.append(plan.empty_output())
+            outs.append(o)
             used += need
             i += 1
         units = sum(p.out_shape[0] * p.out_shape[1] for p in plans)
