@@ -149,6 +149,9 @@ struct ImgLaunch {
   int method;
   int target;
   const int32_t* hoff; const int32_t* hidx; const float* hw;
+  // general area, horizontal: per output column its first source column, source
+  // count and weights (first, interior, last); the interior ones are all equal
+  const int32_t* ha_i0; const int32_t* ha_n; const float4* ha_w;
   const int32_t* voff; const int32_t* vidx; const float* vw;
   int ky, kx;           // integer area: block size
   float inv_area;
@@ -176,6 +179,17 @@ __global__ void __launch_bounds__(kImgThreads) k_resize(ImgLaunch L) {
   const int per = (L.target + kImgThreads - 1) / kImgThreads;
   const int v0 = L.voff[dy], v1 = L.voff[dy + 1];
   const int nv = L.method == kAreaInteger ? L.ky : v1 - v0;
+  int a_i0[kMaxPer], a_n[kMaxPer];
+  float4 a_w[kMaxPer];
+  if (L.method == kAreaGeneral) {
+    for (int q = 0; q < per && q < kMaxPer; ++q) {
+      const int dx = threadIdx.x + q * kImgThreads;
+      if (dx >= L.target) break;
+      a_i0[q] = L.ha_i0[dx];
+      a_n[q] = L.ha_n[dx];
+      a_w[q] = L.ha_w[dx];
+    }
+  }
   for (int j = 0; j < nv; ++j) {
     // taps in summation order: Lanczos vertical taps last to first
     const int k = L.method == kLanczos ? v1 - 1 - j : v0 + j;
@@ -196,8 +210,8 @@ __global__ void __launch_bounds__(kImgThreads) k_resize(ImgLaunch L) {
         for (int i = 1; i < L.kx; ++i)
           h = __fadd_rn(h, staged ? row[sx + i] : to_float(L.src, L.elem, base + sx + i));
       } else {
-        const int h0 = L.hoff[dx], h1 = L.hoff[dx + 1];
         if (L.method == kLanczos) {
+          const int h0 = L.hoff[dx], h1 = L.hoff[dx + 1];
           const int sx = L.hidx[h0];
           h = __fmul_rn(staged ? row[sx] : to_float(L.src, L.elem, base + sx), L.hw[h0]);
           for (int e = h0 + 1; e < h1; ++e) {
@@ -205,11 +219,14 @@ __global__ void __launch_bounds__(kImgThreads) k_resize(ImgLaunch L) {
             h = __fadd_rn(h, __fmul_rn(staged ? row[x] : to_float(L.src, L.elem, base + x), L.hw[e]));
           }
         } else {
-          h = 0.0f;
-          for (int e = h0; e < h1; ++e) {
-            const int x = L.hidx[e];
-            h = __fadd_rn(h, __fmul_rn(staged ? row[x] : to_float(L.src, L.elem, base + x), L.hw[e]));
-          }
+          // first, interior and last sources, each product and sum rounded to float
+          const int x0 = a_i0[q], n = a_n[q];
+          const float4 w = a_w[q];
+          h = __fmul_rn(staged ? row[x0] : to_float(L.src, L.elem, base + x0), w.x);
+          for (int i = 1; i < n - 1; ++i)
+            h = __fadd_rn(h, __fmul_rn(staged ? row[x0 + i] : to_float(L.src, L.elem, base + x0 + i), w.y));
+          if (n > 1)
+            h = __fadd_rn(h, __fmul_rn(staged ? row[x0 + n - 1] : to_float(L.src, L.elem, base + x0 + n - 1), w.z));
         }
       }
       if (L.method == kAreaInteger) {
@@ -365,6 +382,25 @@ extern "C" int dd_images(const void* dm_time, int32_t elem_bytes, int64_t nrows,
       L.voff = upload(v.off, st, scratch);
       L.vidx = upload(v.idx, st, scratch);
       L.vw = upload(v.w, st, scratch);
+      if (method == kAreaGeneral) {
+        std::vector<int32_t> i0(static_cast<size_t>(target)), n(static_cast<size_t>(target));
+        std::vector<float4> w(static_cast<size_t>(target));
+        for (int d = 0; d < target; ++d) {
+          const int a = h.off[d], b = h.off[d + 1];
+          if (b <= a) throw Error{DD_ERR_RUNTIME, "empty area cell"};
+          i0[d] = h.idx[a];
+          n[d] = b - a;
+          const float mid = b - a > 2 ? h.w[a + 1] : h.w[a];
+          for (int e = a; e < b; ++e) {
+            if (h.idx[e] != h.idx[a] + (e - a) || (e > a && e < b - 1 && h.w[e] != mid))
+              throw Error{DD_ERR_RUNTIME, "area table is not a contiguous run"};
+          }
+          w[d] = make_float4(h.w[a], mid, h.w[b - 1], 0.0f);
+        }
+        L.ha_i0 = upload(i0, st, scratch);
+        L.ha_n = upload(n, st, scratch);
+        L.ha_w = upload(w, st, scratch);
+      }
       L.ky = static_cast<int>(nrows / target);
       L.kx = static_cast<int>(cols / target);
       L.inv_area = integer ? static_cast<float>(1.0 / (static_cast<double>(L.kx) * L.ky)) : 1.0f;
