@@ -168,7 +168,7 @@ __device__ __forceinline__ float to_float(const void* src, int elem, int64_t i) 
 // brought into shared memory as float (when it fits), then every thread
 // resamples its output columns from it.
 __global__ void __launch_bounds__(kImgThreads) k_resize(ImgLaunch L) {
-  __shared__ float row[kStageFloats];
+  __shared__ __align__(16) float row[kStageFloats];
   const int dy = blockIdx.x;
   const int s = blockIdx.y;
   const int64_t c0 = L.col0[s];
@@ -197,7 +197,19 @@ __global__ void __launch_bounds__(kImgThreads) k_resize(ImgLaunch L) {
     const int64_t base = sy * L.pitch + c0;
     if (staged) {
       __syncthreads();
-      for (int64_t i = threadIdx.x; i < L.cols; i += kImgThreads) row[i] = to_float(L.src, L.elem, base + i);
+      if (L.elem == 4 && (base & 3) == 0) {  // 16-byte loads of four 32-bit sums
+        const uint4* src4 = reinterpret_cast<const uint4*>(static_cast<const uint32_t*>(L.src) + base);
+        const int64_t n4 = L.cols >> 2;
+        for (int64_t i = threadIdx.x; i < n4; i += kImgThreads) {
+          const uint4 v = __ldg(src4 + i);
+          reinterpret_cast<float4*>(row)[i] = make_float4(__uint2float_rn(v.x), __uint2float_rn(v.y),
+                                                          __uint2float_rn(v.z), __uint2float_rn(v.w));
+        }
+        for (int64_t i = 4 * n4 + threadIdx.x; i < L.cols; i += kImgThreads)
+          row[i] = to_float(L.src, L.elem, base + i);
+      } else {
+        for (int64_t i = threadIdx.x; i < L.cols; i += kImgThreads) row[i] = to_float(L.src, L.elem, base + i);
+      }
       __syncthreads();
     }
     for (int q = 0; q < per && q < kMaxPer; ++q) {
