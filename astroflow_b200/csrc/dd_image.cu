@@ -167,7 +167,10 @@ __device__ __forceinline__ float to_float(const void* src, int elem, int64_t i) 
 // One block per (output row, slice).  Each source row the output row needs is
 // brought into shared memory as float (when it fits), then every thread
 // resamples its output columns from it.
-__global__ void __launch_bounds__(kImgThreads) k_resize(ImgLaunch L) {
+#ifndef DD_IMG_MINB
+#define DD_IMG_MINB 3
+#endif
+__global__ void __launch_bounds__(kImgThreads, DD_IMG_MINB) k_resize(ImgLaunch L) {
   __shared__ __align__(16) float row[kStageFloats];
   const int dy = blockIdx.x;
   const int s = blockIdx.y;
