@@ -424,6 +424,125 @@ def single_dm_with_rfi(data: np.ndarray, nchans: int, g: SingleDmGeometry, tsamp
     return single_dm_spectrum(x, nchans, g), x
 
 
+# ---------------------------------------------------------------- image step
+# The reference makes its detector images with OpenCV (include/data.h:620-727):
+# float slice -> cv::resize to 512x512 (INTER_AREA when both dimensions exceed the
+# target, else INTER_LANCZOS4) -> cv::normalize MINMAX to uint8 -> viridis.  These
+# numpy restatements fix the float arithmetic the GPU kernels (dd_images) follow;
+# tests/test_image_oracle_cpu.py checks them against cv2 bit for bit.
+def _area_cells(ssize: int, dsize: int):
+    """Per output index: [(source index, weight)] of the area resize (overlap of the
+    output cell with each source pixel over the cell width; overlaps under 1e-3
+    of a pixel dropped; the last cell clipped to the source)."""
+    import math
+    scale = ssize / dsize
+    cells = []
+    for d in range(dsize):
+        f1 = d * scale
+        f2 = f1 + scale
+        cw = min(scale, ssize - f1)
+        s1 = min(math.ceil(f1), ssize - 1)
+        s2 = min(math.floor(f2), ssize - 1)
+        e = []
+        if s1 - f1 > 1e-3:
+            e.append((s1 - 1, np.float32((s1 - f1) / cw)))
+        for x in range(s1, s2):
+            e.append((x, np.float32(1.0 / cw)))
+        if f2 - s2 > 1e-3:
+            e.append((s2, np.float32(min(min(f2 - s2, 1.0), cw) / cw)))
+        cells.append(e)
+    return cells
+
+
+def resize_area(src: np.ndarray, dh: int = 512, dw: int = 512) -> np.ndarray:
+    """General-scale area resize of float32 `src`: horizontal sums in increasing
+    source column, then vertical sums in increasing source row, every product and
+    sum rounded to float."""
+    src = np.asarray(src, np.float32)
+    R, C = src.shape
+    h = np.zeros((R, dw), np.float32)
+    for dx, cell in enumerate(_area_cells(C, dw)):
+        acc = np.zeros(R, np.float32)
+        for x, w in cell:
+            acc = (acc + src[:, x] * w).astype(np.float32)
+        h[:, dx] = acc
+    out = np.zeros((dh, dw), np.float32)
+    for dy, cell in enumerate(_area_cells(R, dh)):
+        acc = np.zeros(dw, np.float32)
+        for y, w in cell:
+            acc = (acc + h[y] * w).astype(np.float32)
+        out[dy] = acc
+    return out
+
+
+def _lanczos4_taps(ssize: int, dsize: int):
+    """Per output index: 8 clamped source indices and float weights of the
+    Lanczos-4 resize (weights in double through the angle-addition form of
+    sin(pi x) sin(pi x / 4) / x^2, rounded to float, times the float reciprocal of
+    their float sum)."""
+    import math
+    F = np.float32
+    r = math.sqrt(0.5)
+    rot = [(1, 0), (-r, -r), (0, 1), (r, -r), (-1, 0), (r, r), (0, -1), (-r, r)]
+    scale = ssize / dsize
+    idx = np.zeros((dsize, 8), np.int64)
+    wts = np.zeros((dsize, 8), np.float32)
+    for d in range(dsize):
+        f = F((d + 0.5) * scale - 0.5)
+        s = int(math.floor(f))
+        t = float(F(f - F(s)))
+        if t < np.finfo(np.float32).eps:
+            w = np.zeros(8, np.float32)
+            w[3] = 1
+        else:
+            a0 = -(t + 3) * math.pi * 0.25
+            s0, c0 = math.sin(a0), math.cos(a0)
+            w = np.array([(rot[i][0] * s0 + rot[i][1] * c0) / ((-(t + 3 - i) * math.pi * 0.25) ** 2)
+                          for i in range(8)]).astype(np.float32)
+            tot = F(0)
+            for v in w:
+                tot = F(tot + v)
+            w = (w * F(F(1) / tot)).astype(np.float32)
+        idx[d] = [min(max(s - 3 + i, 0), ssize - 1) for i in range(8)]
+        wts[d] = w
+    return idx, wts
+
+
+def resize_lanczos4(src: np.ndarray, dh: int = 512, dw: int = 512) -> np.ndarray:
+    """Lanczos-4 resize: horizontal taps summed first to last, vertical taps last
+    to first, every product and sum rounded to float."""
+    src = np.asarray(src, np.float32)
+    R, C = src.shape
+    ix, cx = _lanczos4_taps(C, dw)
+    iy, cy = _lanczos4_taps(R, dh)
+    h = np.zeros((R, dw), np.float32)
+    for dx in range(dw):
+        acc = (src[:, ix[dx, 0]] * cx[dx, 0]).astype(np.float32)
+        for k in range(1, 8):
+            acc = (acc + (src[:, ix[dx, k]] * cx[dx, k]).astype(np.float32)).astype(np.float32)
+        h[:, dx] = acc
+    out = np.zeros((dh, dw), np.float32)
+    for dy in range(dh):
+        acc = (h[iy[dy, 7]] * cy[dy, 7]).astype(np.float32)
+        for k in range(6, -1, -1):
+            acc = (acc + (h[iy[dy, k]] * cy[dy, k]).astype(np.float32)).astype(np.float32)
+        out[dy] = acc
+    return out
+
+
+def normalize_u8(img: np.ndarray) -> np.ndarray:
+    """MINMAX to [0, 255] as uint8: scale = 255 / (max - min) in double (0 for a
+    flat image), shift = -min * scale, round-half-even(fma(x, (float)scale,
+    (float)shift)) clamped."""
+    img = np.asarray(img, np.float32)
+    mn, mx = float(img.min()), float(img.max())
+    d = mx - mn
+    scale = 255.0 / d if d > np.finfo(np.float64).eps else 0.0
+    shift = 0.0 - mn * scale
+    v = (img.astype(np.float64) * float(np.float32(scale)) + float(np.float32(shift))).astype(np.float32)
+    return np.clip(np.rint(v), 0, 255).astype(np.uint8)
+
+
 # ---------------------------------------------------------------- reference builds
 _ref_cpu = None
 
