@@ -201,6 +201,19 @@ class Spectrum32(_Spectrum):
     pass
 
 
+def _fma_table(fch1: float, foff: float, n: int) -> np.ndarray:
+    """fch1 + i*foff for i < n in double with one rounding (C fma), as the
+    reference's reader computes it once its build (-Ofast with FMA) contracts the
+    expression (src/data/filterbank.cpp:445-449)."""
+    import ctypes
+    import ctypes.util
+
+    libm = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
+    libm.fma.restype = ctypes.c_double
+    libm.fma.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    return np.array([libm.fma(float(i), float(foff), float(fch1)) for i in range(n)], np.float64)
+
+
 # ------------------------------------------------------------------ SIGPROC reader
 class Filterbank:
     """SIGPROC filterbank reader with the reference's behaviour
@@ -273,7 +286,7 @@ class Filterbank:
             self.fch1 = self.foff = 0.0
             self.frequency_table = np.asarray(table, np.float64)
         else:
-            self.frequency_table = self.fch1 + np.arange(self.nchans, dtype=np.float64) * self.foff
+            self.frequency_table = _fma_table(self.fch1, self.foff, self.nchans)
         dt = {8: np.uint8, 16: np.uint16, 32: np.uint32}.get(self.nbits)
         if dt is None:
             raise RuntimeError(f"Unsupported nbits value: {self.nbits}")

@@ -52,8 +52,11 @@ int64_t inter_elem(const dd_plan& P) { return P.inter16 ? 2 : (P.nbits == 32 ? 8
 // Stage 1 of 8-bit samples into 32-bit sums widens its 16-bit lanes every 256
 // sources only when a subband holds more than 257 channels (257 x 255 fits).
 // 16-bit samples are always summed into 32-bit lanes (the "wide" variant).
+#ifndef DD_SUM16_WIDE
+#define DD_SUM16_WIDE 1
+#endif
 bool stage1_flush(const dd_plan& P) {
-  return (P.nbits == 8 && !P.inter16 && P.sbw > 257) || P.nbits == 16;
+  return (P.nbits == 8 && !P.inter16 && P.sbw > 257) || (P.nbits == 16 && DD_SUM16_WIDE);
 }
 
 // ---- frequency table and band (dedispered.cu:1003-1031, cpucal.hpp:85-116)
@@ -64,18 +67,19 @@ void build_freq(dd_plan& P) {
     if (P.p.freq_table) {
       P.freq.assign(P.p.freq_table, P.p.freq_table + n);
     } else {
-      // src/data/filterbank.cpp:445-449, in double.
+      // src/data/filterbank.cpp:445-449, in double; the reference build (-Ofast
+      // with FMA) contracts fch1 + i*foff into a fused multiply-add.
       const double f1 = P.hdr.fch1, fo = P.hdr.foff;
-      for (int i = 0; i < n; ++i) P.freq[i] = f1 + static_cast<double>(i) * fo;
+      for (int i = 0; i < n; ++i) P.freq[i] = std::fma(static_cast<double>(i), fo, f1);
     }
   } else {
-    // dedispered.cu:1004-1005: header.fch1 + i*header.foff in float.
+    // dedispered.cu:1004-1005: header.fch1 + i*header.foff in float, contracted into a
+    // fused multiply-add by the reference build (-ffast-math with FMA); with separate
+    // roundings about one channel in ten lands one float step away, which moves
+    // delays that sit at a rounding tie.
     const float f1 = static_cast<float>(P.hdr.fch1), fo = static_cast<float>(P.hdr.foff);
-    for (int i = 0; i < n; ++i) {
-      volatile float prod = static_cast<float>(static_cast<size_t>(i)) * fo;
-      volatile float f = f1 + prod;
-      P.freq[i] = static_cast<double>(f);
-    }
+    for (int i = 0; i < n; ++i)
+      P.freq[i] = static_cast<double>(std::fmaf(static_cast<float>(static_cast<size_t>(i)), fo, f1));
   }
   for (int i = 1; i < n; ++i)
     if (!(P.freq[i] > P.freq[i - 1]))

@@ -137,7 +137,8 @@ ParsedHeader parse_header(const char* path) {
     throw Error{DD_ERR_INVALID, "Only supports nifs == 1 in reverse_channanl_data"};
   if (!use_table) {
     P.table.resize(static_cast<size_t>(nchans));
-    for (int32_t i = 0; i < nchans; ++i) P.table[i] = fch1 + static_cast<double>(i) * foff;
+    // fch1 + i*foff, which the reference build contracts into a fused multiply-add
+    for (int32_t i = 0; i < nchans; ++i) P.table[i] = std::fma(static_cast<double>(i), foff, fch1);
   }
   if (h.flipped) {
     std::reverse(P.table.begin(), P.table.end());

@@ -68,7 +68,7 @@ Geometry geometry(const dd_header& h, const dd_single_dm_params& q) {
     if (fil && q.freq_table) {
       freq[i] = static_cast<float>(q.freq_table[i]);
     } else if (fil) {
-      freq[i] = static_cast<float>(h.fch1 + static_cast<double>(i) * h.foff);
+      freq[i] = static_cast<float>(std::fma(static_cast<double>(i), h.foff, h.fch1));
     } else {
       freq[i] = std::fmaf(static_cast<float>(i), static_cast<float>(h.foff), static_cast<float>(h.fch1));
     }

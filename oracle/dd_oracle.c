@@ -40,16 +40,14 @@ static inline uint64_t vmax_of(int nbits) {
 /* dedispered.cu:1003-1005: h_freq[i] = header.fch1 + i*header.foff, evaluated in
  * float (Header's fields are float, data.h:24-31) and stored as double. */
 void orc_freq_table_header(float fch1, float foff, int nchans, double* freq) {
-  for (int i = 0; i < nchans; ++i) {
-    float fi = (float)(size_t)i;
-    float prod = fi * foff;
-    freq[i] = (double)(fch1 + prod);
-  }
+  /* the reference build (-ffast-math, FMA) contracts fch1 + i*foff into one fmaf */
+  for (int i = 0; i < nchans; ++i) freq[i] = (double)fmaf((float)(size_t)i, foff, fch1);
 }
 
 /* src/data/filterbank.cpp:445-449: frequency_table[i] = fch1 + i*foff in double. */
 void orc_freq_table_fil(double fch1, double foff, int nchans, double* freq) {
-  for (int i = 0; i < nchans; ++i) freq[i] = fch1 + (double)i * foff;
+  /* contracted into fma by the reference build (-Ofast with FMA) */
+  for (int i = 0; i < nchans; ++i) freq[i] = fma((double)i, foff, fch1);
 }
 
 /* dedispered.cu:1007-1027 (also cpucal.hpp:85-110 and dedispered.cu:529-548):

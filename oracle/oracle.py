@@ -340,7 +340,7 @@ def single_dm_geometry(nchans, ndata, tsamp, fch1, foff, tstart, tend, dm, freq_
         raise ValueError("tend must be > tstart")
     if fil:
         tbl = (np.asarray(freq_table, np.float64) if freq_table is not None
-               else fch1 + np.arange(nchans, dtype=np.float64) * foff)
+               else np.array([_fma_f64(i, foff, fch1) for i in range(nchans)], np.float64))
         freq = tbl.astype(np.float32)
         t0, t1 = int(float(tstart) / tsamp), int(float(tend) / tsamp)
     else:

@@ -112,6 +112,13 @@ SUB = [
     (128, 3333, 8, 64e-6, 1400.0, 200.0, 0.0, 500.0, 1.0, 1, 64, (0.0, 0.5)),
     (256, 4096, 32, 64e-6, 1500.0, 400.0, 0.0, 400.0, 1.0, 1, 32, None),
     (96, 3000, 32, 1e-4, 1450.0, 300.0, 3.0, 600.0, 0.9, 2, 16, (0.1, 0.8)),
+    # edges: channel counts off the 4-sample word (the layout kernels' general path),
+    # an odd chunk length, a single DM trial, a chunk far shorter than the largest
+    # delay with a binning tail, and a subband width that is not a power of two
+    (251, 3001, 8, 49.152e-6, 1500.0, 400.0, 0.0, 150.0, 1.0, 1, 32, None),
+    (250, 2048, 16, 1e-4, 1500.0, 500.0, 100.0, 100.0, 1.0, 1, 16, None),
+    (97, 1501, 8, 64e-6, 1450.0, 300.0, 0.0, 2000.0, 5.0, 4, 16, None),
+    (130, 2500, 8, 64e-6, 1400.0, 200.0, 0.0, 300.0, 1.0, 1, 20, (0.05, 0.95)),
 ]
 
 
@@ -183,6 +190,8 @@ RFI = [
     (300, 6000, 8, 1, (0.1, 0.95), (1, 0.05, 2.5, 0.05, 0.03)),
     (512, 4096, 16, 1, None, (1, 0.02, 3.0, 0.0, 2.5)),
     (160, 9000, 8, 3, (0.3, 1.0), (0, 0.2, 4.0, 0.1, 0.1)),
+    (301, 5001, 8, 1, None, (0, 0.1, 3.0, 0.0, 0.0)),
+    (254, 4001, 16, 1, (0.0, 0.9), (1, 0.1, 3.0, 0.0, 0.0)),
 ]
 
 
@@ -297,3 +306,45 @@ def test_multi_range_plan_matches_reference_calls_per_range():
                                         sb_width=64, use_zero_dm=True, use_iqrm=True, iq=iq)
         assert np.array_equal(to_np(o), ref), f"range {lo}-{hi}"
     mp.close()
+
+
+def test_delay_tables_match_reference_on_random_plans():
+    """Subband delay and residual tables of 40 seeded random plans (bands, DM
+    grids, downsampling, subband widths) against the reference GPU build's own
+    tables, entry for entry.  Frequencies whose float fch1 + i*foff the reference
+    build fuses into one multiply-add put a few delays on the other side of a
+    rounding tie when evaluated with two roundings; this sweep catches that."""
+    rng = np.random.default_rng(12)
+    checked = 0
+    for _ in range(40):
+        nchans = int(rng.choice([128, 254, 256, 300, 512, 1000, 4096]))
+        N = int(rng.integers(2000, 20000))
+        tsamp = float(F32(rng.choice([49.152e-6, 64e-6, 1e-4])))
+        fhi, bw = float(rng.uniform(1300, 1500)), float(rng.uniform(100, 500))
+        foff = float(F32(bw / nchans))
+        fch1 = float(F32(fhi - (nchans - 1) * foff))
+        freq = O.freq_table_header(fch1, foff, nchans)
+        a, b = sorted(rng.uniform(0, 1, 2))
+        b = min(max(b, a + 0.2), 1.0)
+        fs = float(F32(freq[0] + a * (freq[-1] - freq[0])))
+        fe = float(F32(freq[0] + b * (freq[-1] - freq[0])))
+        lo = float(rng.choice([0.0, 3.0, 10.5]))
+        hi = lo + float(rng.uniform(50, 1500))
+        step = float(rng.choice([0.25, 0.5, 1.0, 2.0]))
+        ds, sbw = int(rng.choice([1, 2, 4])), int(rng.choice([16, 32, 64]))
+        if not O.ref_gpu_available(sbw):
+            continue
+        hdr = dict(tsamp=tsamp, fch1=fch1, foff=foff, nbits=8, nchans=nchans, ndata=N)
+        try:
+            plan = Plan(hdr, lo, hi, fs, fe, step, ds, algorithm="subband", subband_width=sbw)
+        except ValueError:  # a plan the reference would refuse as well
+            continue
+        d1, r2 = plan.tables()
+        d1r, r2r, _ = O.ref_gpu_tables(nchans, N, tsamp, fch1, foff, lo, hi, fs, fe, step, ds,
+                                       sb_width=sbw)
+        np.testing.assert_array_equal(d1, d1r)
+        np.testing.assert_array_equal(r2, r2r)
+        plan.close()
+        checked += 1
+    if checked == 0:
+        pytest.skip("reference GPU builds absent")
