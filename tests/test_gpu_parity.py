@@ -348,3 +348,40 @@ def test_delay_tables_match_reference_on_random_plans():
         checked += 1
     if checked == 0:
         pytest.skip("reference GPU builds absent")
+
+
+def test_full_call_with_rfi_matches_reference_on_random_chunks(tmp_path):
+    """Seeded random chunks through the whole plain call (binning, IQRM window
+    masks, zero-DM, mask file, both subband stages) against the reference GPU
+    call on the same input: IQRM masks and the raw DM-time sums bit for bit."""
+    if not O.ref_gpu_available(32):
+        pytest.skip("reference GPU build absent")
+    rng = np.random.default_rng(31)
+    for it in range(8):
+        nchans = int(rng.choice([128, 254, 300, 512]))
+        N = int(rng.integers(3000, 9000))
+        nbits = int(rng.choice([8, 16]))
+        ds = int(rng.choice([1, 2]))
+        band = None if it % 2 else (float(rng.uniform(0, 0.2)), float(rng.uniform(0.8, 1.0)))
+        iqp = (int(rng.integers(0, 2)), float(rng.uniform(0.02, 0.15)), float(rng.uniform(2.0, 4.0)),
+               float(rng.choice([0.0, 0.1])), float(rng.choice([0.0, 0.05])))
+        case = (nchans, N, nbits, ds, band, iqp)
+        x, hdr, freq, fs, fe, iq = rfi_setup(case, seed=100 + it)
+        bad = sorted(int(b) for b in rng.choice(nchans, size=4, replace=False))
+        mask_file = str(tmp_path / f"m{it}.txt")
+        with open(mask_file, "w") as fh:
+            fh.write(" ".join(str(b) for b in bad) + "\n")
+        hi = float(rng.uniform(100, 400))
+        ref_out = O.ref_gpu_dedisperse_spec(x, nchans, hdr["tsamp"], hdr["fch1"], hdr["foff"], 0.0,
+                                            hi, fs, fe, 1.0, ds, mask_file=mask_file,
+                                            use_mask=True, use_zero_dm=True, use_iqrm=True, iq=iq)
+        ref_x, t0, t1, ref_masks = O.ref_gpu_rfi(x, nchans, hdr["tsamp"], hdr["fch1"], hdr["foff"],
+                                                 fs, fe, ds, mask_file=mask_file, use_mask=True,
+                                                 use_zero_dm=True, use_iqrm=True, iq=iq)
+        plan = Plan(hdr, 0.0, hi, fs, fe, 1.0, ds, algorithm="subband",
+                    rfi=RfiParams(use_mask=True, use_zero_dm=True, use_iqrm=True, iqrm=iq),
+                    bad_channels=bad)
+        out, masks, bounds, prepped = run_prepped(plan, x, nchans)
+        np.testing.assert_array_equal(masks, ref_masks, err_msg=f"chunk {it}: IQRM masks")
+        np.testing.assert_array_equal(prepped, ref_x, err_msg=f"chunk {it}: RFI-processed input")
+        np.testing.assert_array_equal(out, ref_out, err_msg=f"chunk {it}: DM-time sums")
