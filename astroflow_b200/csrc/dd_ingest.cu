@@ -295,6 +295,7 @@ void run_transfer(const Transfer& T, cudaStream_t caller) {
     std::lock_guard<std::mutex> g(err_mu);
     if (!failed.exchange(1)) first_error = m;
   };
+  std::vector<std::thread> threads;
   try {
     for (int w = 0; w < nw; ++w) {
       DD_CUDA_TRY(cudaStreamCreateWithFlags(&streams[w], cudaStreamNonBlocking));
@@ -305,7 +306,6 @@ void run_transfer(const Transfer& T, cudaStream_t caller) {
           DD_CUDA_TRY(cudaMallocAsync(&dstage[w * kBuffersPerWorker + k], kBlockBytes, streams[w]));
       }
     }
-    std::vector<std::thread> threads;
     for (int w = 0; w < nw; ++w) {
       threads.emplace_back([&, w]() {
         cudaSetDevice(dev);
@@ -345,10 +345,13 @@ void run_transfer(const Transfer& T, cudaStream_t caller) {
         }
       });
     }
-    for (auto& t : threads) t.join();
   } catch (const Error& e) {
     fail(e.msg);
+  } catch (const std::exception& e) {  // e.g. a worker thread that could not start
+    fail(e.what());
   }
+  for (auto& t : threads)
+    if (t.joinable()) t.join();
   // order the caller's stream after every block, then release the workers' resources
   for (int w = 0; w < nw; ++w) {
     if (!streams[w]) continue;
