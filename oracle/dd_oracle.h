@@ -1,7 +1,7 @@
 /* ORACLE — test infrastructure, not product code.
  *
  * CPU restatement of astroflow's dedispersion hot path, used only as the
- * checker by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg.
+ * parity reference by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg.
  * The product (astroflow_b200) never links, loads or calls anything here.
  *
  * Parity pin: every function is checked against the reference's own code

@@ -3,7 +3,7 @@
 ctypes front end for the CPU restatement (liboracle.so, built from dd_oracle.c)
 and for the reference's own code built from source (oracle/_ref/libref_cpu.so,
 oracle/_ref/libref_gpu_sb<W>.so).  Only tests/, __graft_entry__.smoke() and
-bench.py's cpu_baseline / reference legs import this module, as the checker.
+bench.py's cpu_baseline / reference legs import this module, as the parity reference.
 """
 from __future__ import annotations
 

@@ -1,5 +1,5 @@
 // Stand-in for the reference's include/data.h, used ONLY when the reference's
-// own dedispersion sources are compiled as a checker (oracle/_ref).  It is test
+// own dedispersion sources are compiled as a parity reference (oracle/_ref).  It is test
 // infrastructure, never part of the product.
 //
 // It declares the same container types as include/data.h:24-163 (Header,
@@ -9,7 +9,7 @@
 // (OpenCV slice -> resize -> normalize -> viridis) is replaced by a capture of
 // the raw integer DM-time arrays, which is what the parity tests compare.
 // AF_DEBUG (include/data.h:22) is left undefined, so the reference's debug
-// timers and the synchronisations they add are off in the checker build; the
+// timers and the synchronisations they add are off in the parity build; the
 // timing build (oracle/Makefile, libref_gpu_timed_*) defines it to print the
 // reference's own per-stage timers, and REF_CAPTURE_DIMS_ONLY to skip the
 // host copy of the sums.
@@ -88,7 +88,7 @@ template <typename OutputType> struct DedispersedDataTyped {
   std::string filname;
 };
 
-// ---- capture sink (checker only) -----------------------------------------
+// ---- capture sink (parity builds only) ------------------------------------
 // Each raw array handed to the post-process is kept alive here, widened to
 // uint64, together with its number of rows and columns.
 struct RefCapture {
