@@ -5,13 +5,13 @@ returning to Python: include/data.h:620-727 (the GPU paths: cut the columns into
 slices of t_sample seconds) and include/data.h:299-369 (the CPU path: one image
 per slice it already produced).  Each image is: uint sums -> float32, resize to
 512x512 (INTER_AREA when both dimensions exceed 512, else INTER_LANCZOS4),
-min-max normalise to uint8, gray -> RGB, COLORMAP_VIRIDIS.  This module does the
-same with OpenCV's Python binding on the host (slice_images, images) and on the
-GPU through dd_images (device_slice_images, device_images): the GPU form resizes,
-normalises and colors in device memory and copies only the images to the host.
+min-max normalise to uint8, gray -> RGB, COLORMAP_VIRIDIS.  Here the GPU does all
+of it through dd_images (device_slice_images, device_images): it resizes,
+normalises and colors in device memory, and only the images come to the host.
 """
 from __future__ import annotations
 
+import threading
 from concurrent.futures import ThreadPoolExecutor
 from typing import List, Optional, Sequence
 
@@ -20,41 +20,10 @@ import numpy as np
 TARGET = 512
 
 
-def _image(block: np.ndarray, target: int = TARGET) -> np.ndarray:
-    import cv2
-
-    f = np.ascontiguousarray(block, dtype=np.float32)
-    rows, cols = f.shape
-    interp = cv2.INTER_AREA if (rows > target and cols > target) else cv2.INTER_LANCZOS4
-    resized = cv2.resize(f, (target, target), interpolation=interp)
-    norm = cv2.normalize(resized, None, 0, 255, cv2.NORM_MINMAX, cv2.CV_8U)
-    rgb = cv2.cvtColor(norm, cv2.COLOR_GRAY2RGB)
-    return np.ascontiguousarray(cv2.applyColorMap(rgb, cv2.COLORMAP_VIRIDIS))
-
-
 def samples_per_slice(tsamp: float, time_downsample: int, slice_duration: float) -> int:
-    """include/data.h:640-643: (size_t)(slice_duration / (tsamp * time_downsample)) in float."""
+    """include/data.h:645-647: (size_t)(slice_duration / (tsamp * time_downsample)) in float."""
     ts = np.float32(np.float32(tsamp) * np.float32(time_downsample))
     return int(np.float32(slice_duration) / ts)
-
-
-def slice_images(raw: np.ndarray, tsamp: float, time_downsample: int, slice_duration: float,
-                 threads: int = 16) -> List[np.ndarray]:
-    """Images of consecutive column slices of raw [dm, time] sums (include/data.h:620-727)."""
-    sps = samples_per_slice(tsamp, time_downsample, slice_duration)
-    if sps <= 0:
-        raise ValueError("t_sample is shorter than one (downsampled) sample")
-    cols = raw.shape[1]
-    n = (cols + sps - 1) // sps
-    blocks = [raw[:, i * sps:min((i + 1) * sps, cols)] for i in range(n)]
-    with ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
-        return list(ex.map(_image, blocks))
-
-
-def images(blocks: Sequence[np.ndarray], threads: int = 16) -> List[np.ndarray]:
-    """One image per block (include/data.h:299-369)."""
-    with ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
-        return list(ex.map(_image, blocks))
 
 
 _LUT: Optional[np.ndarray] = None
@@ -117,20 +86,47 @@ def slice_bounds(cols: int, sps: int):
     return starts, [min(sps, cols - s) for s in starts]
 
 
+# One pinned block, kept for the life of the process and grown on demand, through
+# which images come to the host: pinning a fresh block per call (the returned
+# arrays outlive the call) cost 80-700 ms for 82 MB of images on a busy host, a
+# copy from the device into pageable memory about 35 ms.
+_STAGE = None
+_STAGE_LOCK = threading.Lock()
+_COPY_POOL: Optional[ThreadPoolExecutor] = None
+
+
 def to_host_images(dev_imgs) -> List[np.ndarray]:
-    """One device-to-host copy of [n, t, t, 3] images into pinned memory, returned
-    as n arrays (views that keep the pinned block alive)."""
+    """[n, t, t, 3] device images as n host arrays (views of one new block): one
+    device-to-host copy into the pinned staging block, then a parallel host copy
+    into the returned block."""
     import torch
 
-    host = torch.empty(tuple(dev_imgs.shape), dtype=dev_imgs.dtype, pin_memory=True)
-    host.copy_(dev_imgs)
-    h = host.numpy()
-    return [h[i] for i in range(h.shape[0])]
+    global _STAGE, _COPY_POOL
+    if dev_imgs.dtype != torch.uint8:
+        raise ValueError("images must be uint8")
+    n = int(dev_imgs.shape[0])
+    if n == 0:
+        return []
+    out = np.empty(tuple(dev_imgs.shape), np.uint8)
+    nbytes = dev_imgs.numel() * dev_imgs.element_size()
+    with _STAGE_LOCK:
+        if _STAGE is None or _STAGE.numel() < nbytes:
+            _STAGE = None
+            _STAGE = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        if _COPY_POOL is None:
+            _COPY_POOL = ThreadPoolExecutor(max_workers=8)
+        stage = _STAGE[:nbytes].view(tuple(dev_imgs.shape))
+        stage.copy_(dev_imgs.contiguous())  # synchronous: returns once the bytes are on the host
+        src = stage.numpy()
+        step = max(1, (n + 7) // 8)
+        list(_COPY_POOL.map(lambda i: np.copyto(out[i:i + step], src[i:i + step]),
+                            range(0, n, step)))
+    return [out[i] for i in range(n)]
 
 
 def device_slice_images(out, tsamp: float, time_downsample: int,
                         slice_duration: float) -> List[np.ndarray]:
-    """slice_images on the GPU: the same images from the device DM-time tensor."""
+    """The images of the t_sample-second slices of a device DM-time tensor (include/data.h:620-727)."""
     sps = samples_per_slice(tsamp, time_downsample, slice_duration)
     if sps <= 0:
         raise ValueError("t_sample is shorter than one (downsampled) sample")

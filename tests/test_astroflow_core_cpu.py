@@ -11,6 +11,7 @@ import pytest
 
 from astroflow_b200 import _astroflow_core as C
 from astroflow_b200 import postprocess
+from oracle import cv2_images as CVI
 from sigproc_writer import write_fil
 
 F32 = np.float32
@@ -126,16 +127,21 @@ def test_samples_per_slice_float_arithmetic():
     assert postprocess.samples_per_slice(1e-4, 4, 0.1) == int(F32(0.1) / (F32(1e-4) * F32(4)))
 
 
-def test_slice_images_shapes_and_colormap():
+def test_slice_arithmetic_equals_the_oracle():
+    for ts, ds, dur in [(49.152e-6, 1, 0.5), (1e-4, 4, 0.1), (64e-6, 2, 0.5), (1.26646875e-3, 3, 0.3)]:
+        assert postprocess.samples_per_slice(ts, ds, dur) == CVI.samples_per_slice(ts, ds, dur)
+
+
+def test_oracle_slice_images_shapes_and_colormap():
     pytest.importorskip("cv2")
     rng = np.random.default_rng(0)
     raw = rng.integers(0, 1000, size=(40, 250)).astype(np.uint32)
-    imgs = postprocess.slice_images(raw, 1e-3, 1, 0.1)
+    imgs = CVI.slice_images(raw, 1e-3, 1, 0.1)
     assert len(imgs) == 3 and all(i.shape == (512, 512, 3) and i.dtype == np.uint8 for i in imgs)
     import cv2
 
     # min-max normalisation: the smallest and largest sums map to viridis(0) and viridis(255)
-    ramp = postprocess.images([np.arange(600 * 600, dtype=np.uint32).reshape(600, 600)])[0]
+    ramp = CVI.images([np.arange(600 * 600, dtype=np.uint32).reshape(600, 600)])[0]
     lut = cv2.applyColorMap(np.array([[0, 255]], np.uint8), cv2.COLORMAP_VIRIDIS)[0]
     assert np.array_equal(ramp[0, 0], lut[0]) and np.array_equal(ramp[-1, -1], lut[1])
 

@@ -11,6 +11,7 @@ reference's own code run on the same GPU (oracle/_ref/libref_gpu_sb<W>.so):
 import numpy as np
 import pytest
 
+from oracle import cv2_images as CVI
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -72,7 +73,7 @@ def test_dedisperse_spec_images_match_reference(case, tmp_path):
                                     ds, tslice, sb_width=W, mask_file=str(mask), use_mask=um,
                                     use_zero_dm=uz, use_iqrm=ui, iq=iq)
     tsamp_out = float(F32(F32(hdr.tsamp) * F32(ds)))
-    assert_same_images(res.dm_times, postprocess.slice_images(ref, tsamp_out, 1, tslice))
+    assert_same_images(res.dm_times, CVI.slice_images(ref, tsamp_out, 1, tslice))
     assert res.shape == [512, 512, 3] and res.dm_ndata == 512 and res.downtsample_ndata == 512
     assert (res.dm_low, res.dm_high, res.dm_step) == (float(F32(lo)), float(F32(hi)), float(F32(step)))
     assert res.tsample == float(F32(tslice)) and res.filname == "chunk"
@@ -122,7 +123,7 @@ def test_dedispered_fil_gpu_images_match_reference(case, tmp_path):
                                    mask_file=str(mask), use_mask=um, use_zero_dm=uz,
                                    use_iqrm=ui, iq=iq)
     tsamp_out = float(F32(tsamp * ds))
-    assert_same_images(res.dm_times, postprocess.slice_images(ref, tsamp_out, 1, tslice))
+    assert_same_images(res.dm_times, CVI.slice_images(ref, tsamp_out, 1, tslice))
 
 
 def test_dedispered_fil_cpu_target_matches_oracle(tmp_path):
@@ -136,7 +137,7 @@ def test_dedispered_fil_cpu_target_matches_oracle(tmp_path):
     res = C._dedispered_fil(str(path), lo, hi, fs, fe, step, ds, tslice, 0)
     slices = O.bruteforce_cpu(fil.data.reshape(n, nchans), nchans, fil.frequency_table, fil.tsamp,
                               lo, hi, fs, fe, step, ds, tslice)
-    assert_same_images(res.dm_times, postprocess.images(slices))
+    assert_same_images(res.dm_times, CVI.images(slices))
 
 
 def test_filterbank_path_matches_reference_on_random_files(tmp_path):

@@ -12,6 +12,7 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 cv2 = pytest.importorskip("cv2")
 from astroflow_b200 import postprocess  # noqa: E402
+from oracle import cv2_images as CVI  # noqa: E402
 
 
 def _dev(a: np.ndarray):
@@ -50,7 +51,7 @@ def test_resize_and_images_match_opencv(rows, widths, dt, scale):
             np.testing.assert_allclose(got[i], want, rtol=1e-6, atol=0)
         else:
             np.testing.assert_array_equal(got[i], want)
-            np.testing.assert_array_equal(imgs[i], postprocess._image(raw[:, s:s + w]))
+            np.testing.assert_array_equal(imgs[i], CVI.image(raw[:, s:s + w]))
 
 
 def test_constant_sums():
@@ -62,17 +63,31 @@ def test_constant_sums():
     assert (img == postprocess.viridis_lut()[0]).all()
     raw = np.full((800, 1500), 7, np.uint32)
     img = postprocess.device_images(_dev(raw), [0], [1500]).cpu().numpy()[0]
-    np.testing.assert_array_equal(img, postprocess._image(raw))
+    np.testing.assert_array_equal(img, CVI.image(raw))
 
 
 def test_slice_images_on_device_equal_host():
     rng = np.random.default_rng(1)
     raw = rng.integers(0, 1 << 20, (3001, 25000)).astype(np.uint32)
-    want = postprocess.slice_images(raw, 64e-6, 2, 0.5)
+    want = CVI.slice_images(raw, 64e-6, 2, 0.5)
     got = postprocess.device_slice_images(_dev(raw), 64e-6, 2, 0.5)
     assert len(got) == len(want) == 7
     for a, b in zip(got, want):
         np.testing.assert_array_equal(a, b)
+
+
+def test_host_images_outlive_the_staging_block():
+    """Images come to the host through one reused pinned block; each call's arrays
+    are its own and keep their bytes when the next call (fewer or more images)
+    reuses the block."""
+    rng = np.random.default_rng(5)
+    raws = [rng.integers(0, 1 << 16, (700, c)).astype(np.uint32) for c in (2600, 900, 4100)]
+    results = [postprocess.device_slice_images(_dev(r), 1e-3, 1, 0.5) for r in raws]
+    for r, got in zip(raws, results):
+        want = CVI.slice_images(r, 1e-3, 1, 0.5)
+        assert len(got) == len(want)
+        for a, b in zip(got, want):
+            np.testing.assert_array_equal(a, b)
 
 
 def test_bad_arguments_raise():
