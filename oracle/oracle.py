@@ -16,8 +16,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
-# Arithmetic variants (dd_oracle.h).  PINNED_* are the forms that reproduce the
-# reference builds; tests/test_oracle_pin.py re-establishes them.
+# Arithmetic variants (dd_oracle.h).  The functions' default variants are the
+# forms that reproduce the reference builds; tests/test_oracle_cpu.py checks them
+# against golden vectors made by those builds, and the GPU parity tests against
+# the builds themselves.
 FMA_DM = 1
 RECIP_TSAMP = 2
 RECIP_1349 = 4
