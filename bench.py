@@ -741,10 +741,32 @@ def e2e_dropin_run(wl, hdr, x, units, dist, dev, steps, warmup, t_sample=0.5):
     torch.cuda.synchronize(dev)
     ms_rank = e0.elapsed_time(e1) / steps
     n = len(res.dm_times)
+
+    # untimed: one more call's phases one at a time (synchronised between phases),
+    # through the same functions the call uses
+    from astroflow_b200 import postprocess
+
+    plan = next(reversed(C._PLANS.values()))
+    phases = {}
+
+    def phase(name, f):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        r = f()
+        torch.cuda.synchronize(dev)
+        phases[name] = (time.perf_counter() - t0) * 1e3
+        return r
+
+    xd = phase("to_device_ms", lambda: C._to_device(x_host, dev))
+    o = phase("run_ms", lambda: plan.run(xd))
+    ds = wl["ds"]
+    tsamp_out = float(f32(header.tsamp * f32(ds))) if ds > 1 else header.tsamp
+    phase("images_ms", lambda: postprocess.device_slice_images(o, tsamp_out, 1, t_sample))
     return {"value": dist.job_rate(units, ms_rank * 1e-3), "unit": UNIT,
             "h2d_bytes_per_step": int(x_host.nbytes), "d2h_bytes_per_step": int(n * 512 * 512 * 3),
             "ms_per_step": dist.max(ms_rank), "images": n, "t_sample": t_sample,
-            "api": "_astroflow_core._dedisperse_spec: host numpy chunk in, images out"}
+            "api": "_astroflow_core._dedisperse_spec: host numpy chunk in, images out",
+            "phases_one_call": phases}
 
 
 def main():
