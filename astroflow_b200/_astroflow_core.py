@@ -28,8 +28,10 @@ from __future__ import annotations
 import os
 import re
 import struct
+import threading
 from collections import OrderedDict
-from typing import List, Optional
+from contextlib import contextmanager
+from typing import List, Optional, Tuple
 
 import numpy as np
 
@@ -337,20 +339,38 @@ def load_mask_file(path: str) -> List[int]:
     return chans
 
 
-_PLANS: "OrderedDict[tuple, Plan]" = OrderedDict()
+_PLANS: "OrderedDict[tuple, Tuple[Plan, threading.Lock]]" = OrderedDict()
+_PLANS_LOCK = threading.Lock()
 _MAX_PLANS = 4
 
 
-def _cached_plan(key, make) -> Plan:
-    p = _PLANS.get(key)
-    if p is None:
-        p = make()
-        _PLANS[key] = p
-        while len(_PLANS) > _MAX_PLANS:
-            _PLANS.popitem(last=False)[1].close()
-    else:
-        _PLANS.move_to_end(key)
-    return p
+@contextmanager
+def _cached_plan(key, make):
+    """The cached plan for `key` (made on first use), held for the caller alone.
+    A plan's device workspace serves one call at a time and the library's calls
+    release the GIL, so concurrent calls of one geometry take turns; the caller's
+    work must be complete on the device when it leaves the block.  Plans beyond
+    the newest _MAX_PLANS are closed once no call holds them."""
+    while True:
+        evicted = []
+        with _PLANS_LOCK:
+            entry = _PLANS.get(key)
+            if entry is None:
+                entry = (make(), threading.Lock())
+                _PLANS[key] = entry
+                while len(_PLANS) > _MAX_PLANS:
+                    evicted.append(_PLANS.popitem(last=False)[1])
+            else:
+                _PLANS.move_to_end(key)
+        for old_plan, old_lock in evicted:
+            with old_lock:  # waits for a call that still uses it
+                old_plan.close()
+        plan, lock = entry
+        with lock:
+            if plan.closed:  # evicted between the lookup and the lock: look again
+                continue
+            yield plan
+            return
 
 
 def _as_spec_array(data) -> np.ndarray:
@@ -415,13 +435,15 @@ def _dedisperse_spec(data, header, dm_low, dm_high, freq_start, dm_step=1, ref_f
            _f32(dm_high), _f32(freq_start), _f32(freq_end), _f32(dm_step_), int(ds),
            int(target_id), tuple(bad), rfi.use_mask, rfi.use_zero_dm, rfi.use_iqrm,
            tuple(vars(rfi.iqrm_cfg.params()).values()), SUBBAND_WIDTH, ZERO_DM_MODE)
-    plan = _cached_plan(key, lambda: Plan(
-        hdr, dm_low, dm_high, freq_start, freq_end, dm_step_, int(ds), algorithm="subband",
-        subband_width=SUBBAND_WIDTH, ndm0=NDM0, zero_dm_mode=ZERO_DM_MODE, freq_mode="header",
-        rfi=rfi.params(), bad_channels=bad, device=int(target_id)))
-    out = plan.run(_to_device(a, int(target_id)))
-    tsamp_out = _f32(header.tsamp * np.float32(ds)) if ds > 1 else header.tsamp
-    imgs = postprocess.device_slice_images(out, tsamp_out, 1, t_sample)
+    with _cached_plan(key, lambda: Plan(
+            hdr, dm_low, dm_high, freq_start, freq_end, dm_step_, int(ds), algorithm="subband",
+            subband_width=SUBBAND_WIDTH, ndm0=NDM0, zero_dm_mode=ZERO_DM_MODE,
+            freq_mode="header", rfi=rfi.params(), bad_channels=bad,
+            device=int(target_id))) as plan:
+        out = plan.run(_to_device(a, int(target_id)))
+        tsamp_out = _f32(header.tsamp * np.float32(ds)) if ds > 1 else header.tsamp
+        # the images' copy to the host waits for the plan's work on this stream
+        imgs = postprocess.device_slice_images(out, tsamp_out, 1, t_sample)
     return _result(imgs, dm_low, dm_high, dm_step_, t_sample, header.filename)
 
 

@@ -202,6 +202,10 @@ class Plan:
         _lib.check(_lib.load().dd_run_host(self._h, x.ctypes.data, out.ctypes.data, h))
         return out
 
+    @property
+    def closed(self) -> bool:
+        return not (getattr(self, "_h", None) and self._h.value)
+
     def close(self, stream=None) -> None:
         """Release the plan.  With `stream` (the CUDA stream all of the plan's work
         was issued on) its memory is released stream-ordered, without waiting for

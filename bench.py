@@ -746,7 +746,7 @@ def e2e_dropin_run(wl, hdr, x, units, dist, dev, steps, warmup, t_sample=0.5):
     # through the same functions the call uses
     from astroflow_b200 import postprocess
 
-    plan = next(reversed(C._PLANS.values()))
+    plan = next(reversed(C._PLANS.values()))[0]  # (plan, lock); no other thread uses it
     phases = {}
 
     def phase(name, f):

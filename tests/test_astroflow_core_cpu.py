@@ -191,3 +191,66 @@ def test_viridis_table_is_the_reference_colormap():
     g = np.random.default_rng(3).integers(0, 256, (64, 80), dtype=np.uint8)
     want = cv2.applyColorMap(cv2.cvtColor(g, cv2.COLOR_GRAY2RGB), cv2.COLORMAP_VIRIDIS)
     assert lut.shape == (256, 3) and np.array_equal(lut[g], want)
+
+
+class _FakePlan:
+    def __init__(self, log):
+        self.log, self.closed = log, False
+
+    def close(self):
+        self.log.append("close")
+        self.closed = True
+
+
+def test_plan_cache_serialises_calls_and_closes_evicted_plans(monkeypatch):
+    """Calls of one geometry hold the cached plan one at a time; plans past the
+    newest _MAX_PLANS are closed, after the call that holds one has finished."""
+    import threading
+    import time
+    from collections import OrderedDict
+
+    monkeypatch.setattr(C, "_PLANS", OrderedDict())
+    log = []
+    inside, overlap = [0], [False]
+    lock = threading.Lock()
+
+    def call(key):
+        with C._cached_plan(key, lambda: _FakePlan(log)) as p:
+            with lock:
+                inside[0] += 1
+                overlap[0] |= inside[0] > 1
+            time.sleep(0.02)
+            with lock:
+                inside[0] -= 1
+            assert not p.closed
+
+    threads = [threading.Thread(target=call, args=(("k",),)) for _ in range(6)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not overlap[0] and log == []
+
+    # a call holding the oldest plan delays its closing until the call ends
+    held = threading.Event()
+    release = threading.Event()
+
+    def holder():
+        with C._cached_plan(("k",), lambda: _FakePlan(log)):
+            held.set()
+            release.wait(5)
+            log.append("holder done")
+
+    h = threading.Thread(target=holder)
+    h.start()
+    held.wait(5)
+    evictor = threading.Thread(
+        target=lambda: [call((f"n{i}",)) for i in range(C._MAX_PLANS)])
+    evictor.start()
+    time.sleep(0.1)
+    assert log == []  # the eviction waits for the holder
+    release.set()
+    h.join()
+    evictor.join()
+    assert log == ["holder done", "close"]
+    assert len(C._PLANS) == C._MAX_PLANS and ("k",) not in C._PLANS
