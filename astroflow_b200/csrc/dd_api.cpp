@@ -91,7 +91,9 @@ void build_band(dd_plan& P) {
   const float fmin = static_cast<float>(P.freq.front());
   const float fmax = static_cast<float>(P.freq.back());
   if (P.p.freq_start < fmin || P.p.freq_end > fmax)
-    throw invalid(P.p.algorithm == DD_ALGO_BRUTE
+    // the Filterbank entry points (dedispered.cu:509-516, cpucal.hpp:86-93) name the
+    // file's range, the spectrum call (dedispered.cu:1009-1015) the spectrum's
+    throw invalid(P.p.algorithm == DD_ALGO_BRUTE || P.p.freq_mode == DD_FREQ_FIL
                       ? "Frequency range [%.3f-%.3f MHz] out of filterbank range [%.3f-%.3f MHz]"
                       : "Frequency range [%.3f-%.3f MHz] out of spectrum range [%.3f-%.3f MHz]",
                   P.p.freq_start, P.p.freq_end, fmin, fmax);

@@ -89,10 +89,35 @@ def test_dedisperse_spec_accepts_3d_input():
 
 
 def test_dedisperse_spec_rejects_band_outside_header():
+    """A band outside the header's raises ValueError with the reference's message
+    (src/core/dedispered.cu:1009-1015), word for word against the reference build."""
     x, spec = chunk(64, 2048, 8, 64e-6, seed=1)
     hdr = C.Header(0.0, spec.tsamp, spec.fch1, spec.foff, 8, 64, 2048, "c")
-    with pytest.raises(ValueError):
+    with pytest.raises(ValueError) as ours:
         C._dedisperse_spec(x, hdr, 0, 100, 900.0, 1500.0, 1, 1, 0.05)
+    assert str(ours.value).startswith(
+        "Frequency range [900.000-1500.000 MHz] out of spectrum range [")
+    if O.ref_gpu_available(32):
+        with pytest.raises(ValueError) as ref:
+            O.ref_gpu_dedisperse_spec(x, 64, hdr.tsamp, hdr.fch1, hdr.foff, 0.0, 100.0, 900.0,
+                                      1500.0, 1.0, 1, 0.05)
+        assert str(ref.value).endswith(str(ours.value)), (str(ref.value), str(ours.value))
+
+
+def test_dedispered_fil_rejects_band_outside_the_file(tmp_path):
+    """The same for a file (src/core/dedispered.cu:483-986 through the Filterbank
+    path): ValueError with the reference's message."""
+    x, spec = chunk(64, 2048, 8, 64e-6, seed=2)
+    path = tmp_path / "band.fil"
+    write_fil(path, x, 64e-6, spec.fch1, spec.foff)
+    fe = float(spec.fch1 + 63 * spec.foff)
+    with pytest.raises(ValueError) as ours:
+        C._dedispered_fil(str(path), 0.0, 100.0, 900.0, fe, 1.0, 1, 0.05, 1, 0)
+    assert str(ours.value).startswith("Frequency range [900.000-")
+    if O.ref_gpu_available(32):
+        with pytest.raises(ValueError) as ref:
+            O.ref_gpu_dedispered_fil(path, 0.0, 100.0, 900.0, fe, 1.0, 1, 0.05)
+        assert str(ref.value).endswith(str(ours.value)), (str(ref.value), str(ours.value))
 
 
 FIL = [
