@@ -162,3 +162,44 @@ def test_library_geometry_errors():
     assert L.dd_single_dm_geometry(ctypes.byref(h2), ctypes.byref(q),
                                    ctypes.byref(_lib.SingleDmInfo())) == _lib.DD_ERR_INVALID
     assert "descending" in L.dd_last_error().decode()
+
+
+@pytest.mark.skipif(not O.ref_gpu_available(32), reason="reference build absent")
+@pytest.mark.parametrize("fil", [False, True], ids=["header", "filterbank"])
+def test_library_errors_are_the_reference_messages(fil, tmp_path):
+    """Rejected windows, bands and DMs: dd_single_dm_geometry (host code) fails where
+    the reference's cpucal functions throw, with the same message word for word
+    (include/cpucal.hpp:214-235, 282-284, 350-388, 430-432), and accepts what
+    they accept."""
+    from astroflow_b200 import _lib
+
+    L = _lib.load()
+    nchans, ndata, tsamp, fch1, foff = 64, 2000, 1e-3, 1200.0, 1.0
+    x = np.random.default_rng(0).integers(0, 200, (ndata, nchans)).astype(np.uint8)
+    path = str(tmp_path / "a.fil")
+    write_fil(path, x, tsamp, fch1, foff)
+    cases = [(0.5, 0.5, 10.0, 1200.0, 1250.0), (2.5, 3.0, 10.0, 1200.0, 1250.0),
+             (0.1, 0.5, 10.0, 1250.0, 1250.0), (0.1, 0.5, -1.0, 1200.0, 1250.0),
+             (0.1, 0.5, 10.0, 1100.0, 1250.0), (0.1, 0.5, 10.0, 1200.0, 1300.0),
+             (1.99, 1.995, 500.0, 1200.0, 1263.0), (0.1, 0.5, 10.0, 1200.2, 1200.4)]
+    rejected = 0
+    for ts, te, dm, fs, fe in cases:
+        try:
+            if fil:
+                O.ref_gpu_fil_with_dm(path, 8, ts, te, dm, fs, fe)
+            else:
+                O.ref_gpu_spec_with_dm(x, nchans, tsamp, fch1, foff, ts, te, dm, fs, fe)
+            ref = None
+        except ValueError as e:
+            ref = str(e)
+        h = _lib.Header(0.0, tsamp, fch1, foff, 8, nchans, ndata)
+        q = _lib.SingleDmParams(ts, te, dm, fs, fe, _lib.FREQ_FIL if fil else _lib.FREQ_HEADER,
+                                None)
+        info = _lib.SingleDmInfo()
+        rc = L.dd_single_dm_geometry(ctypes.byref(h), ctypes.byref(q), ctypes.byref(info))
+        ours = None if rc == 0 else L.dd_last_error().decode()
+        assert ours == ref, ((ts, te, dm, fs, fe), ours, ref)
+        if rc:
+            assert rc == _lib.DD_ERR_INVALID
+            rejected += 1
+    assert rejected >= 6
