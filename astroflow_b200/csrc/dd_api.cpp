@@ -471,6 +471,7 @@ void create_rfi(dd_plan& P) {
     upload(P.d_seg_t0, st0.data(), sizeof(uint32_t) * st0.size());
     if (!P.lags.empty()) upload(P.d_lags, P.lags.data(), sizeof(int32_t) * P.lags.size());
     const int64_t csub = std::max<int64_t>(P.ce - P.cs, 1);
+    if (!P.lags.empty()) check_iqrm_channels(csub);
     P.d_stats.alloc(sizeof(unsigned long long) * 2 * csub * nwin);
     P.d_iqrm_scratch.alloc(iqrm_scratch_bytes(nwin, csub, static_cast<int>(P.lags.size())));
     P.d_masks.alloc(static_cast<size_t>(nwin) * n);

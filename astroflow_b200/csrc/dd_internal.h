@@ -153,6 +153,9 @@ void launch_iqrm_stats(const void* x, int nbits, int64_t nsamp, int64_t nchans, 
                        int64_t csub, const uint32_t* d_win, int nwin,
                        unsigned long long* d_sums, cudaStream_t st);
 size_t iqrm_scratch_bytes(int nwin, int64_t csub, int nlags);
+// Throws DD_ERR_INVALID when csub channels exceed what k_iqrm_decide's
+// shared-memory sort holds on the current device.
+void check_iqrm_channels(int64_t csub);
 void launch_iqrm_decide(const unsigned long long* d_sums, int nwin, const uint32_t* d_win,
                         int64_t nchans, int64_t cs, int64_t csub, int mode, float nsigma,
                         const int32_t* d_lags, int nlags, int variant, void* scratch,

@@ -24,7 +24,16 @@
 //
 // The first call on a device looks up the array's device address for that
 // device (cudaGetSymbolAddress) with the device current; make that first call
-// before any stream capture.
+// before any stream capture.  The library's device code is loaded lazily, so
+// that first call is also when the 8 MiB array is placed in the device's
+// memory: a host that reserves most of the GPU's memory for its own pools
+// should make one call (any valid small request) before reserving it.  After
+// cudaDeviceReset the cached address is stale and the process must not call
+// this entry point on that device again.
+//
+// The window list and the lags are written into the array by a kernel that
+// takes their few defining numbers by value, so the GPU work of a call never
+// reads host memory after the call has returned.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -33,7 +42,6 @@
 #include <cstdio>
 #include <mutex>
 #include <string>
-#include <vector>
 
 #include "dd_internal.h"
 
@@ -67,6 +75,44 @@ void* scratch_on_current_device() {
 
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
+// IQRM windows and lags of one call, written into the scratch array.
+// Windows (the reference's plan, src/core/iqrm.cu:348-397): a single window
+// [0, ns) when single != 0; else window k < nfull is [k*hop, k*hop + W) and, when
+// tail != 0, window nfull is [nfull*hop, ns).  Lags (src/core/iqrm.cu:188-200):
+// +lag, -lag for lag = 1, max(floor(g*lag), lag+1), ... while lag <= radius,
+// leaving out lags of magnitude >= csub; the host sized the list with the same
+// double arithmetic.
+__global__ void k_noalloc_tables(uint32_t* win, int nwin, int single, uint32_t ns, uint32_t W,
+                                 uint32_t hop, int nfull, int32_t* lags, int radius, double g,
+                                 int64_t csub) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nwin; k += gridDim.x * blockDim.x) {
+    uint32_t t0, t1;
+    if (single) {
+      t0 = 0u;
+      t1 = ns;
+    } else if (k < nfull) {
+      t0 = static_cast<uint32_t>(static_cast<uint64_t>(k) * hop);
+      t1 = t0 + W;
+    } else {
+      t0 = static_cast<uint32_t>(static_cast<uint64_t>(nfull) * hop);
+      t1 = ns;
+    }
+    win[2 * k] = t0;
+    win[2 * k + 1] = t1;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int n = 0;
+    for (int lag = 1; lag <= radius;) {
+      if (lag < csub) {
+        lags[n++] = +lag;
+        lags[n++] = -lag;
+      }
+      const int nxt = static_cast<int>(g * lag);
+      lag = nxt > lag + 1 ? nxt : lag + 1;
+    }
+  }
+}
+
 }  // namespace
 }  // namespace dd
 
@@ -93,22 +139,18 @@ extern "C" int dd_iqrm_masks_noalloc(const void* input, int32_t nbits, int64_t n
     const uint32_t ns = static_cast<uint32_t>(nsamp);
     const uint32_t W = win_sec > 0.0 ? static_cast<uint32_t>(std::floor(win_sec / tsamp)) : 0u;
     const uint32_t H = hop_sec > 0.0 ? static_cast<uint32_t>(std::floor(hop_sec / tsamp)) : W;
-    std::vector<uint32_t> win;
-    if (W == 0 || W >= ns) {
-      win = {0u, ns};
-    } else {
-      uint32_t t0 = 0;
+    const bool single = (W == 0 || W >= ns);
+    const uint32_t hop = H ? H : W;
+    int nfull = 0, tail = 0;
+    if (!single) {
+      uint64_t t0 = 0;
       while (t0 + W <= ns) {
-        win.push_back(t0);
-        win.push_back(t0 + W);
-        t0 += (H ? H : W);
+        ++nfull;
+        t0 += hop;
       }
-      if (cfg->include_tail && t0 < ns && ns > t0 + 4) {
-        win.push_back(t0);
-        win.push_back(ns);
-      }
+      tail = (cfg->include_tail && t0 < ns && ns > t0 + 4) ? 1 : 0;
     }
-    const int nwin = static_cast<int>(win.size() / 2);
+    const int nwin = single ? 1 : nfull + tail;
     *n_windows = nwin;
     if (nwin > max_windows)
       throw Error{DD_ERR_INVALID, "max_windows (" + std::to_string(max_windows) +
@@ -120,18 +162,15 @@ extern "C" int dd_iqrm_masks_noalloc(const void* input, int32_t nbits, int64_t n
     volatile float rprod = rf * static_cast<float>(csub);
     const int radius = std::max(1, static_cast<int>(std::floor(static_cast<float>(rprod))));
     const double g = cfg->geofactor > 1.0 ? cfg->geofactor : 1.5;
-    std::vector<int32_t> lags;
+    int nlags = 0;
     for (int lag = 1; lag <= radius;) {
-      if (lag < csub) {
-        lags.push_back(+lag);
-        lags.push_back(-lag);
-      }
+      if (lag < csub) nlags += 2;
       lag = std::max(static_cast<int>(g * lag), lag + 1);
     }
-    const int nlags = static_cast<int>(lags.size());
+    if (nlags) check_iqrm_channels(csub);  // the per-window sort fits shared memory
 
     // Scratch layout inside g_iqrm_scratch.
-    const size_t b_win = align256(sizeof(uint32_t) * win.size());
+    const size_t b_win = align256(sizeof(uint32_t) * 2 * nwin);
     const size_t b_lags = align256(sizeof(int32_t) * std::max(1, nlags));
     const size_t b_sums = align256(sizeof(unsigned long long) * 2 * csub * nwin);
     const size_t b_work = align256(iqrm_scratch_bytes(nwin, csub, nlags));
@@ -150,11 +189,11 @@ extern "C" int dd_iqrm_masks_noalloc(const void* input, int32_t nbits, int64_t n
     unsigned long long* d_sums = reinterpret_cast<unsigned long long*>(base + b_win + b_lags);
     void* d_work = base + b_win + b_lags + b_sums;
 
-    DD_CUDA_TRY(cudaMemcpyAsync(d_win, win.data(), sizeof(uint32_t) * win.size(),
-                                cudaMemcpyHostToDevice, st));
-    if (nlags)
-      DD_CUDA_TRY(cudaMemcpyAsync(d_lags, lags.data(), sizeof(int32_t) * nlags,
-                                  cudaMemcpyHostToDevice, st));
+    const int tb = 256;
+    const int tg = static_cast<int>(std::min<int64_t>((nwin + tb - 1) / tb, 1024));
+    k_noalloc_tables<<<tg, tb, 0, st>>>(d_win, nwin, single ? 1 : 0, ns, W, hop, nfull, d_lags,
+                                        radius, g, csub);
+    DD_LAUNCHED();
     if (nlags) {
       // launch_iqrm_stats clears the sums before accumulating into them.
       launch_iqrm_stats(input, nbits, nsamp, nchans, chan_start, csub, d_win, nwin, d_sums, st);
@@ -163,7 +202,7 @@ extern "C" int dd_iqrm_masks_noalloc(const void* input, int32_t nbits, int64_t n
     } else {
       DD_CUDA_TRY(cudaMemsetAsync(masks, 0, static_cast<size_t>(nwin) * nchans, st));
     }
-    DD_CUDA_TRY(cudaMemcpyAsync(bounds, d_win, sizeof(uint32_t) * win.size(),
+    DD_CUDA_TRY(cudaMemcpyAsync(bounds, d_win, sizeof(uint32_t) * 2 * nwin,
                                 cudaMemcpyDeviceToDevice, st));
     return DD_OK;
   } catch (const Error& e) {

@@ -19,6 +19,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 
 #include "dd_internal.h"
 
@@ -504,6 +505,27 @@ size_t iqrm_scratch_bytes(int nwin, int64_t csub, int nlags) {
   return static_cast<size_t>(nwin) * csub * (4 + 4 + 4 + 4 + nlags) + 256;
 }
 
+// k_iqrm_decide sorts one window's csub statistics in shared memory (the next
+// power of two of csub floats); reject band widths whose sort buffer exceeds the
+// current device's opt-in shared memory per block.
+void check_iqrm_channels(int64_t csub) {
+  int64_t sort_n = 1;
+  while (sort_n < csub) sort_n <<= 1;
+  int dev = 0, optin = 0;
+  DD_CUDA_TRY(cudaGetDevice(&dev));
+  DD_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const int64_t need = static_cast<int64_t>(sizeof(float)) * sort_n;
+  if (need > optin) {
+    char msg[200];
+    std::snprintf(msg, sizeof(msg),
+                  "IQRM over %lld channels needs a %lld-byte sort buffer, more than the %d bytes "
+                  "of shared memory a block can have (at most %d channels)",
+                  static_cast<long long>(csub), static_cast<long long>(need), optin,
+                  optin / static_cast<int>(sizeof(float)));
+    throw Error{DD_ERR_INVALID, msg};
+  }
+}
+
 void launch_iqrm_decide(const unsigned long long* d_sums, int nwin, const uint32_t* d_win,
                         int64_t nchans, int64_t cs, int64_t csub, int mode, float nsigma,
                         const int32_t* d_lags, int nlags, int variant, void* scratch,
@@ -514,6 +536,7 @@ void launch_iqrm_decide(const unsigned long long* d_sums, int nwin, const uint32
   int* recv = reinterpret_cast<int*>(p); p += sizeof(int) * nwin * csub;
   int* cast_ = reinterpret_cast<int*>(p); p += sizeof(int) * nwin * csub;
   uint8_t* flags = reinterpret_cast<uint8_t*>(p);
+  check_iqrm_channels(csub);
   int sort_n = 1;
   while (sort_n < csub) sort_n <<= 1;
   const size_t smem = sizeof(float) * sort_n;

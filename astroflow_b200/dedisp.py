@@ -445,6 +445,24 @@ def iqrm_masks_noalloc(x, nchans: int, chan_start: int, chan_end: int, tsamp: fl
     static scratch array per GPU, so their GPU work must not overlap.  Returns
     the number of windows."""
     torch = _torch()
+    nchans, chan_start, chan_end = int(nchans), int(chan_start), int(chan_end)
+    if nchans < 1:
+        raise ValueError("nchans must be >= 1")
+    if x.dtype not in (torch.uint8, torch.uint16, torch.uint32, torch.int16, torch.int32):
+        raise ValueError("x must hold 8-, 16- or 32-bit samples")
+    if not x.is_contiguous() or x.numel() == 0 or x.numel() % nchans:
+        raise ValueError("x must be a non-empty contiguous tensor of whole [nsamp, nchans] rows")
+    if masks.dtype != torch.uint8 or masks.dim() != 2 or masks.shape[1] != nchans \
+            or not masks.is_contiguous():
+        raise ValueError("masks must be a contiguous uint8 tensor of shape [max_windows, nchans]")
+    if bounds.dtype not in (torch.int32, torch.uint32) or bounds.dim() != 2 \
+            or bounds.shape[1] != 2 or bounds.shape[0] < masks.shape[0] or not bounds.is_contiguous():
+        raise ValueError("bounds must be a contiguous int32 tensor of shape [>= max_windows, 2]")
+    if not (0 <= chan_start < chan_end <= nchans):
+        raise ValueError("channel range must satisfy 0 <= chan_start < chan_end <= nchans")
+    for name, t in (("x", x), ("masks", masks), ("bounds", bounds)):
+        if not t.is_cuda or t.device.index != torch.cuda.current_device():
+            raise ValueError(f"{name} must be on the current CUDA device")
     if stream is None:
         stream = torch.cuda.current_stream()
     n = ctypes.c_int32()

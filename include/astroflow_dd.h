@@ -270,12 +270,17 @@ int dd_measure_int_add_rate(int32_t device, double* adds_per_second);
  * same values dd_run_ex reports; *n_windows (host) receives the window count.
  * Runs on the calling thread's current device, on `stream`.
  *
- * All working memory comes from an 8 MiB array that the library places in
- * every GPU's memory for the life of the process; requests whose working set
- * exceeds it fail with DD_ERR_INVALID.  The first call on a device resolves the
- * array's address with that device current: make it before any stream capture.
- * Calls share the array, so calls whose GPU work overlaps race with each other
- * and must be serialised by the caller. */
+ * All working memory comes from an 8 MiB array that the library keeps in a
+ * GPU's memory from the first call on that GPU until the process exits;
+ * requests whose working set exceeds it, and bands wider than the per-window
+ * sort's shared memory holds, fail with DD_ERR_INVALID.  The first call on a
+ * device resolves the array's address with that device current: make it before
+ * any stream capture.  The library's device code loads lazily, so that first
+ * call is also when the array takes its 8 MiB: a host that reserves most of the
+ * GPU's memory for its own pools should make one small call before reserving
+ * it.  Do not call it again on a device after cudaDeviceReset.  Calls share the
+ * array, so calls whose GPU work overlaps race with each other and must be
+ * serialised by the caller. */
 int dd_iqrm_masks_noalloc(const void* input, int32_t nbits, int64_t nsamp, int32_t nchans,
                           int32_t chan_start, int32_t chan_end, double tsamp,
                           const dd_iqrm_config* cfg, uint8_t* masks, uint32_t* bounds,

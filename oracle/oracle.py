@@ -16,6 +16,19 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
+
+def reference_tree() -> str:
+    """The reference source tree: $ASTROFLOW_REFERENCE, else the tree the parity
+    builds in _ref were compiled from ("" when neither is known)."""
+    env = os.environ.get("ASTROFLOW_REFERENCE")
+    if env:
+        return env
+    try:
+        with open(os.path.join(REF_DIR, "reference_tree.txt")) as fh:
+            return fh.read().strip()
+    except OSError:
+        return ""
+
 # Arithmetic variants (dd_oracle.h).  The functions' default variants are the
 # forms that reproduce the reference builds; tests/test_oracle_cpu.py checks them
 # against golden vectors made by those builds, and the GPU parity tests against

@@ -1,7 +1,8 @@
 """Real data: the reference's own test file, tests/FRB180417.fil of the reference
 tree (336 channels of 8-bit samples, 5120 samples of 1.266 ms, the burst FRB
 180417 at DM 474.8, docs/quick_start.md:65).  It is read where the reference tree
-is (ASTROFLOW_REFERENCE, default /root/reference); elsewhere these tests skip.
+is ($ASTROFLOW_REFERENCE, else the tree oracle/_ref was built from); elsewhere
+these tests skip.
 They pin on real data: the library's SIGPROC header reader against the drop-in's
 host reader, the oracle's brute force and single-DM spectrum against the
 reference's own builds, the reference's DM-0 identity
@@ -13,7 +14,7 @@ import pytest
 
 from oracle import oracle as O
 
-REFERENCE_TREE = os.environ.get("ASTROFLOW_REFERENCE", "/root/reference")
+REFERENCE_TREE = O.reference_tree()
 FIL = os.path.join(REFERENCE_TREE, "tests", "FRB180417.fil")
 F32 = np.float32
 
