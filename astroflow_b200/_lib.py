@@ -21,13 +21,13 @@ DD_ERR_TIMEOUT = 5
 DD_ERR_UNSUPPORTED = 6
 
 ALGO_SUBBAND, ALGO_BRUTE = 0, 1
-ZDM_CALLSITE, ZDM_RANGE = 0, 1
-TABLE_REFERENCE, TABLE_FP64 = 0, 1
+ZDM_CALLSITE, ZDM_RANGE, ZDM_RANGE_REF = 0, 1, 2
+TABLE_REFERENCE, TABLE_FP64, TABLE_IEEE = 0, 1, 2
 FREQ_HEADER, FREQ_FIL = 0, 1
 
 # Every symbol include/astroflow_dd.h declares.
 EXPORTS = ("dd_plan_create", "dd_plan_destroy", "dd_plan_destroy_async", "dd_plan_get_info",
-           "dd_plan_get_tables",
+           "dd_plan_get_tables", "dd_brute_delay_table",
            "dd_plan_set_delay_table", "dd_run", "dd_run_ex", "dd_run_host", "dd_run_profiled",
            "dd_measure_int_add_rate", "dd_iqrm_masks_noalloc", "dd_batch_create",
            "dd_batch_run", "dd_batch_status", "dd_batch_get_info", "dd_batch_destroy",
@@ -138,6 +138,9 @@ def load():
     L.dd_plan_destroy.argtypes = [P]
     L.dd_plan_get_info.argtypes = [P, ctypes.POINTER(PlanInfo)]
     L.dd_plan_get_tables.argtypes = [P, P, P]
+    L.dd_brute_delay_table.argtypes = [P, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                       ctypes.c_float, ctypes.c_float, ctypes.c_int64,
+                                       ctypes.c_double, ctypes.c_int32, P, P]
     L.dd_plan_set_delay_table.argtypes = [P, P]
     L.dd_run.argtypes = [P, P, P, P]
     L.dd_run_ex.argtypes = [P, P, P, P, P, P, P]

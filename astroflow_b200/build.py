@@ -7,7 +7,9 @@ Compile units:
                        its kernels must reproduce the reference's fast-math delay tables
                        and zero-DM arithmetic bit for bit;
   csrc/dd_rfi.cu, csrc/dd_dedisp.cu  plain -O3 (IEEE arithmetic, explicit roundings);
-  csrc/dd_api.cpp      host code, -ffp-contract=off, no fast-math.
+  csrc/dd_api.cpp      host code, -ffp-contract=off, no fast-math;
+  csrc/dd_hosttable.cpp  the reference CPU path's host flags (-Ofast, FMA, AVX2), because
+                       the brute-force delay table must equal the reference build's.
 The CUDA runtime is linked statically so the library does not depend on which
 libcudart the host process (e.g. torch) has already loaded.
 """
@@ -42,6 +44,13 @@ UNITS = [
     ("dd_ingest.cu", []),
 ]
 HOST = ["dd_api.cpp"]
+# The brute-force delay table in the reference's host arithmetic: its CPU path's
+# flags (CMakeLists.txt:116-118; -march=native pinned to x86-64-v3, as the
+# parity build of the reference does, so the library runs on any AVX2 host).
+HOST_REFMATH = [("dd_hosttable.cpp", ["-std=gnu++17", "-Ofast", "-march=x86-64-v3", "-mtune=native",
+                                      "-fno-math-errno", "-ffast-math", "-funroll-loops",
+                                      "-fomit-frame-pointer", "-mfma", "-mavx2", "-msse4.2",
+                                      "-DNDEBUG", "-fPIC"])]
 HEADERS = ["dd_internal.h", os.path.join("..", "..", "include", "astroflow_dd.h")]
 
 
@@ -79,6 +88,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if force or not _newer(o, [s, *headers, __file__]):
             _run(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
                   "-Wall", "-I", os.path.join(CUDA, "include"), "-c", s, "-o", o])
+    for src, flags in HOST_REFMATH:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src + ".o")
+        objs.append(o)
+        if force or not _newer(o, [s, __file__]):
+            _run(["g++", *flags, "-c", s, "-o", o])
     if force or not _newer(LIB, objs):
         _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static"])
     return LIB

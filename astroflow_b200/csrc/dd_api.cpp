@@ -113,36 +113,51 @@ void build_band(dd_plan& P) {
   P.ref_freq = static_cast<float>(P.freq[ce]);  // REF_FREQ_END
 }
 
-// ---- brute-force delay table (cpucal.hpp:119-132) in IEEE float
-void build_brute_table(dd_plan& P) {
-  const int64_t nc = P.nc;
-  P.h_delay.assign(static_cast<size_t>(P.dm_steps * nc), 0);
-  const float ref = P.ref_freq;
+// ---- brute-force delay table (cpucal.hpp:119-132)
+// table[m][c - cs] for c in [cs, ce); freq[ref_ch]: the reference frequency.
+// Returns the number of entries that differ from the FP64 evaluation.
+int64_t brute_table(const double* freq, int64_t cs, int64_t ce, int64_t ref_ch, float dm_low,
+                    float dm_step, int64_t dm_steps, double tsamp, int mode, int32_t* table) {
+  const int64_t nc = ce - cs;
+  const float ref = static_cast<float>(freq[ref_ch]);
+  if (mode == DD_TABLE_REFERENCE)
+    brute_delay_table_fastmath(freq, static_cast<size_t>(cs), static_cast<size_t>(ce), dm_low,
+                               dm_step, static_cast<size_t>(dm_steps), ref, tsamp, table);
   volatile float ref2 = ref * ref;
   const float inv_ref2 = 1.0f / ref2;
-  const double tsamp = P.tsamp;
   int64_t mism = 0;
-  for (int64_t s = 0; s < P.dm_steps; ++s) {
+  for (int64_t s = 0; s < dm_steps; ++s) {
     volatile float idx = static_cast<float>(static_cast<size_t>(s));
-    volatile float prod = idx * P.p.dm_step;
-    volatile float dm = P.p.dm_low + prod;
+    volatile float prod = idx * dm_step;
+    volatile float dm = dm_low + prod;
     for (int64_t c = 0; c < nc; ++c) {
-      const float fr = static_cast<float>(P.freq[P.cs + c]);
-      volatile float f2 = fr * fr;
-      volatile float a = 1.0f / f2;
-      volatile float diff = a - inv_ref2;
-      volatile float kd = 4148.808f * dm;
-      volatile float delay = kd * diff;
-      const int v32 = static_cast<int>(std::round(static_cast<double>(delay) / tsamp));
-      const double dm64 = static_cast<double>(P.p.dm_low) + static_cast<double>(s) * P.p.dm_step;
-      const double f = P.freq[P.cs + c], r = P.freq[P.ce];
+      const double dm64 = static_cast<double>(dm_low) + static_cast<double>(s) * dm_step;
+      const double f = freq[cs + c], r = freq[ref_ch];
       const double e = 4148.808 * dm64 * (1.0 / (f * f) - 1.0 / (r * r)) / tsamp;
       const int v64 = static_cast<int>(std::floor(e + 0.5));
-      mism += (v32 != v64);
-      P.h_delay[s * nc + c] = P.p.table_mode == DD_TABLE_FP64 ? v64 : v32;
+      int32_t& out = table[s * nc + c];
+      if (mode == DD_TABLE_IEEE) {
+        const float fr = static_cast<float>(freq[cs + c]);
+        volatile float f2 = fr * fr;
+        volatile float a = 1.0f / f2;
+        volatile float diff = a - inv_ref2;
+        volatile float kd = 4148.808f * dm;
+        volatile float delay = kd * diff;
+        out = static_cast<int>(std::round(static_cast<double>(delay) / tsamp));
+      } else if (mode == DD_TABLE_FP64) {
+        out = v64;
+      }
+      mism += (out != v64);
     }
   }
-  P.table_mismatch_fp64 = mism;
+  return mism;
+}
+
+void build_brute_table(dd_plan& P) {
+  P.h_delay.assign(static_cast<size_t>(P.dm_steps * P.nc), 0);
+  P.table_mismatch_fp64 = brute_table(P.freq.data(), P.cs, P.cs + P.nc, P.ce, P.p.dm_low,
+                                      P.p.dm_step, P.dm_steps, P.tsamp, P.p.table_mode,
+                                      P.h_delay.data());
 }
 
 // ---- IQRM window plan (iqrm.cu:348-397) and lags (iqrm.cu:188-200)
@@ -482,6 +497,7 @@ void create_rfi(dd_plan& P) {
                   double(P.ce), double(P.cs));
   if (P.rfi.use_zero_dm) {
     if (P.p.zero_dm_mode == DD_ZDM_RANGE) P.d_zdm.alloc(sizeof(uint32_t) * P.nbin);
+    else if (P.p.zero_dm_mode == DD_ZDM_RANGE_REF) P.d_zdm.alloc(sizeof(float) * P.nbin);
     else if (callsite_zdm_active(P)) P.d_zdm.alloc(sizeof(float) * (P.ce + 1));
   }
 }
@@ -547,6 +563,12 @@ void run_rfi_and_prep(dd_plan& P, const void* input, uint8_t* masks_out, uint32_
       launch_zdm_offsets(src, P.nbits, P.nbin, n, P.cs, P.ce, segmask, P.d_seg_t0.as<uint32_t>(),
                          nseg, P.d_zdm.as<uint32_t>(), st);
       a.zdm_off = P.d_zdm.as<uint32_t>();
+      a.zdm_cs = P.cs;
+      a.zdm_ce = P.ce;
+    } else if (P.rfi.use_zero_dm && P.p.zero_dm_mode == DD_ZDM_RANGE_REF) {
+      launch_zdm_range_mean(src, P.nbits, P.nbin, n, P.cs, P.ce, segmask,
+                            P.d_seg_t0.as<uint32_t>(), nseg, P.d_zdm.as<float>(), st);
+      a.zdm_mean = P.d_zdm.as<float>();
       a.zdm_cs = P.cs;
       a.zdm_ce = P.ce;
     }
@@ -903,6 +925,9 @@ dd_plan* make_plan(const dd_header* header, const dd_plan_params* params, const 
   if (header->nchans < 2 || header->ndata < 1 || !(header->tsamp > 0))
     throw Error{DD_ERR_INVALID, "header needs nchans >= 2, ndata >= 1 and tsamp > 0"};
   if (params->time_downsample < 1) throw Error{DD_ERR_INVALID, "time_downsample must be >= 1"};
+  if (params->zero_dm_mode != DD_ZDM_CALLSITE && params->zero_dm_mode != DD_ZDM_RANGE &&
+      params->zero_dm_mode != DD_ZDM_RANGE_REF)
+    throw Error{DD_ERR_INVALID, "unknown zero-DM mode"};
   if (!(params->dm_step > 0) || params->dm_high < params->dm_low)
     throw Error{DD_ERR_INVALID, "Invalid DM parameters"};
   int ndev = 0;
@@ -1016,6 +1041,23 @@ int dd_plan_get_tables(const dd_plan* P, int32_t* delay, int32_t* residual) {
     if (delay) std::memcpy(delay, P->h_delay.data(), sizeof(int32_t) * P->h_delay.size());
     if (residual && !P->h_res.empty())
       std::memcpy(residual, P->h_res.data(), sizeof(int32_t) * P->h_res.size());
+  });
+}
+
+int dd_brute_delay_table(const double* freq, int64_t chan_start, int64_t chan_end,
+                         int64_t ref_channel, float dm_low, float dm_step, int64_t dm_steps,
+                         double tsamp, int32_t mode, int32_t* table, int64_t* mismatch_fp64) {
+  if (!freq || !table) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  return guarded([&] {
+    if (chan_start < 0 || chan_end <= chan_start || ref_channel < 0 || dm_steps < 1 ||
+        !(tsamp > 0) || !(dm_step > 0))
+      throw Error{DD_ERR_INVALID, "need 0 <= chan_start < chan_end, ref_channel >= 0, "
+                                  "dm_steps >= 1, tsamp > 0 and dm_step > 0"};
+    if (mode != DD_TABLE_REFERENCE && mode != DD_TABLE_IEEE && mode != DD_TABLE_FP64)
+      throw Error{DD_ERR_INVALID, "unknown table mode"};
+    const int64_t m = brute_table(freq, chan_start, chan_end, ref_channel, dm_low, dm_step,
+                                  dm_steps, tsamp, mode, table);
+    if (mismatch_fp64) *mismatch_fp64 = m;
   });
 }
 

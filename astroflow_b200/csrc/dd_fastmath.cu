@@ -12,7 +12,10 @@
 //    divide_delay_inplace_kernel (:379-382) fused, and the residual shifts of
 //    compute_residual2_kernel (:385-413);
 //  * the zero-DM filter as the reference's call site invokes it
-//    (dedispered.cu:1107 -> RfiMarker::zero_dm_filter, src/rfi/rfimarker.cu:130-169).
+//    (dedispered.cu:1107 -> RfiMarker::zero_dm_filter, src/rfi/rfimarker.cu:130-169);
+//  * the per-sample mean of the range zero-DM filter (rfimarker.cu:172-216),
+//    whose subtraction the layout kernels apply (DD_ZDM_RANGE_REF).
+#include <algorithm>
 #include <cstdint>
 #include <limits>
 
@@ -122,6 +125,64 @@ __global__ void k_zdm_subtract(T* __restrict__ data, unsigned int num_channels,
   data[idx] = zdm_clip_sub<T>(data[idx], delta);
 }
 
+// Range zero-DM mean (rfimarker.cu:172-216 arithmetic): one block of 256
+// threads per sample; thread i sums, in channel order, the float values of the
+// non-zero samples of channels cs+i, cs+i+256, ... below ce (samples that the
+// IQRM segment mask drops count as zero); the 256 partial sums are combined
+// pairwise, i += i+s for s = 128, 64, ..., 1 (the last five steps as warp
+// shuffles, which pair the same lanes), and the mean is the float quotient of
+// this translation unit's fast-math divide.
+template <typename T>
+__global__ void __launch_bounds__(256) k_zdm_range_mean(
+    const T* __restrict__ x, int64_t nsamp, int64_t nchans, int64_t cs, int64_t ce,
+    const uint8_t* __restrict__ segmask, const uint32_t* __restrict__ seg_t0, int nseg,
+    float* __restrict__ mean) {
+  __shared__ float ssum[256];
+  __shared__ unsigned int scnt[256];
+  const int tid = threadIdx.x;
+  for (int64_t t = blockIdx.x; t < nsamp; t += gridDim.x) {
+    const uint8_t* sm = nullptr;
+    if (segmask) {
+      int lo = 0, hi = nseg - 1;  // last segment whose first sample is <= t
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (static_cast<int64_t>(seg_t0[mid]) <= t) lo = mid; else hi = mid - 1;
+      }
+      sm = segmask + static_cast<int64_t>(lo) * nchans;
+    }
+    const T* row = x + t * nchans;
+    float sum = 0.0f;
+    unsigned int cnt = 0u;
+    for (int64_t c = cs + tid; c < ce; c += 256) {
+      const T v = (sm && sm[c]) ? T(0) : row[c];
+      if (v != T(0)) {
+        sum += static_cast<float>(v);
+        cnt += 1u;
+      }
+    }
+    ssum[tid] = sum;
+    scnt[tid] = cnt;
+    __syncthreads();
+    for (int s = 128; s >= 32; s >>= 1) {
+      if (tid < s) {
+        ssum[tid] += ssum[tid + s];
+        scnt[tid] += scnt[tid + s];
+      }
+      __syncthreads();
+    }
+    if (tid < 32) {
+      sum = ssum[tid];
+      cnt = scnt[tid];
+      for (int s = 16; s > 0; s >>= 1) {
+        sum += __shfl_down_sync(0xffffffffu, sum, s);
+        cnt += __shfl_down_sync(0xffffffffu, cnt, s);
+      }
+      if (tid == 0) mean[t] = cnt > 0u ? sum / static_cast<float>(cnt) : 0.0f;
+    }
+    __syncthreads();
+  }
+}
+
 template <typename T>
 void zero_dm_callsite_t(T* data, size_t chan_start, size_t chan_end, size_t down_ndata,
                         float* mean, cudaStream_t st) {
@@ -179,6 +240,19 @@ void launch_subband_tables(const double* d_freq, int64_t cs, int64_t ce, float d
   DD_LAUNCHED();
   DD_CUDA_TRY(cudaFreeAsync(d_sbfreq, st));
   DD_CUDA_TRY(cudaStreamSynchronize(st));
+}
+
+void launch_zdm_range_mean(const void* x, int nbits, int64_t nsamp, int64_t nchans, int64_t cs,
+                           int64_t ce, const uint8_t* d_segmask, const uint32_t* d_seg_t0,
+                           int nseg, float* d_mean, cudaStream_t st) {
+  if (nsamp <= 0) return;
+  const unsigned grid = static_cast<unsigned>(std::min<int64_t>(nsamp, 148 * 16));
+  switch (nbits) {
+    case 8: k_zdm_range_mean<uint8_t><<<grid, 256, 0, st>>>(static_cast<const uint8_t*>(x), nsamp, nchans, cs, ce, d_segmask, d_seg_t0, nseg, d_mean); break;
+    case 16: k_zdm_range_mean<uint16_t><<<grid, 256, 0, st>>>(static_cast<const uint16_t*>(x), nsamp, nchans, cs, ce, d_segmask, d_seg_t0, nseg, d_mean); break;
+    default: k_zdm_range_mean<uint32_t><<<grid, 256, 0, st>>>(static_cast<const uint32_t*>(x), nsamp, nchans, cs, ce, d_segmask, d_seg_t0, nseg, d_mean); break;
+  }
+  DD_LAUNCHED();
 }
 
 void launch_zero_dm_callsite(void* data, int nbits, size_t chan_start, size_t chan_end,

@@ -144,6 +144,11 @@ void launch_subband_tables(const double* d_freq, int64_t cs, int64_t ce, float d
 // mean_ws: device workspace of chan_end floats.
 void launch_zero_dm_callsite(void* data, int nbits, size_t chan_start, size_t chan_end,
                              size_t down_ndata, float* mean_ws, cudaStream_t st);
+// Per-sample float mean of the non-zero (after the IQRM segment masks) values of
+// channels [cs, ce), in the arithmetic of the reference's range kernels.
+void launch_zdm_range_mean(const void* x, int nbits, int64_t nsamp, int64_t nchans, int64_t cs,
+                           int64_t ce, const uint8_t* d_segmask, const uint32_t* d_seg_t0,
+                           int nseg, float* d_mean, cudaStream_t st);
 
 // ---- RFI and layout (dd_rfi.cu) ----
 void launch_time_binning(const void* in, void* out, int nbits, int64_t ndata, int64_t nchans,
@@ -177,6 +182,7 @@ struct PrepArgs {
   const uint32_t* seg_t0;
   int nseg;
   const uint32_t* zdm_off; // nullptr: no zero-DM subtraction in this pass
+  const float* zdm_mean;   // per-sample float mean (DD_ZDM_RANGE_REF), or nullptr
   int64_t zdm_cs, zdm_ce;  // channel range the zero-DM offset applies to
   const uint8_t* keep;     // nullptr: no static mask
   // channel-major output: out[(c - c0) * rows_per_chan + phase][q] with
@@ -360,6 +366,11 @@ void launch_sum_batch(const SumBatchGroup* d_groups, int ngroups, long long tota
 // Grouped launch: one grid over independent groups of one variant (`kind`).
 void launch_sum_grouped(const SumBatchGroup* d_groups, int ngroups, long long total, int kind,
                         size_t smem, cudaStream_t st);
+
+// ---- brute-force table in the reference's host arithmetic (dd_hosttable.cpp) ----
+void brute_delay_table_fastmath(const double* freq, size_t chan_start, size_t chan_end,
+                                float dm_low, float dm_step, size_t dm_steps,
+                                float ref_freq_value, double tsamp, int32_t* table);
 
 // ---- probes (dd_probe.cu) ----
 double measure_int_add_rate(int device);

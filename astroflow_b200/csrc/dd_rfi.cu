@@ -273,6 +273,18 @@ __global__ void k_zdm_offsets(const T* __restrict__ x, int64_t nsamp, int64_t nc
   if (lane == 0) off[t] = n ? static_cast<uint32_t>((s + n - 1) / n) : 0u;
 }
 
+// Range zero-DM subtraction with a float mean (zdm_sat_sub of
+// rfimarker.cu:218-225 with alpha 1 and clipping): float(v) - mean, clipped to
+// [0, max of T], truncated.
+template <typename T>
+__device__ __forceinline__ T zdm_float_sub(T v, float mean) {
+  float r = __fsub_rn(static_cast<float>(v), mean);
+  if (r < 0.0f) r = 0.0f;
+  const float vmax = static_cast<float>(Lim<T>::vmax);
+  if (r > vmax) r = vmax;
+  return static_cast<T>(r);
+}
+
 // Fused RFI application and transpose to the channel-major layout.
 // Tile: 64 samples x 64 channels, 256 threads.
 template <typename T>
@@ -297,6 +309,7 @@ __global__ void k_prep(PrepArgs a) {
         const uint32_t m = a.zdm_off[t];
         v = static_cast<T>(static_cast<uint32_t>(v) > m ? static_cast<uint32_t>(v) - m : 0u);
       }
+      if (a.zdm_mean && c >= a.zdm_cs && c < a.zdm_ce) v = zdm_float_sub<T>(v, a.zdm_mean[t]);
       if (a.keep && !a.keep[c]) v = 0;
     }
     tile[r][tx] = v;
@@ -465,6 +478,7 @@ __global__ void k_prep_full(PrepArgs a) {
     const uint32_t m = a.zdm_off[t];
     v = static_cast<T>(static_cast<uint32_t>(v) > m ? static_cast<uint32_t>(v) - m : 0u);
   }
+  if (a.zdm_mean && c >= a.zdm_cs && c < a.zdm_ce) v = zdm_float_sub<T>(v, a.zdm_mean[t]);
   if (a.keep && !a.keep[c]) v = 0;
   out[t * a.nchans + c] = v;
   }
@@ -581,13 +595,14 @@ void launch_zdm_offsets(const void* x, int nbits, int64_t nsamp, int64_t nchans,
 }
 
 void launch_prep(const PrepArgs& a, cudaStream_t st) {
-  if (a.out && a.nbits == 8 && a.ds == 1 && a.nchans % 4 == 0 && a.pitch % 4 == 0 &&
+  // the word-wise kernels apply integer zero-DM offsets only
+  if (a.out && !a.zdm_mean && a.nbits == 8 && a.ds == 1 && a.nchans % 4 == 0 && a.pitch % 4 == 0 &&
       reinterpret_cast<uintptr_t>(a.x) % 4 == 0 && reinterpret_cast<uintptr_t>(a.out) % 4 == 0) {
     const int64_t cw0 = a.c0 & ~int64_t(3);
     dim3 grid(static_cast<unsigned>((a.nsamp + 63) / 64), static_cast<unsigned>((a.c1 - cw0 + 63) / 64));
     k_prep_u8<<<grid, 256, 0, st>>>(a);
     DD_LAUNCHED();
-  } else if (a.out && a.nbits == 16 && a.ds == 1 && a.nchans % 4 == 0 && a.pitch % 4 == 0 &&
+  } else if (a.out && !a.zdm_mean && a.nbits == 16 && a.ds == 1 && a.nchans % 4 == 0 && a.pitch % 4 == 0 &&
              reinterpret_cast<uintptr_t>(a.x) % 8 == 0 && reinterpret_cast<uintptr_t>(a.out) % 8 == 0) {
     const int64_t cw0 = a.c0 & ~int64_t(3);
     dim3 grid(static_cast<unsigned>((a.nsamp + 63) / 64), static_cast<unsigned>((a.c1 - cw0 + 63) / 64));

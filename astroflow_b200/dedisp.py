@@ -16,8 +16,8 @@ import numpy as np
 from . import _lib
 
 _ALGOS = {"subband": _lib.ALGO_SUBBAND, "brute": _lib.ALGO_BRUTE}
-_ZDM = {"callsite": _lib.ZDM_CALLSITE, "range": _lib.ZDM_RANGE}
-_TABLES = {"reference": _lib.TABLE_REFERENCE, "fp64": _lib.TABLE_FP64}
+_ZDM = {"callsite": _lib.ZDM_CALLSITE, "range": _lib.ZDM_RANGE, "range_ref": _lib.ZDM_RANGE_REF}
+_TABLES = {"reference": _lib.TABLE_REFERENCE, "fp64": _lib.TABLE_FP64, "ieee": _lib.TABLE_IEEE}
 _FREQ = {"header": _lib.FREQ_HEADER, "fil": _lib.FREQ_FIL}
 _NP = {8: np.uint8, 16: np.uint16, 32: np.uint32}
 
@@ -473,6 +473,24 @@ def iqrm_masks_noalloc(x, nchans: int, chan_start: int, chan_end: int, tsamp: fl
         tsamp, ctypes.byref(q), masks.data_ptr(), bounds.data_ptr(), masks.shape[0],
         ctypes.byref(n), ctypes.c_void_p(stream.cuda_stream)))
     return n.value
+
+
+def brute_delay_table(freq, chan_start: int, chan_end: int, ref_channel: int, dm_low: float,
+                      dm_step: float, dm_steps: int, tsamp: float, table_mode: str = "reference"):
+    """The brute-force delay table (include/cpucal.hpp:119-132) computed on the host
+    without a plan or a GPU (dd_brute_delay_table): an int32 array
+    [dm_steps, chan_end - chan_start] and the number of entries that differ from
+    the FP64 evaluation."""
+    f = np.ascontiguousarray(freq, dtype=np.float64)
+    if not (0 <= chan_start < chan_end <= f.size and 0 <= ref_channel < f.size):
+        raise ValueError("channel range or reference channel outside the frequency table")
+    out = np.zeros((int(dm_steps), chan_end - chan_start), np.int32)
+    mism = ctypes.c_int64()
+    _lib.check(_lib.load().dd_brute_delay_table(
+        f.ctypes.data, int(chan_start), int(chan_end), int(ref_channel), float(dm_low),
+        float(dm_step), int(dm_steps), float(tsamp), _TABLES[table_mode], out.ctypes.data,
+        ctypes.byref(mism)))
+    return out, mism.value
 
 
 def measure_int_add_rate(device: int = 0) -> float:

@@ -101,18 +101,32 @@ enum dd_zero_dm_mode {
    * subtract the mean of the non-zero values of [chan_start, chan_end) from
    * those channels and clip at zero, with the mean taken exactly
    * (v -> max(0, v - ceil(sum/count))). */
-  DD_ZDM_RANGE = 1
+  DD_ZDM_RANGE = 1,
+  /* The same range filter in the arithmetic of the reference's range kernels
+   * (rfimarker.cu:172-305): per sample a float sum of the non-zero values in
+   * the kernels' order (256 threads, channel-strided partial sums, pairwise
+   * tree), the mean by the fast-math float divide, then
+   * v -> trunc(max(0, float(v) - mean)).  Equal to DD_ZDM_RANGE while the float
+   * sums are exact and the quotient rounds the same way; it differs where the
+   * sums pass 2^24 (16-bit samples over thousands of channels). */
+  DD_ZDM_RANGE_REF = 2
 };
 
 enum dd_table_mode {
   /* Delay tables with the reference path's own arithmetic: for the subband
    * algorithm the single-precision device expressions of dedispered.cu:318-335
    * and 385-413 evaluated on the GPU with the same fast-math flags; for the
-   * brute-force algorithm the float expression of cpucal.hpp:124-131 in IEEE
-   * arithmetic. */
+   * brute-force algorithm the float expression of cpucal.hpp:124-131 compiled
+   * with the reference's host flags (-Ofast, FMA, AVX2), which reproduces the
+   * reference build's table on the same host CPU (its vector reciprocal is
+   * CPU-dependent at rounding ties). */
   DD_TABLE_REFERENCE = 0,
   /* round(4148.808*DM*(f^-2 - fref^-2)/tsamp) evaluated in FP64 on the host. */
-  DD_TABLE_FP64 = 1
+  DD_TABLE_FP64 = 1,
+  /* Brute force only: the float expression of cpucal.hpp:124-131 in strict
+   * IEEE single precision (no contraction, exact reciprocals); host-independent,
+   * and about one entry in 36,000 away from the reference build at ties. */
+  DD_TABLE_IEEE = 2
 };
 
 enum dd_freq_mode {
@@ -183,6 +197,17 @@ int dd_plan_get_info(const dd_plan* plan, dd_plan_info* info);
 /* Copy the plan's delay tables to host memory: delay is [delay_rows][delay_cols]
  * int32; residual is [dm_steps][nsb] int32 (subband only, may be NULL). */
 int dd_plan_get_tables(const dd_plan* plan, int32_t* delay, int32_t* residual);
+
+/* The brute-force delay table of the reference's CPU path (cpucal.hpp:119-132)
+ * without a plan or a GPU: table[m][c - chan_start] for DM trial m of
+ * dm_low + m*dm_step (m < dm_steps) and channel c of [chan_start, chan_end), with
+ * freq[] the channel frequencies (ascending) and the reference frequency
+ * freq[ref_channel] taken as float.  mode: DD_TABLE_REFERENCE, DD_TABLE_IEEE or
+ * DD_TABLE_FP64 as above.  *mismatch_fp64 (may be NULL) receives the number of
+ * entries that differ from the FP64 evaluation.  Host memory only. */
+int dd_brute_delay_table(const double* freq, int64_t chan_start, int64_t chan_end,
+                         int64_t ref_channel, float dm_low, float dm_step, int64_t dm_steps,
+                         double tsamp, int32_t mode, int32_t* table, int64_t* mismatch_fp64);
 
 /* Replace the brute-force delay table ([dm_steps][delay_cols] int32, host). */
 int dd_plan_set_delay_table(dd_plan* plan, const int32_t* delay);

@@ -613,6 +613,46 @@ def ref_cpu_delays(nchans, ndata, fch1, foff, tsamp, dm_low, dm_high, freq_start
     return D.astype(np.int32)
 
 
+def ref_cpu_delay_table(nchans, fch1, foff, tsamp, dm_low, dm_high, freq_start, freq_end,
+                        dm_step):
+    """The reference CPU build's [ndm, chan_end-chan_start] delay table, read one
+    channel at a time from cpucal::dedispered_fil_omp: with 32-bit samples
+    x[t][c] = t + 1 in the probed channel and zero elsewhere, output column 0 of
+    DM row m is x[delay[m][c]][c] = delay[m][c] + 1.  time_downsample equal to
+    the probe length makes that column the only one, so a probe costs ndm x nc
+    additions and a full table takes seconds even for 1000 DMs x 1000 channels.
+    Entries whose delay reaches past the probe are -1."""
+    freq = freq_table_fil(fch1, foff, nchans)
+    cs, ce = chan_range(freq, freq_start, freq_end)
+    steps = dm_steps(dm_low, dm_high, dm_step)
+    nc = ce - cs
+    dmax = int(4148.808 * max(dm_high, 0) * (1 / freq[cs] ** 2 - 1 / freq[ce] ** 2) / tsamp) + 8
+    n = dmax + 2
+    x = np.zeros((n, nchans), np.uint32)
+    ramp = np.arange(1, n + 1, dtype=np.uint32)
+    cap = steps * 4 + 64
+    out = np.zeros(cap, np.uint64)
+    cols = np.zeros(16, np.int64)
+    ns, nd = _c_long(), _c_long()
+    err = ctypes.create_string_buffer(512)
+    t_sample = n * tsamp * (1 - 1e-6)
+    D = np.empty((steps, nc), np.int64)
+    L = ref_cpu()
+    for c in range(nc):
+        x[:, cs + c] = ramp
+        rc = L.ref_cpu_dedispered_fil_omp(32, _ptr(x), n, nchans, fch1, foff, tsamp, dm_low,
+                                          dm_high, freq_start, freq_end, dm_step, n, t_sample,
+                                          _ptr(out), cap, ctypes.byref(ns), _ptr(cols), cols.size,
+                                          ctypes.byref(nd), err, 512)
+        x[:, cs + c] = 0
+        if rc:
+            raise ValueError(f"reference rejected the arguments: {err.value.decode()}")
+        if nd.value != steps or cols[0] != 1:
+            raise RuntimeError(f"probe geometry {nd.value} rows x {cols[0]} columns")
+        D[:, c] = out[:steps].astype(np.int64) - 1
+    return D.astype(np.int32)
+
+
 def ref_bruteforce_cpu(data, nchans, fch1, foff, tsamp, dm_low, dm_high, freq_start, freq_end,
                        dm_step, ds, t_sample):
     """The reference's cpucal::dedispered_fil_omp on a Filterbank built from `data`."""
@@ -686,8 +726,65 @@ def ref_gpu(sb_width: int):
         L.ref_gpu_dedispered_fil.argtypes = [
             ctypes.c_char_p, _c_float, _c_float, _c_float, _c_float, _c_float, _c_int, _c_float,
             _c_int, ctypes.c_char_p, _P, _P, _c_long, _P, _P, ctypes.c_char_p, _c_int]
+        L.ref_set_capture_sink.restype = None
+        L.ref_set_capture_sink.argtypes = [_P, _P, _c_long]
+        L.ref_capture_elem.restype = _c_long
+        L.ref_capture_elem.argtypes = []
+        L.ref_gpu_zero_dm_range.restype = _c_int
+        L.ref_gpu_zero_dm_range.argtypes = [_c_int, _P, _c_int, _c_long, _c_int, _c_int, _P,
+                                            ctypes.c_char_p, _c_int]
         _ref_gpu[sb_width] = L
     return _ref_gpu[sb_width]
+
+
+def ref_gpu_dedisperse_spec_rows(data, nchans, tsamp, fch1, foff, dm_low, dm_high, freq_start,
+                                 freq_end, dm_step, ds, rows=None, t_sample=0.5, sb_width=32,
+                                 mask_file="", use_mask=False, use_zero_dm=False, use_iqrm=False,
+                                 iq=None, device=0):
+    """Rows of the raw [dm_steps, down_ndata] output of the reference's
+    gpucal::dedisperse_spec, captured in the output's own type (uint32, or uint64
+    for 32-bit samples) without the widened host copy, so chunks of 10^9 output
+    samples fit in host memory.  rows: DM-row indices (None: all rows)."""
+    data = np.ascontiguousarray(data)
+    nbits = data.dtype.itemsize * 8
+    ndata = data.size // nchans
+    steps = dm_steps(dm_low, dm_high, dm_step)
+    cols = (ndata + ds - 1) // ds
+    sel = np.arange(steps, dtype=np.int64) if rows is None else np.asarray(rows, dtype=np.int64)
+    out = np.zeros((sel.size, cols), np.uint64 if nbits == 32 else np.uint32)
+    L = ref_gpu(sb_width)
+    nr, nc = _c_long(), _c_long()
+    err = ctypes.create_string_buffer(512)
+    r = _tap_rfi(use_mask, use_zero_dm, use_iqrm, iq)
+    L.ref_set_capture_sink(_ptr(out), _ptr(sel), 0 if rows is None else int(sel.size))
+    try:
+        rc = L.ref_gpu_dedisperse_spec(
+            nbits, _ptr(data), 0.0, tsamp, fch1, foff, nchans, ndata, dm_low, dm_high, freq_start,
+            freq_end, dm_step, ds, t_sample, device, mask_file.encode(), ctypes.byref(r), None, 0,
+            ctypes.byref(nr), ctypes.byref(nc), err, 512)
+        elem = L.ref_capture_elem()
+    finally:
+        L.ref_set_capture_sink(None, None, 0)
+    if rc:
+        raise ValueError(f"reference GPU call failed: {err.value.decode()}")
+    if (nr.value, nc.value) != (steps, cols) or elem != out.itemsize:
+        raise RuntimeError(f"reference output {nr.value}x{nc.value} of {elem}-byte elements, "
+                           f"expected {steps}x{cols} of {out.itemsize}")
+    return out
+
+
+def ref_gpu_zero_dm_range(data, nchans, chan_start, chan_end, sb_width=32):
+    """The reference's range zero-DM filter (RfiMarker<T>::zero_dm_filter with a
+    channel range, src/rfi/rfimarker.cu:257-305) applied to a copy of `data`."""
+    data = np.ascontiguousarray(data)
+    out = np.empty_like(data)
+    err = ctypes.create_string_buffer(512)
+    rc = ref_gpu(sb_width).ref_gpu_zero_dm_range(data.dtype.itemsize * 8, _ptr(data), nchans,
+                                                 data.size // nchans, chan_start, chan_end,
+                                                 _ptr(out), err, 512)
+    if rc:
+        raise ValueError(f"reference zero-DM failed: {err.value.decode()}")
+    return out
 
 
 def ref_gpu_dedisperse_spec(data, nchans, tsamp, fch1, foff, dm_low, dm_high, freq_start,

@@ -221,6 +221,52 @@ int run_rfi(const void* data, float tsamp, float fch1, float foff, int nchans, l
 
 extern "C" int ref_gpu_subband_width(void) { return AF_SUBBAND_SIZE_CH; }
 
+// Direct capture of the next calls' raw sums (see RefCapture::sink): rows
+// `rows[0..nrows)` (all rows when nrows is 0) into `sink` in the output's own
+// element type; NULL sink turns it off.  Returns nothing; ref_capture_elem()
+// reports the element size the last captured call wrote.
+extern "C" void ref_set_capture_sink(void* sink, const long* rows, long nrows) {
+  RefCapture& cap = ref_capture();
+  cap.sink = sink;
+  cap.sink_rows = rows;
+  cap.sink_nrows = nrows;
+  cap.sink_elem = 0;
+}
+extern "C" long ref_capture_elem(void) { return static_cast<long>(ref_capture().sink_elem); }
+
+// The reference's range zero-DM filter, RfiMarker<T>::zero_dm_filter(d, num_channels,
+// num_samples, chan_start, chan_end, alpha, clip_to_zero) (src/rfi/rfimarker.cu:257-305),
+// which no reference call site reaches, run on a device copy of `data`
+// ([nsamp][nchans], host) with the default alpha 1 and clipping; the filtered
+// samples are copied back into `out`.
+template <typename T>
+int run_zdm_range(const void* data, int nchans, long nsamp, int chan_start, int chan_end,
+                  void* out, char* err, int errlen) {
+  T* d = nullptr;
+  const size_t bytes = static_cast<size_t>(nsamp) * nchans * sizeof(T);
+  TAP_CUDA(cudaMalloc(&d, bytes));
+  TAP_CUDA(cudaMemcpy(d, data, bytes, cudaMemcpyHostToDevice));
+  RfiMarker<T> marker{std::string("")};
+  marker.zero_dm_filter(d, static_cast<unsigned int>(nchans), static_cast<unsigned int>(nsamp),
+                        static_cast<unsigned int>(chan_start), static_cast<unsigned int>(chan_end));
+  TAP_CUDA(cudaDeviceSynchronize());
+  TAP_CUDA(cudaMemcpy(out, d, bytes, cudaMemcpyDeviceToHost));
+  TAP_CUDA(cudaFree(d));
+  return 0;
+}
+
+extern "C" int ref_gpu_zero_dm_range(int nbits, const void* data, int nchans, long nsamp,
+                                     int chan_start, int chan_end, void* out, char* err,
+                                     int errlen) {
+  switch (nbits) {
+    case 8: return run_zdm_range<uint8_t>(data, nchans, nsamp, chan_start, chan_end, out, err, errlen);
+    case 16: return run_zdm_range<uint16_t>(data, nchans, nsamp, chan_start, chan_end, out, err, errlen);
+    case 32: return run_zdm_range<uint32_t>(data, nchans, nsamp, chan_start, chan_end, out, err, errlen);
+  }
+  std::snprintf(err, errlen, "unsupported nbits");
+  return 5;
+}
+
 extern "C" int ref_gpu_dedisperse_spec(int nbits, const void* data, float mjd, float tsamp,
                                        float fch1, float foff, int nchans, long ndata,
                                        float dm_low, float dm_high, float freq_start,

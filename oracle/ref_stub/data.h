@@ -97,6 +97,15 @@ struct RefCapture {
   size_t rows = 0;
   size_t cols = 0;
   void clear() { u64.clear(); typed.clear(); rows = cols = 0; }
+  // Optional direct sink for the GPU path's array, set by the harness before a
+  // call and kept across clear(): rows sink_rows[0..sink_nrows) (all rows when
+  // sink_nrows is 0) are copied into `sink` as [n][cols] in the array's own
+  // element type (sink_elem bytes), and the widened copy is skipped.  Large
+  // chunks need this: the widened copy of a full chunk would not fit in host memory.
+  void* sink = nullptr;
+  const long* sink_rows = nullptr;
+  long sink_nrows = 0;
+  size_t sink_elem = 0;
 };
 inline RefCapture& ref_capture() { static RefCapture c; return c; }
 
@@ -125,6 +134,19 @@ inline dedisperseddata_uint8 preprocess_typed_dedisperseddata_with_slicing(
   cap.clear();
   cap.rows = in.shape.at(0);
   cap.cols = in.shape.at(1);
+  if (cap.sink) {
+    using Out = dedispersion_output_t<InputType>;
+    const Out* src = in.dm_times.at(0).get();
+    cap.sink_elem = sizeof(Out);
+    const size_t n = cap.sink_nrows > 0 ? static_cast<size_t>(cap.sink_nrows) : cap.rows;
+    for (size_t i = 0; i < n; ++i) {
+      const size_t r = cap.sink_nrows > 0 ? static_cast<size_t>(cap.sink_rows[i]) : i;
+      if (r >= cap.rows) continue;
+      std::memcpy(static_cast<char*>(cap.sink) + i * cap.cols * sizeof(Out), src + r * cap.cols,
+                  cap.cols * sizeof(Out));
+    }
+    return dedisperseddata_uint8{};
+  }
 #ifdef REF_CAPTURE_DIMS_ONLY
   // timing build: keep the dimensions only (no host copy of the sums)
   return dedisperseddata_uint8{};

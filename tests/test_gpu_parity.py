@@ -70,7 +70,9 @@ def test_brute_force_matches_oracle(case):
     freq = O.freq_table_fil(fch1, foff, nchans)
     fs, fe = float(F32(freq[0])), float(F32(freq[-1]))
     hdr = dict(tsamp=tsamp, fch1=fch1, foff=foff, nbits=nbits, nchans=nchans, ndata=N)
-    plan = Plan(hdr, lo, hi, fs, fe, step, ds, tslice, algorithm="brute", freq_mode="fil")
+    # the oracle restates the table in IEEE arithmetic: compare with that mode
+    plan = Plan(hdr, lo, hi, fs, fe, step, ds, tslice, algorithm="brute", freq_mode="fil",
+                table_mode="ieee")
     out = to_np(plan.run(dev(x)))
     ref = np.concatenate(O.bruteforce_cpu(x, nchans, freq, tsamp, lo, hi, fs, fe, step, ds, tslice), axis=1)
     d, _ = plan.tables()
