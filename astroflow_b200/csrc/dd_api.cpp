@@ -60,6 +60,10 @@ bool stage1_flush(const dd_plan& P) {
 }
 
 // ---- frequency table and band (dedispered.cu:1003-1031, cpucal.hpp:85-116)
+// Kernel variant of stage 2: 16-bit subband sums (8-bit input, subbands of at
+// most 64 channels) four per pipeline stage, else 32-bit sums.
+int stage2_kind(const dd_plan& P) { return P.inter16 ? kSumKindU16Quad : kSumKindU32; }
+
 void build_freq(dd_plan& P) {
   const int n = P.hdr.nchans;
   P.freq.resize(n);
@@ -280,9 +284,9 @@ int table_spread(const std::vector<int32_t>& tab, int64_t nrows, int64_t ncols, 
 // Bytes of one staged window: the tile plus the rows' spread, 16-byte alignment
 // slack and the funnel shift's extra word; 0 when the four windows of a block
 // would not fit comfortably in shared memory.
-int window_bytes(int spread, int tile, int elem) {
+int window_bytes(int spread, int tile, int elem, int qs = 2) {
   const int64_t w = round_up(static_cast<int64_t>(spread + tile) * elem + 40, 16);
-  return sum_smem_bytes(static_cast<int>(w), 2) <= 200 * 1024 ? static_cast<int>(w) : 0;
+  return sum_smem_bytes(static_cast<int>(w), 2, qs) <= 200 * 1024 ? static_cast<int>(w) : 0;
 }
 
 void upload_desc(DevBuf& b, const std::vector<SumDesc>& d) {
@@ -327,7 +331,7 @@ void set_tiling(dd_plan& P, int64_t budget) {
   P.inter_budget = budget;
   // Stage-2 blocks past the tile's last column read up to one block tile beyond it
   // (their columns are not stored).
-  const int64_t T2 = P.win2 ? sum_variant_tile(static_cast<int>(inter_elem(P)), false) : kT;
+  const int64_t T2 = P.win2 ? sum_kind_tile(stage2_kind(P)) : kT;
   P.tile_pitch = round_up(round_up(L + P.max_res, kT) + T2 + 64, 64);
   const int64_t ntiles = (P.nbin + L - 1) / L;
   P.xpitch = round_up(ntiles * L + round_up(L + P.max_res, 8192) + P.max_delay + 8192, 64);
@@ -396,9 +400,9 @@ void create_subband(dd_plan& P) {
   if (mind < 0 || minr < 0)
     throw invalid("negative dispersion delays (DM below zero or band order) are not supported");
 #ifndef DD_INTER32
-#define DD_INTER32 1
+#define DD_INTER32 0
 #endif
-  P.inter16 = (P.nbits == 8 && P.sbw <= 257 && !DD_INTER32) ? 1 : 0;
+  P.inter16 = (P.nbits == 8 && P.sbw <= 64 && !DD_INTER32) ? 1 : 0;
   if (P.nbits <= 16) {
     const int T1 = sum_variant_tile(P.elem, stage1_flush(P));
     P.win1 = window_bytes(table_spread(P.h_delay, P.ndm_nom, P.dch, kSumRows, 0), T1, P.elem);
@@ -406,8 +410,9 @@ void create_subband(dd_plan& P) {
   if (P.nbits <= 16) {
     // stage-2 sources: the stage-1 sums (uint16 or uint32)
     const int e2 = static_cast<int>(inter_elem(P));
-    const int T2 = sum_variant_tile(e2, false);
-    P.win2 = window_bytes(table_spread(P.h_res, P.dm_steps, P.nsb, kSumRows, P.ndm0), T2, e2);
+    const int T2 = sum_kind_tile(stage2_kind(P));
+    P.win2 = window_bytes(table_spread(P.h_res, P.dm_steps, P.nsb, kSumRows, P.ndm0), T2, e2,
+                          sum_kind_qs(stage2_kind(P)));
   }
   if (P.win1) upload_desc(P.d_desc1, build_sum_desc(P.h_delay, P.ndm_nom, P.dch, 0));
   if (P.win2) upload_desc(P.d_desc2, build_sum_desc(P.h_res, P.dm_steps, P.nsb, P.ndm0));
@@ -637,12 +642,12 @@ SumLaunch stage2_launch(const dd_plan& P, int64_t t0, void* output, int buf = 0)
   L.win_bytes = P.win2;
   L.src_bytes = static_cast<int>(inter_elem(P));
   L.flush = 0;
-  L.lane_per = P.inter16 ? 65535 / (255 * P.sbw) : 1;
+  L.lane_per = P.inter16 ? 65535 / (255 * P.sbw) : 1;  // >= 4 for subbands of <= 64 channels
   L.grid_y = static_cast<unsigned>(P.ndm_nom * ((P.ndm0 + kSumRows - 1) / kSumRows));
   L.grid_z = 1;
   L.desc = P.d_desc2.as<SumDesc>();
   L.desc_pitch = P.nsb;
-  L.stages = P.stages_override ? P.stages_override : sum_stages(P.win2);
+  L.stages = P.stages_override ? P.stages_override : sum_stages(P.win2, sum_kind_qs(stage2_kind(P)));
   L.err = P.d_err.as<int>();
   L.one = 1;
   return L;
@@ -1125,7 +1130,8 @@ int dd_plan_autotune(dd_plan* P, const void* input, void* output, int32_t reps, 
     // stage counts that keep two blocks per SM for both stages
     auto fits = [&](int S) {
       return S >= 2 && S <= kSumMaxStages &&
-             sum_smem_bytes(P->win1, S) <= 113 * 1024 && sum_smem_bytes(P->win2, S) <= 113 * 1024;
+             sum_smem_bytes(P->win1, S) <= 113 * 1024 &&
+             sum_smem_bytes(P->win2, S, sum_kind_qs(stage2_kind(*P))) <= 113 * 1024;
     };
     const int64_t budget0 = P->inter_budget;
     const int stages0 = P->stages_override;
@@ -1334,7 +1340,7 @@ namespace {
 // Shared memory of a staged sum that leaves two persistent blocks per SM.
 constexpr size_t kBatchSmemCap = 100 * 1024;
 
-size_t win_smem(int win) { return win ? sum_smem_bytes(win, sum_stages(win)) : 0; }
+size_t win_smem(int win, int qs = 2) { return win ? sum_smem_bytes(win, sum_stages(win, qs), qs) : 0; }
 
 // Whether plan P's sums run in the batched launches.
 bool batched_plan(const dd_plan& P, bool persistent) {
@@ -1343,7 +1349,8 @@ bool batched_plan(const dd_plan& P, bool persistent) {
   if (brute ? !P.winb : (!P.win1 || !P.win2)) return false;
   if (!persistent) return true;
   return brute ? win_smem(P.winb) <= kBatchSmemCap
-               : win_smem(P.win1) <= kBatchSmemCap && win_smem(P.win2) <= kBatchSmemCap;
+               : win_smem(P.win1) <= kBatchSmemCap &&
+                     win_smem(P.win2, sum_kind_qs(stage2_kind(P))) <= kBatchSmemCap;
 }
 
 long long group_blocks(const SumBatchGroup& g) {
@@ -1407,7 +1414,7 @@ void build_groups(dd_batch& B, void* const* outputs) {
         g.first = la.blocks;
         g.done_ctr = B.nctrs++;
         la.blocks += group_blocks(g);
-        la.smem = std::max(la.smem, sum_smem_bytes(L.win_bytes, L.stages));
+        la.smem = std::max(la.smem, sum_launch_smem(L));
         if (!brute) {
           (s1 ? s1_ctr[p] : prev_ctr[p]) = g.done_ctr;
           (s1 ? s1_need[p] : prev_need[p]) = static_cast<int>(group_blocks(g));
@@ -1431,7 +1438,7 @@ void build_groups(dd_batch& B, void* const* outputs) {
           la.kind = kind;
           for (auto& [p, L] : list) {
             SumBatchGroup g = make_group(L);
-            const size_t sm = sum_smem_bytes(L.win_bytes, L.stages);
+            const size_t sm = sum_launch_smem(L);
             if (g.kind != kind || (sm > kBatchSmemCap) != (wide != 0)) continue;
             g.first = la.blocks;
             la.blocks += group_blocks(g);

@@ -289,9 +289,10 @@ constexpr int kSumMaxStages = DD_SUM_MAX_STAGES;  // staged source pairs in flig
 void launch_sum(const SumLaunch& L, cudaStream_t st);
 int sum_tile_samples(int src_bytes, int nw);
 // Shared memory of a staged sum with `stages` pairs in flight.
-size_t sum_smem_bytes(int win_bytes, int stages);
+// qs: source windows per pipeline stage (2, or 4 for the quad kernel).
+size_t sum_smem_bytes(int win_bytes, int stages, int qs = 2);
 // Pairs in flight that fit the shared memory of two blocks per SM (at least 2).
-int sum_stages(int win_bytes);
+int sum_stages(int win_bytes, int qs = 2);
 // Descriptors of a [nrows][ncols] offset table for row groups of kSumRows rows,
 // grouped within blocks of `group` rows (0: one block), in the launch's
 // blockIdx.y order.  Fails if a group's spread exceeds 65535.
@@ -329,6 +330,11 @@ constexpr int kSum32NW = DD_SUM32_NW;  // words per lane of the 32-bit staged su
 #ifndef DD_SUM16W_NW
 #define DD_SUM16W_NW 5
 #endif
+// Words per lane of the 16-bit quad stage-2 kernel (odd: conflict-free consecutive words).
+#ifndef DD_SUM16Q_NW
+#define DD_SUM16Q_NW 5
+#endif
+constexpr int kSum16QNW = DD_SUM16Q_NW;
 // flush: 8-bit sources widened every 256 sources; 16-bit sources summed into
 // 32-bit lanes (the k_sum_u16w variant).
 inline int sum_variant_tile(int src_bytes, bool flush) {
@@ -336,12 +342,28 @@ inline int sum_variant_tile(int src_bytes, bool flush) {
                                      : src_bytes == 2 ? (flush ? DD_SUM16W_NW : DD_SUM16_NW)
                                                       : (flush ? DD_SUM8F_NW : DD_SUM8_NW));
 }
+// Tile (samples per block) of a kernel variant (SumKind below).
+inline int sum_kind_tile(int kind);
 // Kernel variant of a staged sum: 8-bit sources into 16-bit sums, 8-bit sources
 // widened to 32 bits (many sources), 8-bit, 16-bit and 32-bit sources.
 enum SumKind { kSumKindU8Out16 = 0, kSumKindU8Flush = 1, kSumKindU8 = 2, kSumKindU16 = 3,
-               kSumKindU32 = 4, kSumKindU16Wide = 5 };
-constexpr int kSumKinds = 6;
+               kSumKindU32 = 4, kSumKindU16Wide = 5, kSumKindU16Quad = 6 };
+constexpr int kSumKinds = 7;
 int sum_kind(const SumLaunch& L);
+inline int sum_kind_tile(int kind) {
+  switch (kind) {
+    case kSumKindU8Out16: case kSumKindU8: return sum_tile_samples(1, DD_SUM8_NW);
+    case kSumKindU8Flush: return sum_tile_samples(1, DD_SUM8F_NW);
+    case kSumKindU16: return sum_tile_samples(2, DD_SUM16_NW);
+    case kSumKindU16Wide: return sum_tile_samples(2, DD_SUM16W_NW);
+    case kSumKindU16Quad: return sum_tile_samples(2, kSum16QNW);
+    default: return sum_tile_samples(4, kSum32NW);
+  }
+}
+// Source windows per pipeline stage of a kernel variant (4 for kSumKindU16Quad, else 2).
+inline int sum_kind_qs(int kind) { return kind == kSumKindU16Quad ? 4 : 2; }
+// Shared memory of a launch (its variant's windows per stage).
+size_t sum_launch_smem(const SumLaunch& L);
 // Stage 1 of one tile and stage 2 of another in one launch (false: no paired
 // kernel for these variants; nothing launched).
 bool launch_sum_pair(const SumLaunch& L1, const SumLaunch& L2, cudaStream_t st);

@@ -172,26 +172,30 @@ __device__ __forceinline__ Geo make_geo(const SumLaunch& L, int T, uint3 blk) {
   return g;
 }
 
-// Shared state of the pipeline.
-struct Pipe {
-  uint64_t full[kMaxStages];   // completes when a stage's two windows have landed
+// Shared state of the pipeline.  A stage holds QS (2 or 4) source windows.
+struct __align__(16) Pipe {
+  uint64_t full[kMaxStages];   // completes when a stage's windows have landed
   uint64_t empty[kMaxStages];  // completes when all warps released a stage
-  // per row: word index and shift (bits) of sample 0 in source 0's window, then
-  // the same for source 1
-  int4 row[kMaxStages][kSumRows];
+  // per row: word index and shift (bits) of sample 0 in the window of source
+  // i of the stage at [2i], [2i+1]
+  int row[kMaxStages][kSumRows][8];
   int failed;
 };
+__device__ __forceinline__ int4 row_pair(const Pipe& P, int s, int r, int half) {
+  return *reinterpret_cast<const int4*>(&P.row[s][r][4 * half]);
+}
 
-// Producer step for source pair q in stage s (warp 0, lanes 0 and 1; lane l
-// handles source 2q + l).  The caller has made sure stage s is free.
-template <int SB>
+// Producer step for source group q in stage s (warp 0, lanes 0..QS-1; lane l
+// handles source QS*q + l).  The caller has made sure stage s is free.
+template <int SB, int QS>
 __device__ __forceinline__ void produce(const Geo& g, Pipe& P, uint32_t* sw, int ww, int zero_q,
                                         int tile_bytes, int q, int s, int lane) {
-  const int src = 2 * q + lane;
+  const int src = QS * q + lane;
   uint32_t nbytes = 0;
   const char* gsrc = nullptr;
-  uint32_t* dst = sw + (2 * s + lane) * ww;
-  if (lane < 2) {
+  uint32_t* dst = sw + (QS * s + lane) * ww;
+  if (lane < QS) {
+    int* rw = &P.row[s][0][0] + 2 * lane;
     if (src < g.nsrc) {
       const SumDesc d = g.desc[src];
       const int64_t first = (g.base + d.lo) * SB;
@@ -199,42 +203,41 @@ __device__ __forceinline__ void produce(const Geo& g, Pipe& P, uint32_t* sw, int
       const int64_t last = (g.base + d.lo + d.span) * SB + tile_bytes + 8;  // + funnel word
       nbytes = static_cast<uint32_t>((last - a0 + 15) & ~int64_t(15));
       gsrc = g.src + static_cast<int64_t>(src) * g.src_pitch + a0;
-      const int qbase = (2 * s + lane) * ww;
+      const int qbase = (QS * s + lane) * ww;
       const int ob0 = static_cast<int>(first - a0);
-      int* rw = reinterpret_cast<int*>(P.row[s]) + 2 * lane;
 #pragma unroll
       for (int r = 0; r < kSumRows; ++r) {
         // rows past nrows take offset lo (rel 0): their reads stay in the window
         const int ob = ob0 + (r < g.nrows ? static_cast<int>(d.rel[r]) : 0) * SB;
-        rw[4 * r] = qbase + (ob >> 2);
-        rw[4 * r + 1] = (ob & 3) * 8;
+        rw[8 * r] = qbase + (ob >> 2);
+        rw[8 * r + 1] = (ob & 3) * 8;
       }
     } else {
-      int* rw = reinterpret_cast<int*>(P.row[s]) + 2 * lane;
 #pragma unroll
       for (int r = 0; r < kSumRows; ++r) {
-        rw[4 * r] = zero_q;
-        rw[4 * r + 1] = 0;
+        rw[8 * r] = zero_q;
+        rw[8 * r + 1] = 0;
       }
     }
   }
-  const uint32_t other = __shfl_xor_sync(0xffffffffu, nbytes, 1);
+  uint32_t total = nbytes + __shfl_xor_sync(0xffffffffu, nbytes, 1);
+  if (QS == 4) total += __shfl_xor_sync(0xffffffffu, total, 2);
   __syncwarp();
-  if (lane == 0) mbar_arrive_expect_tx(&P.full[s], nbytes + other);
+  if (lane == 0) mbar_arrive_expect_tx(&P.full[s], total);
   __syncwarp();
-  if (lane < 2 && nbytes) bulk_copy(dst, gsrc, nbytes, &P.full[s]);
+  if (lane < QS && nbytes) bulk_copy(dst, gsrc, nbytes, &P.full[s]);
 }
 
 // Pipeline driver shared by the kernels: calls body(stage, cur) for every
-// source pair once its windows are in shared memory.
-template <int SB, typename Body>
+// group of QS sources once their windows are in shared memory.
+template <int SB, int QS = 2, typename Body>
 __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, Pipe& P,
                                              uint32_t* sw, int tile_bytes, Body&& body) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ww = L.win_bytes >> 2;
   const int S = L.stages;
-  const int zero_q = 2 * S * ww;
-  const int npairs = (g.nsrc + 1) / 2;
+  const int zero_q = QS * S * ww;
+  const int npairs = (g.nsrc + QS - 1) / QS;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&P.full[s], 1);
@@ -252,7 +255,7 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
   int issued = 0;  // pairs whose copies warp 0 has issued
   if (warp == 0)
     for (; issued < min(S - 1, npairs); ++issued)
-      produce<SB>(g, P, sw, ww, zero_q, tile_bytes, issued, issued, lane);
+      produce<SB, QS>(g, P, sw, ww, zero_q, tile_bytes, issued, issued, lane);
   int s_cur = 0, p = 0;
   uint32_t ph_cur = 0;
   for (; p < npairs; ++p) {
@@ -271,7 +274,7 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
         }
         break;
       }
-      produce<SB>(g, P, sw, ww, zero_q, tile_bytes, q, s, lane);
+      produce<SB, QS>(g, P, sw, ww, zero_q, tile_bytes, q, s, lane);
       ++issued;
     }
     const bool ok = mbar_wait(&P.full[s_cur], ph_cur, failed, L.err);
@@ -338,7 +341,7 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
   run_pipeline<1>(L, g, P, sw, T, [&](int s, const uint32_t* win) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
-      const int4 rw = P.row[s][r];
+      const int4 rw = row_pair(P, s, r, 0);
       const uint32_t* w0 = win + rw.x + wbase;
       const uint32_t* w1 = win + rw.z + wbase;
       uint32_t va[NW + 1], vb[NW + 1];
@@ -443,7 +446,7 @@ __device__ __forceinline__ void sum_u16(const SumLaunch& L, uint3 blk, uint32_t*
     if (per >= 2) {
 #pragma unroll
       for (int r = 0; r < RB; ++r) {
-        const int4 rw = P.row[s][r];
+        const int4 rw = row_pair(P, s, r, 0);
         const uint32_t* w0 = win + rw.x + wbase;
         const uint32_t* w1 = win + rw.z + wbase;
         if ((rw.y | rw.w) == 0) {  // both sources word-aligned (uniform over the block)
@@ -481,7 +484,7 @@ __device__ __forceinline__ void sum_u16(const SumLaunch& L, uint3 blk, uint32_t*
     } else {
 #pragma unroll
       for (int r = 0; r < RB; ++r) {
-        const int4 rw = P.row[s][r];
+        const int4 rw = row_pair(P, s, r, 0);
         const uint32_t* w0 = win + rw.x + wbase;
         const uint32_t* w1 = win + rw.z + wbase;
 #pragma unroll
@@ -537,7 +540,7 @@ __device__ __forceinline__ void sum_u16_wide(const SumLaunch& L, uint3 blk, uint
   run_pipeline<2>(L, g, P, sw, 2 * T, [&](int s, const uint32_t* win) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
-      const int4 rw = P.row[s][r];
+      const int4 rw = row_pair(P, s, r, 0);
       const uint32_t* w0 = win + rw.x + wbase;
       const uint32_t* w1 = win + rw.z + wbase;
       uint32_t va[NW + 1], vb[NW + 1];
@@ -602,7 +605,7 @@ __device__ __forceinline__ void sum_u32(const SumLaunch& L, uint3 blk, uint32_t*
   run_pipeline<4>(L, g, P, sw, 4 * T, [&](int s, const uint32_t* win) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
-      const int4 rw = P.row[s][r];
+      const int4 rw = row_pair(P, s, r, 0);
       const uint32_t* w0 = win + rw.x + wbase;
       const uint32_t* w1 = win + rw.z + wbase;
 #pragma unroll
@@ -618,6 +621,82 @@ __device__ __forceinline__ void sum_u32(const SumLaunch& L, uint3 blk, uint32_t*
     for (int k = 0; k < NW; ++k) {
       const int64_t t = wbase + 32 * k;
       if (t < g.valid) row[t] = acc[r][k];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ 16-bit sums, four sources per stage
+// Stage 2 of 8-bit input: sources are 16-bit subband sums of at most 64 channels
+// (each <= 64 x 255 = 16320), so the sum of four of them still fits a 16-bit lane
+// (<= 65280).  A lane owns NW consecutive 32-bit words of the block's tile (two
+// samples each); per row and group of four sources it adds the four aligned
+// words in packed 16-bit lanes (a source offset by one sample is aligned with a
+// byte permute of two neighbouring words), then folds the packed sum q into two
+// 32-bit accumulators: lo += q (wrapping) and hi += q >> 16 (a multiply-high on
+// the FMA pipe).  Since no group's low lane carries, the low samples' sum is
+// lo - (hi << 16) at the end.  Shared-memory bytes per sample addition are
+// about half those of 32-bit subband sums.
+template <int NW>
+__device__ __forceinline__ void add_u16_src(uint32_t (&q)[NW], const uint32_t* w, int shift) {
+  if (shift == 0) {  // uniform over the block: the source's offset is even
+#pragma unroll
+    for (int k = 0; k < NW; ++k) q[k] += w[k];
+  } else {
+    uint32_t v[NW + 1];
+#pragma unroll
+    for (int i = 0; i <= NW; ++i) v[i] = w[i];
+#pragma unroll
+    for (int k = 0; k < NW; ++k) q[k] += __byte_perm(v[k], v[k + 1], 0x5432);
+  }
+}
+
+template <int RB, int NW>
+__device__ __forceinline__ void sum_u16_quad(const SumLaunch& L, uint3 blk, uint32_t* sw, Pipe& P) {
+  static_assert(NW & 1, "an odd number of consecutive words per lane keeps the loads conflict-free");
+  constexpr int T = kWarps * 32 * NW * 2;
+  const Geo g = make_geo(L, T, blk);
+  if (g.nrows <= 0) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wbase = warp * 32 * NW + lane * NW;
+  uint32_t lo[RB][NW], hi[RB][NW];
+#pragma unroll
+  for (int r = 0; r < RB; ++r)
+#pragma unroll
+    for (int k = 0; k < NW; ++k) lo[r][k] = hi[r][k] = 0;
+  run_pipeline<2, 4>(L, g, P, sw, 2 * T, [&](int s, const uint32_t* win) {
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+      const int4 a = row_pair(P, s, r, 0), b = row_pair(P, s, r, 1);
+      uint32_t q[NW];
+#pragma unroll
+      for (int k = 0; k < NW; ++k) q[k] = 0;
+      add_u16_src<NW>(q, win + a.x + wbase, a.y);
+      add_u16_src<NW>(q, win + a.z + wbase, a.w);
+      add_u16_src<NW>(q, win + b.x + wbase, b.y);
+      add_u16_src<NW>(q, win + b.z + wbase, b.w);
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        lo[r][k] += q[k];
+        hi[r][k] = __umulhi(q[k], 0x10000u) + hi[r][k];
+      }
+    }
+  });
+  if (P.failed) return;
+#pragma unroll
+  for (int r = 0; r < RB; ++r) {
+    if (r >= g.nrows) break;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      const int64_t t = static_cast<int64_t>(wbase + k) * 2;
+      if (t >= g.valid) continue;
+      const uint32_t s0 = lo[r][k] - (hi[r][k] << 16), s1 = hi[r][k];
+      uint32_t* dst = reinterpret_cast<uint32_t*>(g.out + r * g.out_pitch) + t;
+      if (t + 2 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
+        *reinterpret_cast<uint2*>(dst) = make_uint2(s0, s1);
+      } else {
+        dst[0] = s0;
+        if (t + 1 < g.valid) dst[1] = s1;
+      }
     }
   }
 }
@@ -639,6 +718,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_sum_u16w(SumLaunch L) {
   extern __shared__ __align__(128) uint32_t sw[];
   __shared__ Pipe P;
   sum_u16_wide<RB, NW>(L, blockIdx, sw, P);
+}
+template <int RB, int NW>
+__global__ void __launch_bounds__(kThreads, 2) k_sum_u16q(SumLaunch L) {
+  extern __shared__ __align__(128) uint32_t sw[];
+  __shared__ Pipe P;
+  sum_u16_quad<RB, NW>(L, blockIdx, sw, P);
 }
 template <int RB, int NW>
 __global__ void __launch_bounds__(kThreads, DD_SUM32_MINB) k_sum_u32(SumLaunch L) {
@@ -682,6 +767,7 @@ __device__ __forceinline__ void run_one(const SumLaunch& L, uint3 blk, uint32_t*
   else if constexpr (KIND == kSumKindU8) sum_u8<kSumRows, DD_SUM8_NW, false, false>(L, blk, sw, P);
   else if constexpr (KIND == kSumKindU16) sum_u16<kSumRows, DD_SUM16_NW>(L, blk, sw, P);
   else if constexpr (KIND == kSumKindU16Wide) sum_u16_wide<kSumRows, DD_SUM16W_NW>(L, blk, sw, P);
+  else if constexpr (KIND == kSumKindU16Quad) sum_u16_quad<kSumRows, kSum16QNW>(L, blk, sw, P);
   else sum_u32<kSumRows, kSum32NW>(L, blk, sw, P);
 }
 
@@ -716,6 +802,7 @@ __device__ __forceinline__ void run_kind(int kind, const SumLaunch& L, uint3 blk
     case kSumKindU8: run_one<kSumKindU8>(L, blk, sw, P); break;
     case kSumKindU16: run_one<kSumKindU16>(L, blk, sw, P); break;
     case kSumKindU16Wide: run_one<kSumKindU16Wide>(L, blk, sw, P); break;
+    case kSumKindU16Quad: run_one<kSumKindU16Quad>(L, blk, sw, P); break;
     default: run_one<kSumKindU32>(L, blk, sw, P); break;
   }
 }
@@ -788,9 +875,13 @@ void launch_k(K kernel, dim3 grid, size_t smem, const SumLaunch& L, cudaStream_t
 
 int sum_tile_samples(int src_bytes, int nw) { return kWarps * 32 * nw * (4 / src_bytes); }
 
-// Ring of `stages` window pairs plus one zeroed window.
-size_t sum_smem_bytes(int win_bytes, int stages) {
-  return static_cast<size_t>(2 * stages + 1) * win_bytes;
+// Ring of `stages` groups of qs windows plus one zeroed window.
+size_t sum_smem_bytes(int win_bytes, int stages, int qs) {
+  return static_cast<size_t>(qs * stages + 1) * win_bytes;
+}
+
+size_t sum_launch_smem(const SumLaunch& L) {
+  return sum_smem_bytes(L.win_bytes, L.stages, sum_kind_qs(sum_kind(L)));
 }
 
 #ifndef DD_SUM_SMEM_KB
@@ -798,9 +889,9 @@ size_t sum_smem_bytes(int win_bytes, int stages) {
 #endif
 // Staged source pairs for a window size: as many as fit DD_SUM_SMEM_KB of shared
 // memory (two blocks per SM at the default), at least two.
-int sum_stages(int win_bytes) {
+int sum_stages(int win_bytes, int qs) {
   int s = kMaxStages;
-  while (s > 2 && sum_smem_bytes(win_bytes, s) > DD_SUM_SMEM_KB * 1024) --s;
+  while (s > 2 && sum_smem_bytes(win_bytes, s, qs) > DD_SUM_SMEM_KB * 1024) --s;
   return s;
 }
 
@@ -839,7 +930,7 @@ void launch_sum(const SumLaunch& L, cudaStream_t st) {
   dim3 grid(sum_grid_x(L), L.grid_y, L.grid_z);
   if (L.stages < 2 || L.stages > kMaxStages) throw Error{DD_ERR_RUNTIME, "bad stage count"};
   if (!L.desc || !L.err) throw Error{DD_ERR_RUNTIME, "staged sum without descriptors"};
-  const size_t smem = sum_smem_bytes(L.win_bytes, L.stages);
+  const size_t smem = sum_launch_smem(L);
   if (L.rows_per_block != kSumRows) throw Error{DD_ERR_RUNTIME, "unsupported rows per block"};
   switch (sum_kind(L)) {
     case kSumKindU8Out16: launch_k(k_sum_u8<kSumRows, DD_SUM8_NW, true, false>, grid, smem, L, st); break;
@@ -847,6 +938,7 @@ void launch_sum(const SumLaunch& L, cudaStream_t st) {
     case kSumKindU8: launch_k(k_sum_u8<kSumRows, DD_SUM8_NW, false, false>, grid, smem, L, st); break;
     case kSumKindU16: launch_k(k_sum_u16<kSumRows, DD_SUM16_NW>, grid, smem, L, st); break;
     case kSumKindU16Wide: launch_k(k_sum_u16w<kSumRows, DD_SUM16W_NW>, grid, smem, L, st); break;
+    case kSumKindU16Quad: launch_k(k_sum_u16q<kSumRows, kSum16QNW>, grid, smem, L, st); break;
     default: launch_k(k_sum_u32<kSumRows, kSum32NW>, grid, smem, L, st); break;
   }
 }
@@ -856,12 +948,12 @@ int sum_kind(const SumLaunch& L) {
     if (L.out_elem == 2) return kSumKindU8Out16;
     return L.flush ? kSumKindU8Flush : kSumKindU8;
   }
-  if (L.src_bytes == 2) return L.flush ? kSumKindU16Wide : kSumKindU16;
+  if (L.src_bytes == 2) return L.flush ? kSumKindU16Wide : L.lane_per >= 4 ? kSumKindU16Quad : kSumKindU16;
   return kSumKindU32;
 }
 
 unsigned sum_grid_x(const SumLaunch& L) {
-  const int T = sum_variant_tile(L.src_bytes, L.flush && L.out_elem != 2);
+  const int T = sum_kind_tile(sum_kind(L));
   return static_cast<unsigned>((L.ncols + T - 1) / T);
 }
 
@@ -924,8 +1016,7 @@ void launch_pair_k(const SumLaunch& L1, const SumLaunch& L2, cudaStream_t st) {
   const unsigned gx1 = sum_grid_x(L1), gx2 = sum_grid_x(L2);
   const long long n1 = static_cast<long long>(gx1) * L1.grid_y * L1.grid_z;
   const long long n2 = static_cast<long long>(gx2) * L2.grid_y * L2.grid_z;
-  const size_t smem = std::max(sum_smem_bytes(L1.win_bytes, L1.stages),
-                               sum_smem_bytes(L2.win_bytes, L2.stages));
+  const size_t smem = std::max(sum_launch_smem(L1), sum_launch_smem(L2));
   if (n1 + n2 >= (1LL << 31)) throw Error{DD_ERR_RUNTIME, "paired launch too large"};
   if (smem > 48 * 1024)
     DD_CUDA_TRY(cudaFuncSetAttribute(k_sum_pair<K1, K2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -942,6 +1033,7 @@ bool launch_sum_pair(const SumLaunch& L1, const SumLaunch& L2, cudaStream_t st) 
   }
   const int k1 = sum_kind(L1), k2 = sum_kind(L2);
   if (k1 == kSumKindU8 && k2 == kSumKindU32) launch_pair_k<kSumKindU8, kSumKindU32>(L1, L2, st);
+  else if (k1 == kSumKindU8Out16 && k2 == kSumKindU16Quad) launch_pair_k<kSumKindU8Out16, kSumKindU16Quad>(L1, L2, st);
   else if (k1 == kSumKindU16Wide && k2 == kSumKindU32) launch_pair_k<kSumKindU16Wide, kSumKindU32>(L1, L2, st);
   else if (k1 == kSumKindU8Flush && k2 == kSumKindU32) launch_pair_k<kSumKindU8Flush, kSumKindU32>(L1, L2, st);
   else return false;
@@ -958,6 +1050,7 @@ void launch_sum_grouped(const SumBatchGroup* d_groups, int ngroups, long long to
     case kSumKindU8: launch_grouped_k<kSumKindU8>(d_groups, ngroups, total, smem, st); break;
     case kSumKindU16: launch_grouped_k<kSumKindU16>(d_groups, ngroups, total, smem, st); break;
     case kSumKindU16Wide: launch_grouped_k<kSumKindU16Wide>(d_groups, ngroups, total, smem, st); break;
+    case kSumKindU16Quad: launch_grouped_k<kSumKindU16Quad>(d_groups, ngroups, total, smem, st); break;
     default: launch_grouped_k<kSumKindU32>(d_groups, ngroups, total, smem, st); break;
   }
 }

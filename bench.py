@@ -158,37 +158,41 @@ class ClockSampler:
 # ---------------------------------------------------------------- reference CPU
 def reference_cpu_rate(x_host: np.ndarray, hdr: dict, wl: dict, target_s: float):
     """Time the reference's cpucal::dedispered_fil_omp (built from source into
-    oracle/_ref) on a bounded sample: all DM trials of the workload over the first
-    n samples of the chunk, n chosen so one call takes about target_s seconds.
-    Returns (DM-trial*samples/s, threads, sample description, seconds)."""
+    oracle/_ref) on a bounded sample of the workload: every k-th DM trial of the
+    workload's grid (DM lo, lo + k*step, ...) over the whole chunk, k chosen so one
+    call takes about target_s seconds.  Keeping the whole time axis keeps the
+    share of delayed samples that fall past the chunk's end (which the reference
+    skips, include/cpucal.hpp:181) the same as in the full workload; the DM
+    subsample spans the whole DM range.  Returns (DM-trial*samples/s, threads,
+    sample description, seconds of the timed call)."""
     from oracle import oracle as O
 
     lib = O.ref_cpu()
     threads = int(lib.ref_cpu_threads())
     nchans = hdr["nchans"]
+    n = x_host.shape[0]
     lo, hi, step = wl["dm"]
     freq = O.freq_table_fil(hdr["fch1"], hdr["foff"], nchans)
     fs, fe = float(np.float32(freq[0])), float(np.float32(freq[-1]))
-    ndm = O.dm_steps(lo, hi, step)
+    ndm_full = O.dm_steps(lo, hi, step)
+    xs = np.ascontiguousarray(x_host)
 
-    def run(n):
-        xs = np.ascontiguousarray(x_host[:n])
+    def run(k):
+        st = float(np.float32(step * k))
         t = time.perf_counter()
         O.ref_bruteforce_cpu(xs, nchans, hdr["fch1"], hdr["foff"], hdr["tsamp"], lo, hi, fs, fe,
-                             step, 1, n * hdr["tsamp"] * 0.999)
-        return time.perf_counter() - t
+                             st, 1, n * hdr["tsamp"] * 0.999)
+        return time.perf_counter() - t, O.dm_steps(lo, hi, st)
 
-    n = 256
-    dt = run(n)
-    while dt < 0.5 and n < x_host.shape[0]:
-        n = min(x_host.shape[0], n * 4)
-        dt = run(n)
-    n = int(min(x_host.shape[0], max(256, n * target_s / max(dt, 1e-3))))
-    dt = run(n)
-    rate = ndm * n / dt
+    k = max(1, ndm_full // 3)
+    dt, nd = run(k)
+    k = int(max(1, min(k, round(k * dt / target_s))))
+    dt, nd = run(k)
+    rate = nd * n / dt
     sample = (f"reference cpucal::dedispered_fil_omp (brute force, the reference's CPU path) on "
-              f"the first {n} samples x {nchans} channels, all {ndm} DM trials, "
-              f"{threads} OpenMP threads")
+              f"{nd} of the {ndm_full} DM trials (every {k}-th, DM {lo:g} to {hi:g}) over all "
+              f"{n} samples x {nchans} channels, {threads} OpenMP threads; the rate is "
+              f"extrapolated to the full DM grid")
     return rate, threads, sample, dt
 
 
@@ -619,7 +623,103 @@ def reference_gpu_arm(args, wl, spec, hdr, config, dist, dev):
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------- extras
+EXTRAS = [
+    # (key, bench.py arguments): short runs, each in its own process on this GPU
+    ("reference-gpu", ["--impl", "reference-gpu", "--steps", "2", "--warmup", "1"]),
+    ("plain-1024ch-u8-2^17-1001dm-brute", ["--workload", "plain-1024ch-u8-2^17-1001dm-brute",
+                                           "--steps", "10", "--warmup", "3", "--e2e-steps", "2"]),
+    ("batched-64-heterogeneous-subband32", ["--workload", "batched-64-heterogeneous-subband32",
+                                            "--steps", "2", "--warmup", "1", "--no-autotune"]),
+    ("serving-19beams-4096ch-u8-3001dm-files", ["--workload",
+                                                "serving-19beams-4096ch-u8-3001dm-files",
+                                                "--steps", "10", "--warmup", "3"]),
+]
+EXTRA_KEYS = ("impl", "value", "unit", "ms_per_step", "steps", "warmup", "e2e", "cpu_baseline",
+              "batched_over_plain", "forms", "latency", "clocks", "gpu_launches", "unavailable",
+              "reference_timers_ms", "files", "chunks")
+
+
+def run_extras(dev):
+    """The other workloads and the reference's plain GPU call, run briefly after the
+    headline measurement so that their numbers come from the same bench run.  Each
+    runs as `bench.py --no-extras ...` in a child process on this GPU (the headline's
+    buffers are released first); the child's JSON line is kept, trimmed to its
+    results and roofline."""
+    import subprocess
+
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(dev)))
+    for k in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(k, None)
+    out = {}
+    for key, argv in EXTRAS:
+        t = time.perf_counter()
+        try:
+            r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--no-extras", *argv],
+                               capture_output=True, text=True, timeout=900, env=env)
+            lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+            d = json.loads(lines[-1]) if lines else {"error": (r.stderr or r.stdout)[-400:]}
+        except subprocess.TimeoutExpired:
+            d = {"error": "timed out after 900 s"}
+        res = {k: d[k] for k in EXTRA_KEYS if k in d}
+        if "roofline" in d and d["roofline"]:
+            res["roofline"] = {k: d["roofline"].get(k) for k in
+                               ("achieved", "peak", "unit", "frac", "step_frac", "int_add", "kernel",
+                                "stages_ms") if k in d["roofline"]}
+        if "config" in d:
+            res["config"] = d["config"]
+        if "error" in d:
+            res["error"] = d["error"]
+        res["run_seconds"] = round(time.perf_counter() - t, 1)
+        out[key] = res
+    return out
+
+
 # ---------------------------------------------------------------- helpers
+def parity_rows(wl, plan):
+    """DM rows checked against the reference build: the first two, the rows of the
+    injected pulses' DMs, the middle and the last two."""
+    lo, hi, step = wl["dm"]
+    n = int(plan.out_shape[0])
+    rows = {0, 1, n // 2, n - 2, n - 1}
+    for dm, *_ in wl["chunk"].get("pulses", []):
+        rows.add(int(min(n - 1, max(0, round((dm - lo) / step)))))
+    return sorted(r for r in rows if 0 <= r < n)
+
+
+def reference_parity(x_host, hdr, wl, rows, ours_rows, dev):
+    """The timed output's rows (all columns) against the reference's own GPU path
+    (gpucal::dedisperse_spec, src/core/dedispered.cu:988-1304, built from its
+    sources into oracle/_ref) run on the same chunk.  A checker: it runs after the
+    timed region and its time is not part of any reported number."""
+    from oracle import oracle as O
+
+    sbw = wl["subband_width"]
+    if not O.ref_gpu_available(sbw):
+        return None
+    lo, hi, step = wl["dm"]
+    f32 = np.float32
+    fs = float(f32(hdr["fch1"]))
+    fe = float(f32(f32(hdr["fch1"]) + f32(hdr["nchans"] - 1) * f32(hdr["foff"])))
+    r = wl["rfi"] or {}
+    iq = None
+    if r.get("use_iqrm"):
+        from types import SimpleNamespace
+        iq = SimpleNamespace(**r["iqrm"])
+    t = time.perf_counter()
+    ref = O.ref_gpu_dedisperse_spec_rows(x_host, hdr["nchans"], hdr["tsamp"], hdr["fch1"],
+                                         hdr["foff"], lo, hi, fs, fe, step, wl["ds"], rows=rows,
+                                         sb_width=sbw, use_zero_dm=r.get("use_zero_dm", False),
+                                         use_iqrm=r.get("use_iqrm", False), iq=iq, device=dev)
+    dt = time.perf_counter() - t
+    ours = ours_rows.view(__import__("torch").int32).numpy().view(np.uint32)
+    bad = int((ours != ref).sum()) if ours.shape == ref.shape else -1
+    return {"ok": bad == 0, "rows": rows, "columns": int(ref.shape[1]), "mismatches": bad,
+            "reference": f"oracle/_ref/libref_gpu_sb{sbw}.so: the reference's gpucal::dedisperse_spec "
+                         "(src/core/dedispered.cu) built from its sources for sm_100a, raw sums",
+            "seconds": round(dt, 1)}
+
+
 def roofline_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -780,6 +880,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="keep the plan's default launch shape")
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="skip the short runs of the other workloads and of the reference GPU "
+                         "arm that the default single-GPU run adds to its line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     wl = WORKLOADS[args.workload]
@@ -830,8 +933,7 @@ def main():
             dist.close()
             return
         x, _ = make_chunk_device(spec, dev)
-        nsamp_sample = min(wl["nsamp"], 1 << 14)
-        x_host = x[:nsamp_sample].cpu().numpy()
+        x_host = x.cpu().numpy()
         del x
         from oracle import oracle as O
 
@@ -840,24 +942,27 @@ def main():
                               "oracle/_ref/libref_cpu.so is missing (build with make -C oracle ref)"}))
             return
         for _ in range(args.warmup):
-            reference_cpu_rate(x_host, hdr, wl, target_s=2.0)
+            reference_cpu_rate(x_host, hdr, wl, target_s=1.0)
         rates, secs = [], []
         for _ in range(args.steps):
-            r, threads, sample, dt = reference_cpu_rate(x_host, hdr, wl, target_s=6.0)
+            r, threads, sample, dt = reference_cpu_rate(x_host, hdr, wl, target_s=4.0)
             rates.append(r)
             secs.append(dt)
         value = float(np.median(rates))
-        ms = 1e3 * wl["nsamp"] * O.dm_steps(*wl["dm"]) / value
+        full_ms = 1e3 * wl["nsamp"] * O.dm_steps(*wl["dm"]) / value
         line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * float(np.median(secs)),
+                "full_workload_ms_extrapolated": full_ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
                 "data": "synthetic", "config": config,
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
                                  "kind": "reference", "sample": sample},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0},
-                "note": "each step times one bounded sample; ms_per_step extrapolates the rate "
-                        "to the full workload"}
+                "note": "each step times one bounded sample (a DM subsample over the whole "
+                        "chunk); ms_per_step is that sample's time, full_workload_ms_extrapolated "
+                        "the full workload's time at the measured rate"}
         print(json.dumps(line))
         return
 
@@ -897,6 +1002,13 @@ def main():
     ms_rank = e0.elapsed_time(e1) / args.steps
     value = dist.job_rate(units, ms_rank * 1e-3)
     ms = dist.max(ms_rank)
+
+    # rows of the timed output, kept for the check against the reference build in the
+    # cpu_baseline leg (every column, so every time tile is covered)
+    check_rows = parity_rows(wl, plan) if wl["algorithm"] == "subband" else None
+    ours_rows = None
+    if check_rows is not None:
+        ours_rows = out.index_select(0, torch.tensor(check_rows, device=out.device)).cpu()
 
     # per-stage breakdown: the profiled form of the run after the timed steps (its
     # stages run one after another; CUDA events on the run's stream)
@@ -953,15 +1065,28 @@ def main():
         e2e_dropin = e2e_dropin_run(wl, hdr, x, units, dist, dev, args.e2e_steps, args.warmup)
 
     cpu = None
+    parity = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
 
+        x_host = x.cpu().numpy() if x.dtype == torch.uint8 else x.view(torch.int16).cpu().numpy().view(np.uint16)
         if O.ref_cpu_available():
-            x_host = x[: min(wl["nsamp"], 1 << 14)].cpu().numpy()
             rate, threads, sample, dt = reference_cpu_rate(x_host, hdr, wl, target_s=12.0)
             cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
                    "sample": sample, "seconds": dt}
+        if check_rows is not None:
+            parity = reference_parity(x_host, hdr, wl, check_rows, ours_rows, dev)
+        del x_host
     dist.barrier()
+    extras = None
+    if dist.rank == 0 and dist.world == 1 and args.extras and args.workload == DEFAULT_WORKLOAD:
+        # release the headline's device buffers: the children need the GPU's memory
+        if not plan.closed:
+            plan.close()
+        out = x = None
+        torch.cuda.synchronize(dev)
+        torch.cuda.empty_cache()
+        extras = run_extras(dev)
     if dist.rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -970,7 +1095,10 @@ def main():
                 "config": config, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "e2e_dropin": e2e_dropin, "gpu_launches": launches, "clocks": clk,
                 "autotune": tune,
-                "host_path_matches_device": same}
+                "host_path_matches_device": same,
+                "parity_vs_reference": None if parity is None else parity["ok"],
+                "parity_vs_reference_detail": parity,
+                "extras": extras}
         print(json.dumps(line))
     dist.close()
 
