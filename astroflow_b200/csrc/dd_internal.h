@@ -273,7 +273,7 @@ struct SumLaunch {
   int64_t ncols;           // columns of the launch
   int win_bytes;           // bytes of one staged source window
   int src_bytes;           // 1 or 2
-  int flush;               // 8-bit sources: widen lanes every 256 sources
+  int flush;               // 8-bit sources: add the lanes into the output every 256 sources
   int lane_per;            // 16-bit sources: sources per 16-bit lane before widening
   unsigned grid_y, grid_z;
   const SumDesc* desc;     // [grid_y][desc_pitch] staging descriptors
@@ -311,7 +311,7 @@ constexpr int kErrWaitEmpty = 2;  // the producer gave up waiting for a free sta
 #define DD_SUM8_NW 5
 #endif
 #ifndef DD_SUM8F_NW
-#define DD_SUM8F_NW 2
+#define DD_SUM8F_NW 5
 #endif
 // Blocks per SM the staged-sum kernels are compiled for (register budget).
 #ifndef DD_SUM16_MINB
@@ -335,7 +335,7 @@ constexpr int kSum32NW = DD_SUM32_NW;  // words per lane of the 32-bit staged su
 #define DD_SUM16Q_NW 5
 #endif
 constexpr int kSum16QNW = DD_SUM16Q_NW;
-// flush: 8-bit sources widened every 256 sources; 16-bit sources summed into
+// flush: 8-bit lanes added into the output every 256 sources; 16-bit sources summed into
 // 32-bit lanes (the k_sum_u16w variant).
 inline int sum_variant_tile(int src_bytes, bool flush) {
   return sum_tile_samples(src_bytes, src_bytes == 4   ? kSum32NW

@@ -20,9 +20,11 @@
 // shift that is not a multiple of 4 bytes costs one funnel shift of two words.
 // 8-bit samples are split into two 16-bit-lane words by byte permutes and two
 // sources are added by one three-input add (four sample additions per add);
-// lanes are widened to 32 bits every 256 sources.  16-bit samples are added as
-// lane pairs and widened before they can overflow.  A missing second source (odd
-// source count) reads a zeroed window.
+// with more than 256 sources the lanes are added into the 32-bit output every
+// 256 sources (the block owns its output tile, so it reads back its own sums).
+// 16-bit samples are added as lane pairs and widened before they can overflow;
+// 16-bit stage-1 sums are added four at a time (sum_u16_quad).  A missing
+// source (source count not a multiple of the group) reads a zeroed window.
 //
 // Every wait on an mbarrier is bounded (about two seconds of SM clock); a wait
 // that gives up records an error code in L.err and the block stops summing, and
@@ -315,6 +317,7 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
 // ------------------------------------------------------------------ 8-bit samples
 template <int RB, int NW, bool OUT16, bool FLUSH>
 __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* sw, Pipe& P) {
+  static_assert(!(OUT16 && FLUSH), "16-bit outputs hold at most 257 sources: no flushes");
   constexpr int T = kWarps * 32 * NW * 4;
   const Geo g = make_geo(L, T, blk);
   if (g.nrows <= 0) return;
@@ -326,18 +329,53 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
   const int wbase = kConsec ? warp * 32 * NW + lane * NW : warp * 32 * NW + lane;
   const uint32_t one = L.one;
   uint32_t ev[RB][NW], od[RB][NW];  // 16-bit lanes: samples (4w, 4w+2) and (4w+1, 4w+3)
-  uint32_t w32[FLUSH ? RB : 1][FLUSH ? NW * 4 : 1];
 #pragma unroll
   for (int r = 0; r < RB; ++r)
 #pragma unroll
     for (int k = 0; k < NW; ++k) ev[r][k] = od[r][k] = 0;
-  if constexpr (FLUSH) {
+  // Writes the lane sums of rows [0, nrows) to the output, adding them to the
+  // partial sums an earlier flush stored there when `add`, and clears the lanes.
+  auto emit = [&](bool add) {
 #pragma unroll
-    for (int r = 0; r < RB; ++r)
+    for (int r = 0; r < RB; ++r) {
+      if (r >= g.nrows) break;
 #pragma unroll
-      for (int k = 0; k < NW * 4; ++k) w32[r][k] = 0;
-  }
-  int since = 0;
+      for (int k = 0; k < NW; ++k) {
+        const int64_t t = static_cast<int64_t>(wbase + kStride * k) * 4;  // block-local sample
+        if (t < g.valid) {
+          const uint32_t s0 = ev[r][k] & 0xffffu, s1 = od[r][k] & 0xffffu;
+          const uint32_t s2 = ev[r][k] >> 16, s3 = od[r][k] >> 16;
+          char* row = g.out + r * g.out_pitch;
+          if constexpr (OUT16) {
+            uint16_t* dst = reinterpret_cast<uint16_t*>(row) + t;
+            if (t + 4 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
+              *reinterpret_cast<uint2*>(dst) = make_uint2(__byte_perm(ev[r][k], od[r][k], 0x5410),
+                                                          __byte_perm(ev[r][k], od[r][k], 0x7632));
+            } else {
+              const uint32_t v[4] = {s0, s1, s2, s3};
+              for (int q = 0; q < 4 && t + q < g.valid; ++q) dst[q] = static_cast<uint16_t>(v[q]);
+            }
+          } else {
+            uint32_t* dst = reinterpret_cast<uint32_t*>(row) + t;
+            if (t + 4 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+              uint4 v = make_uint4(s0, s1, s2, s3);
+              if (add) {
+                const uint4 o = *reinterpret_cast<const uint4*>(dst);
+                v.x += o.x; v.y += o.y; v.z += o.z; v.w += o.w;
+              }
+              *reinterpret_cast<uint4*>(dst) = v;
+            } else {
+              const uint32_t v[4] = {s0, s1, s2, s3};
+              for (int q = 0; q < 4 && t + q < g.valid; ++q) dst[q] = add ? dst[q] + v[q] : v[q];
+            }
+          }
+        }
+        ev[r][k] = od[r][k] = 0;
+      }
+    }
+  };
+  int since = 0;       // sources summed in the 16-bit lanes since the last flush
+  bool stored = false; // the output holds partial sums of an earlier flush
   run_pipeline<1>(L, g, P, sw, T, [&](int s, const uint32_t* win) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
@@ -355,7 +393,7 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
                                    : __funnelshift_r(w0[32 * k], w0[32 * k + 1], rw.y);
         const uint32_t b = kConsec ? __funnelshift_r(vb[k], vb[k + 1], rw.w)
                                    : __funnelshift_r(w1[32 * k], w1[32 * k + 1], rw.w);
-        if constexpr (kSumImad && !FLUSH) {
+        if constexpr (kSumImad) {
           ev[r][k] = mad_u32(__byte_perm(a, 0u, 0x4240), one, ev[r][k]);
           ev[r][k] = mad_u32(__byte_perm(b, 0u, 0x4240), one, ev[r][k]);
           od[r][k] = mad_u32(__byte_perm(a, 0u, 0x4341), one, od[r][k]);
@@ -368,58 +406,15 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
     }
     if constexpr (FLUSH) {
       since += 2;
-      if (since >= 256) {  // 256 x 255 fits a 16-bit lane
-#pragma unroll
-        for (int r = 0; r < RB; ++r)
-#pragma unroll
-          for (int k = 0; k < NW; ++k) {
-            w32[r][4 * k + 0] += ev[r][k] & 0xffffu; w32[r][4 * k + 2] += ev[r][k] >> 16;
-            w32[r][4 * k + 1] += od[r][k] & 0xffffu; w32[r][4 * k + 3] += od[r][k] >> 16;
-            ev[r][k] = od[r][k] = 0;
-          }
+      if (since >= 256) {  // 256 x 255 fits a 16-bit lane: move the lanes to the output
+        emit(stored);
+        stored = true;
         since = 0;
       }
     }
   });
   if (P.failed) return;
-#pragma unroll
-  for (int r = 0; r < RB; ++r) {
-    if (r >= g.nrows) break;
-#pragma unroll
-    for (int k = 0; k < NW; ++k) {
-      const int64_t t = static_cast<int64_t>(wbase + kStride * k) * 4;  // block-local sample
-      if (t >= g.valid) continue;
-      uint32_t s0, s1, s2, s3;
-      if constexpr (FLUSH) {
-        s0 = w32[r][4 * k + 0] + (ev[r][k] & 0xffffu);
-        s1 = w32[r][4 * k + 1] + (od[r][k] & 0xffffu);
-        s2 = w32[r][4 * k + 2] + (ev[r][k] >> 16);
-        s3 = w32[r][4 * k + 3] + (od[r][k] >> 16);
-      } else {
-        s0 = ev[r][k] & 0xffffu; s1 = od[r][k] & 0xffffu;
-        s2 = ev[r][k] >> 16;     s3 = od[r][k] >> 16;
-      }
-      char* row = g.out + r * g.out_pitch;
-      if constexpr (OUT16) {
-        uint16_t* dst = reinterpret_cast<uint16_t*>(row) + t;
-        if (t + 4 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
-          *reinterpret_cast<uint2*>(dst) = make_uint2(__byte_perm(ev[r][k], od[r][k], 0x5410),
-                                                      __byte_perm(ev[r][k], od[r][k], 0x7632));
-        } else {
-          const uint32_t v[4] = {s0, s1, s2, s3};
-          for (int q = 0; q < 4 && t + q < g.valid; ++q) dst[q] = static_cast<uint16_t>(v[q]);
-        }
-      } else {
-        uint32_t* dst = reinterpret_cast<uint32_t*>(row) + t;
-        if (t + 4 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
-          *reinterpret_cast<uint4*>(dst) = make_uint4(s0, s1, s2, s3);
-        } else {
-          const uint32_t v[4] = {s0, s1, s2, s3};
-          for (int q = 0; q < 4 && t + q < g.valid; ++q) dst[q] = v[q];
-        }
-      }
-    }
-  }
+  emit(FLUSH && stored);
 }
 
 // ------------------------------------------------------------------ 16-bit samples

@@ -168,17 +168,18 @@ class BatchChunk:
     subband_width: int
 
 
-def draw_batch(n: int = 64, seed: int = 2024, subband_width: int = 32) -> List[BatchChunk]:
+def draw_batch(n: int = 64, seed: int = 2024, subband_width: int = 32,
+               log2_nsamp: Tuple[float, float] = (15.0, 19.0)) -> List[BatchChunk]:
     """Seeded draw of a heterogeneous batch: nchan in {1024, 2048, 4096}, 8- or 16-bit
-    samples, nsamp log-uniform in [2^15, 2^19], band 1000-1500 or 1250-1550 MHz,
-    maximum DM in {500, 1500, 3000} with a step in {0.5, 1, 1.5, 2}, time
-    downsampling in {1, 2, 4, 8}, one dispersed pulse per chunk at a random DM."""
+    samples, nsamp log-uniform in [2^15, 2^19] (log2_nsamp), band 1000-1500 or
+    1250-1550 MHz, maximum DM in {500, 1500, 3000} with a step in {0.5, 1, 1.5, 2},
+    time downsampling in {1, 2, 4, 8}, one dispersed pulse per chunk at a random DM."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n):
         nchans = int(rng.choice([1024, 2048, 4096]))
         nbits = int(rng.choice([8, 16]))
-        nsamp = int(round(2 ** rng.uniform(15, 19)))
+        nsamp = int(round(2 ** rng.uniform(*log2_nsamp)))
         f_hi, bw = ((1500.0, 500.0), (1550.0, 300.0))[int(rng.integers(2))]
         dm_high = float(rng.choice([500.0, 1500.0, 3000.0]))
         dm_step = float(rng.choice([0.5, 1.0, 1.5, 2.0]))

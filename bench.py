@@ -81,6 +81,10 @@ WORKLOADS = {
     # two bands, DM ranges up to 3000, downsampling 1-8), dedispersed as batches
     "batched-64-heterogeneous-subband32": dict(kind="batch", nchunks=64, seed=2024,
                                                subband_width=32, budget_gb=140.0),
+    # the same draw restricted to short chunks (2^15-2^16 samples), where launch
+    # overhead is a larger share of each plain call
+    "batched-256-short-subband32": dict(kind="batch", nchunks=256, seed=2025, subband_width=32,
+                                        budget_gb=140.0, log2_nsamp=(15.0, 16.0)),
     # 8192 ch u16, 2^21 samples, three DM ranges on one resident chunk (DM 0:0.25:500 ds 1,
     # 500:0.5:2000 ds 2, 2000:1:5000 ds 4), subband width 64 (128 subbands), IQRM + zero-DM
     "large-8192ch-u16-2^21-multirange-subband64-rfi": dict(
@@ -208,7 +212,8 @@ def bench_batch(args, wl, dist, dev):
     from astroflow_b200.synth import draw_batch, make_chunk_device
 
     f32 = np.float32
-    chunks = draw_batch(wl["nchunks"], seed=wl["seed"] + dist.rank, subband_width=wl["subband_width"])
+    chunks = draw_batch(wl["nchunks"], seed=wl["seed"] + dist.rank, subband_width=wl["subband_width"],
+                        log2_nsamp=wl.get("log2_nsamp", (15.0, 19.0)))
     budget = wl["budget_gb"] * 1e9
     stream = torch.cuda.current_stream(dev)
     times = {"plain": 0.0, "grouped": 0.0, "persistent": 0.0}
@@ -301,7 +306,7 @@ def bench_batch(args, wl, dist, dev):
         line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": dist.world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "u8/u16", "data": "synthetic (seeded draw of 64 chunks, generated on the GPU)",
+                "dtype": "u8/u16", "data": f"synthetic (seeded draw of {len(chunks)} chunks, generated on the GPU)",
                 "config": {"workload": args.workload, "chunks": len(chunks), "batched_form": best,
                            "waves": waves, "seed": wl["seed"], "subband_width": wl["subband_width"],
                            "hbm_budget_gb": wl["budget_gb"],
@@ -631,6 +636,8 @@ EXTRAS = [
                                            "--steps", "10", "--warmup", "3", "--e2e-steps", "2"]),
     ("batched-64-heterogeneous-subband32", ["--workload", "batched-64-heterogeneous-subband32",
                                             "--steps", "2", "--warmup", "1", "--no-autotune"]),
+    ("batched-256-short-subband32", ["--workload", "batched-256-short-subband32",
+                                     "--steps", "3", "--warmup", "1", "--no-autotune"]),
     ("serving-19beams-4096ch-u8-3001dm-files", ["--workload",
                                                 "serving-19beams-4096ch-u8-3001dm-files",
                                                 "--steps", "10", "--warmup", "3"]),

@@ -125,7 +125,7 @@ enum dd_table_mode {
   DD_TABLE_FP64 = 1,
   /* Brute force only: the float expression of cpucal.hpp:124-131 in strict
    * IEEE single precision (no contraction, exact reciprocals); host-independent,
-   * and about one entry in 36,000 away from the reference build at ties. */
+   * and a few entries per ten thousand away from the reference build at ties. */
   DD_TABLE_IEEE = 2
 };
 
