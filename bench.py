@@ -1026,19 +1026,29 @@ def main():
     hbm_peak, peak_kind = roofline_peaks()
     add_peak = measure_int_add_rate(dev)
     bytes_per_unit = (wl["nsamp"] * wl["nchans"] * wl["nbits"] / 8 + units * 4) / units
+    elem = wl["nbits"] // 8
     if wl["algorithm"] == "subband":
         tile = min(int(info["nsamp_binned"]), int(info["tile_samples"]))
+        dch = info["chan_end"] - info["chan_start"] + 1
+        # bytes of one subband sum: 16-bit for 8-bit samples in subbands of <= 64
+        # channels, else the reference's accumulator type
+        inter = 2 if (wl["nbits"] == 8 and wl["subband_width"] <= 64) else (8 if wl["nbits"] == 32 else 4)
         if st["stage1_ms"] >= st["stage2_ms"]:
             kname, kms, kn = "stage1", st["stage1_ms"], s1n
-            adds_launch = info["ndm_nom"] * (info["chan_end"] - info["chan_start"] + 1) * tile
+            adds_launch = info["ndm_nom"] * dch * tile
+            # the tile's prepared input, read once, and its subband sums, written once
+            kbytes = dch * tile * elem + info["ndm_nom"] * info["nsb"] * tile * inter
         else:
             kname, kms, kn = "stage2", st["stage2_ms"], s2n
             adds_launch = info["dm_steps"] * info["nsb"] * tile
+            # the tile's subband sums, read once, and its DM-time output, written once
+            kbytes = info["ndm_nom"] * info["nsb"] * tile * inter + info["dm_steps"] * tile * 4
         units_launch = info["dm_steps"] * tile
     else:
         kname, kms, kn = "brute", st["stage2_ms"], s2n
         units_launch = units / max(kn, 1)
         adds_launch = info["adds_per_run"] / max(kn, 1)
+        kbytes = (wl["nsamp"] * (info["chan_end"] - info["chan_start"]) * elem + units * 4) / max(kn, 1)
     avg_launch_s = kms / max(kn, 1) * 1e-3
     achieved = units_launch * bytes_per_unit / avg_launch_s / 1e9
     adds_rate = adds_launch / avg_launch_s
@@ -1050,6 +1060,10 @@ def main():
         "traffic": ncu_traffic(kname, units_launch),
         "bytes_per_unit": bytes_per_unit, "units_per_launch": units_launch,
         "avg_launch_ms": avg_launch_s * 1e3,
+        # the dominant kernel's own algorithmic bytes (its inputs read once, its
+        # outputs written once) against its launch time: compare with `traffic`
+        "kernel_bytes_per_launch": kbytes, "kernel_achieved": kbytes / avg_launch_s / 1e9,
+        "kernel_frac": kbytes / avg_launch_s / 1e9 / hbm_peak,
         "int_add": {"achieved": adds_rate, "peak": add_peak, "unit": "adds/s",
                     "frac": adds_rate / add_peak, "peak_kind": "measured live (IADD3 probe)"},
         "binding": "int_add" if info["adds_per_run"] / add_peak > units * bytes_per_unit / (hbm_peak * 1e9) else "hbm",

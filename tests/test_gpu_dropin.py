@@ -160,8 +160,14 @@ def test_dedispered_fil_cpu_target_matches_oracle(tmp_path):
     fs, fe = float(fil.frequency_table[0]), float(fil.frequency_table[-1])
     lo, hi, step, ds, tslice = 0.0, 200.0, 1.0, 2, 0.05
     res = C._dedispered_fil(str(path), lo, hi, fs, fe, step, ds, tslice, 0)
+    # the oracle's sums with the delay table of the reference CPU build's arithmetic
+    # (the library's default; the table itself is pinned by tests/test_brute_table_cpu.py)
+    from astroflow_b200.dedisp import brute_delay_table
+    freq = np.asarray(fil.frequency_table, np.float64)
+    cs, ce = O.chan_range(freq, fs, fe)
+    table, _ = brute_delay_table(freq, cs, ce, ce, lo, step, O.dm_steps(lo, hi, step), fil.tsamp)
     slices = O.bruteforce_cpu(fil.data.reshape(n, nchans), nchans, fil.frequency_table, fil.tsamp,
-                              lo, hi, fs, fe, step, ds, tslice)
+                              lo, hi, fs, fe, step, ds, tslice, delay=table)
     assert_same_images(res.dm_times, CVI.images(slices))
 
 
