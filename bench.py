@@ -163,23 +163,24 @@ class ClockSampler:
 def reference_cpu_rate(x_host: np.ndarray, hdr: dict, wl: dict, target_s: float):
     """Time the reference's cpucal::dedispered_fil_omp (built from source into
     oracle/_ref) on a bounded sample of the workload: every k-th DM trial of the
-    workload's grid (DM lo, lo + k*step, ...) over the whole chunk, k chosen so one
-    call takes about target_s seconds.  Keeping the whole time axis keeps the
-    share of delayed samples that fall past the chunk's end (which the reference
-    skips, include/cpucal.hpp:181) the same as in the full workload; the DM
-    subsample spans the whole DM range.  Returns (DM-trial*samples/s, threads,
-    sample description, seconds of the timed call)."""
+    workload's grid over the chunk's first n = min(nsamp, 2^18) samples.  n is
+    longer than the largest delay of every workload plus a 0.5 s slice, so the
+    share of delayed samples past the sample's end (which the reference skips,
+    include/cpucal.hpp:181) stays small; the reference parallelises over DM
+    trials, so the sample keeps at least one trial per thread, and k is chosen
+    so that one call takes about target_s seconds.  Returns (DM-trial*samples/s,
+    threads, sample description, seconds of the timed call)."""
     from oracle import oracle as O
 
     lib = O.ref_cpu()
     threads = int(lib.ref_cpu_threads())
     nchans = hdr["nchans"]
-    n = x_host.shape[0]
+    n = min(x_host.shape[0], 1 << 18)
     lo, hi, step = wl["dm"]
     freq = O.freq_table_fil(hdr["fch1"], hdr["foff"], nchans)
     fs, fe = float(np.float32(freq[0])), float(np.float32(freq[-1]))
     ndm_full = O.dm_steps(lo, hi, step)
-    xs = np.ascontiguousarray(x_host)
+    xs = np.ascontiguousarray(x_host[:n])
 
     def run(k):
         st = float(np.float32(step * k))
@@ -188,15 +189,17 @@ def reference_cpu_rate(x_host: np.ndarray, hdr: dict, wl: dict, target_s: float)
                              st, 1, n * hdr["tsamp"] * 0.999)
         return time.perf_counter() - t, O.dm_steps(lo, hi, st)
 
-    k = max(1, ndm_full // 3)
+    k = max(1, ndm_full // threads)
     dt, nd = run(k)
-    k = int(max(1, min(k, round(k * dt / target_s))))
-    dt, nd = run(k)
+    grow = int(target_s / max(dt, 1e-3))
+    if grow > 1:
+        k = max(1, k // grow)
+        dt, nd = run(k)
     rate = nd * n / dt
     sample = (f"reference cpucal::dedispered_fil_omp (brute force, the reference's CPU path) on "
-              f"{nd} of the {ndm_full} DM trials (every {k}-th, DM {lo:g} to {hi:g}) over all "
-              f"{n} samples x {nchans} channels, {threads} OpenMP threads; the rate is "
-              f"extrapolated to the full DM grid")
+              f"{nd} of the {ndm_full} DM trials (every {k}-th, DM {lo:g} to {hi:g}) over the "
+              f"first {n} samples x {nchans} channels, {threads} OpenMP threads; the rate is "
+              f"extrapolated to the full DM grid and chunk")
     return rate, threads, sample, dt
 
 
