@@ -281,7 +281,6 @@ struct SumLaunch {
   int stages;              // staged source pairs in flight (2..4)
   int* err;                // device error word: set when a bounded wait gives up
   unsigned one;            // 1 (a multiplier the compiler cannot fold)
-  int tiles_per_block;     // consecutive time tiles each block sums (0 or 1: one)
 };
 #ifndef DD_SUM_MAX_STAGES
 #define DD_SUM_MAX_STAGES 8

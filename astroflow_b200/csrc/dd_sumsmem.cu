@@ -119,29 +119,16 @@ struct Geo {
   const SumDesc* desc; // descriptor of source 0 for this block's row group
   int64_t base;        // element index added to every offset
   int nsrc, nrows;
-  char* out;           // row 0, first column of the block's first tile (byte address)
+  char* out;           // row 0, first column of the block (byte address)
   int64_t out_pitch;   // bytes between output rows
-  int64_t valid;       // columns from the block's first column to the launch's end
-  int ntiles;          // tiles of T columns this block sums, one after another
-  int out_elem;        // bytes per output element
+  int64_t valid;       // columns of this block to store (<= T)
 };
-// Tile t of the block: its first column's output address and its columns to store.
-__device__ __forceinline__ char* tile_out(const Geo& g, int t, int T) {
-  return g.out + static_cast<int64_t>(t) * T * g.out_elem;
-}
-__device__ __forceinline__ int64_t tile_valid(const Geo& g, int t, int T) {
-  return g.valid - static_cast<int64_t>(t) * T;
-}
 
 __device__ __forceinline__ Geo make_geo(const SumLaunch& L, int T, uint3 blk) {
   Geo g;
-  const int tpb = L.tiles_per_block > 1 ? L.tiles_per_block : 1;
-  const int64_t tile = static_cast<int64_t>(blk.x) * tpb;
+  const int64_t tile = blk.x;
   const int64_t col = tile * T;  // launch-local column of the block
   g.valid = L.ncols - col;
-  g.ntiles = static_cast<int>(max(static_cast<int64_t>(0),
-                                  min(static_cast<int64_t>(tpb), (g.valid + T - 1) / T)));
-  g.out_elem = L.out_elem;
   const SumDesc* drow = L.desc + static_cast<int64_t>(blk.y) * L.desc_pitch;
   switch (L.mode) {
     case SumLaunch::kStage1: {
@@ -203,8 +190,8 @@ __device__ __forceinline__ int4 row_pair(const Pipe& P, int s, int r, int half) 
 // Producer step for source group q in stage s (warp 0, lanes 0..QS-1; lane l
 // handles source QS*q + l).  The caller has made sure stage s is free.
 template <int SB, int QS>
-__device__ __forceinline__ void produce(const Geo& g, int64_t base, Pipe& P, uint32_t* sw, int ww,
-                                        int zero_q, int tile_bytes, int q, int s, int lane) {
+__device__ __forceinline__ void produce(const Geo& g, Pipe& P, uint32_t* sw, int ww, int zero_q,
+                                        int tile_bytes, int q, int s, int lane) {
   const int src = QS * q + lane;
   uint32_t nbytes = 0;
   const char* gsrc = nullptr;
@@ -213,9 +200,9 @@ __device__ __forceinline__ void produce(const Geo& g, int64_t base, Pipe& P, uin
     int* rw = &P.row[s][0][0] + 2 * lane;
     if (src < g.nsrc) {
       const SumDesc d = g.desc[src];
-      const int64_t first = (base + d.lo) * SB;
+      const int64_t first = (g.base + d.lo) * SB;
       const int64_t a0 = first & ~int64_t(15);
-      const int64_t last = (base + d.lo + d.span) * SB + tile_bytes + 8;  // + funnel word
+      const int64_t last = (g.base + d.lo + d.span) * SB + tile_bytes + 8;  // + funnel word
       nbytes = static_cast<uint32_t>((last - a0 + 15) & ~int64_t(15));
       gsrc = g.src + static_cast<int64_t>(src) * g.src_pitch + a0;
       const int qbase = (QS * s + lane) * ww;
@@ -243,21 +230,16 @@ __device__ __forceinline__ void produce(const Geo& g, int64_t base, Pipe& P, uin
   if (lane < QS && nbytes) bulk_copy(dst, gsrc, nbytes, &P.full[s]);
 }
 
-// Pipeline driver shared by the kernels: for each of the block's g.ntiles tiles
-// of T samples, calls body(stage, cur) for every group of QS sources once their
-// windows are in shared memory, then tile_end(tile) once the tile's last group
-// has been summed.  The ring of stages runs on across tiles, so the next
-// tile's first windows are in flight while a tile ends.
-template <int SB, int QS = 2, typename Body, typename TileEnd>
+// Pipeline driver shared by the kernels: calls body(stage, cur) for every
+// group of QS sources once their windows are in shared memory.
+template <int SB, int QS = 2, typename Body>
 __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, Pipe& P,
-                                             uint32_t* sw, int T, Body&& body, TileEnd&& tile_end) {
+                                             uint32_t* sw, int tile_bytes, Body&& body) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ww = L.win_bytes >> 2;
   const int S = L.stages;
   const int zero_q = QS * S * ww;
-  const int tile_bytes = T * SB;
-  const int ngroups = (g.nsrc + QS - 1) / QS;
-  const int npairs = ngroups * g.ntiles;  // groups of all tiles, tile by tile
+  const int npairs = (g.nsrc + QS - 1) / QS;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&P.full[s], 1);
@@ -275,8 +257,7 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
   int issued = 0;  // pairs whose copies warp 0 has issued
   if (warp == 0)
     for (; issued < min(S - 1, npairs); ++issued)
-      produce<SB, QS>(g, g.base + static_cast<int64_t>(issued / ngroups) * T, P, sw, ww, zero_q,
-                      tile_bytes, issued % ngroups, issued, lane);
+      produce<SB, QS>(g, P, sw, ww, zero_q, tile_bytes, issued, issued, lane);
   int s_cur = 0, p = 0;
   uint32_t ph_cur = 0;
   for (; p < npairs; ++p) {
@@ -295,8 +276,7 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
         }
         break;
       }
-      produce<SB, QS>(g, g.base + static_cast<int64_t>(q / ngroups) * T, P, sw, ww, zero_q,
-                      tile_bytes, q % ngroups, s, lane);
+      produce<SB, QS>(g, P, sw, ww, zero_q, tile_bytes, q, s, lane);
       ++issued;
     }
     const bool ok = mbar_wait(&P.full[s_cur], ph_cur, failed, L.err);
@@ -314,7 +294,6 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
       s_cur = 0;
       ph_cur ^= 1u;
     }
-    if ((p + 1) % ngroups == 0) tile_end(p / ngroups);
   }
   if (warp == 0 && lane == 0 && *failed) {
     // let the copies already issued land before the block's shared memory goes away
@@ -356,31 +335,29 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
     for (int k = 0; k < NW; ++k) ev[r][k] = od[r][k] = 0;
   // Writes the lane sums of rows [0, nrows) to the output, adding them to the
   // partial sums an earlier flush stored there when `add`, and clears the lanes.
-  auto emit = [&](int tt, bool add) {
-    char* out = tile_out(g, tt, T);
-    const int64_t valid = tile_valid(g, tt, T);
+  auto emit = [&](bool add) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
       if (r >= g.nrows) break;
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
-        const int64_t t = static_cast<int64_t>(wbase + kStride * k) * 4;  // tile-local sample
-        if (t < valid) {
+        const int64_t t = static_cast<int64_t>(wbase + kStride * k) * 4;  // block-local sample
+        if (t < g.valid) {
           const uint32_t s0 = ev[r][k] & 0xffffu, s1 = od[r][k] & 0xffffu;
           const uint32_t s2 = ev[r][k] >> 16, s3 = od[r][k] >> 16;
-          char* row = out + r * g.out_pitch;
+          char* row = g.out + r * g.out_pitch;
           if constexpr (OUT16) {
             uint16_t* dst = reinterpret_cast<uint16_t*>(row) + t;
-            if (t + 4 <= valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
+            if (t + 4 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
               *reinterpret_cast<uint2*>(dst) = make_uint2(__byte_perm(ev[r][k], od[r][k], 0x5410),
                                                           __byte_perm(ev[r][k], od[r][k], 0x7632));
             } else {
               const uint32_t v[4] = {s0, s1, s2, s3};
-              for (int q = 0; q < 4 && t + q < valid; ++q) dst[q] = static_cast<uint16_t>(v[q]);
+              for (int q = 0; q < 4 && t + q < g.valid; ++q) dst[q] = static_cast<uint16_t>(v[q]);
             }
           } else {
             uint32_t* dst = reinterpret_cast<uint32_t*>(row) + t;
-            if (t + 4 <= valid && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+            if (t + 4 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
               uint4 v = make_uint4(s0, s1, s2, s3);
               if (add) {
                 const uint4 o = *reinterpret_cast<const uint4*>(dst);
@@ -389,7 +366,7 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
               *reinterpret_cast<uint4*>(dst) = v;
             } else {
               const uint32_t v[4] = {s0, s1, s2, s3};
-              for (int q = 0; q < 4 && t + q < valid; ++q) dst[q] = add ? dst[q] + v[q] : v[q];
+              for (int q = 0; q < 4 && t + q < g.valid; ++q) dst[q] = add ? dst[q] + v[q] : v[q];
             }
           }
         }
@@ -398,8 +375,7 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
     }
   };
   int since = 0;       // sources summed in the 16-bit lanes since the last flush
-  bool stored = false; // the output holds partial sums of an earlier flush of this tile
-  int cur_tile = 0;    // tile the body is summing
+  bool stored = false; // the output holds partial sums of an earlier flush
   run_pipeline<1>(L, g, P, sw, T, [&](int s, const uint32_t* win) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
@@ -431,46 +407,14 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
     if constexpr (FLUSH) {
       since += 2;
       if (since >= 256) {  // 256 x 255 fits a 16-bit lane: move the lanes to the output
-        emit(cur_tile, stored);
+        emit(stored);
         stored = true;
         since = 0;
       }
     }
-  }, [&](int tt) {
-    emit(tt, FLUSH && stored);
-    stored = false;
-    since = 0;
-    cur_tile = tt + 1;
   });
-}
-
-// Stores the 32-bit sums of samples (2w, 2w+1) of tile tt, word w = wbase +
-// kStride*k, rows [0, g.nrows), and clears them.
-template <int RB, int NW>
-__device__ __forceinline__ void store_word_pairs(const Geo& g, int tt, int T, int wbase,
-                                                 int kStride, uint32_t (&lo)[RB][NW],
-                                                 uint32_t (&hi)[RB][NW]) {
-  char* out = tile_out(g, tt, T);
-  const int64_t valid = tile_valid(g, tt, T);
-#pragma unroll
-  for (int r = 0; r < RB; ++r) {
-    if (r < g.nrows) {
-#pragma unroll
-      for (int k = 0; k < NW; ++k) {
-        const int64_t t = static_cast<int64_t>(wbase + kStride * k) * 2;
-        if (t >= valid) continue;
-        uint32_t* dst = reinterpret_cast<uint32_t*>(out + r * g.out_pitch) + t;
-        if (t + 2 <= valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
-          *reinterpret_cast<uint2*>(dst) = make_uint2(lo[r][k], hi[r][k]);
-        } else {
-          dst[0] = lo[r][k];
-          if (t + 1 < valid) dst[1] = hi[r][k];
-        }
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < NW; ++k) lo[r][k] = hi[r][k] = 0;
-  }
+  if (P.failed) return;
+  emit(FLUSH && stored);
 }
 
 // ------------------------------------------------------------------ 16-bit samples
@@ -492,7 +436,7 @@ __device__ __forceinline__ void sum_u16(const SumLaunch& L, uint3 blk, uint32_t*
   const int npairs = (g.nsrc + 1) / 2;
   const int per = L.lane_per;
   int since = 0, done = 0;
-  run_pipeline<2>(L, g, P, sw, T, [&](int s, const uint32_t* win) {
+  run_pipeline<2>(L, g, P, sw, 2 * T, [&](int s, const uint32_t* win) {
     ++done;
     if (per >= 2) {
 #pragma unroll
@@ -547,10 +491,24 @@ __device__ __forceinline__ void sum_u16(const SumLaunch& L, uint3 blk, uint32_t*
         }
       }
     }
-  }, [&](int tt) {
-    store_word_pairs<RB, NW>(g, tt, T, wbase, kStride, lo32, hi32);
-    since = done = 0;
   });
+  if (P.failed) return;
+#pragma unroll
+  for (int r = 0; r < RB; ++r) {
+    if (r >= g.nrows) break;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      const int64_t t = static_cast<int64_t>(wbase + kStride * k) * 2;
+      if (t >= g.valid) continue;
+      uint32_t* dst = reinterpret_cast<uint32_t*>(g.out + r * g.out_pitch) + t;
+      if (t + 2 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
+        *reinterpret_cast<uint2*>(dst) = make_uint2(lo32[r][k], hi32[r][k]);
+      } else {
+        dst[0] = lo32[r][k];
+        if (t + 1 < g.valid) dst[1] = hi32[r][k];
+      }
+    }
+  }
 }
 
 // 16-bit samples into 32-bit sums (stage 1 and brute force of 16-bit input).
@@ -574,7 +532,7 @@ __device__ __forceinline__ void sum_u16_wide(const SumLaunch& L, uint3 blk, uint
   for (int r = 0; r < RB; ++r)
 #pragma unroll
     for (int k = 0; k < NW; ++k) lo32[r][k] = hi32[r][k] = 0;
-  run_pipeline<2>(L, g, P, sw, T, [&](int s, const uint32_t* win) {
+  run_pipeline<2>(L, g, P, sw, 2 * T, [&](int s, const uint32_t* win) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
       const int4 rw = row_pair(P, s, r, 0);
@@ -604,7 +562,24 @@ __device__ __forceinline__ void sum_u16_wide(const SumLaunch& L, uint3 blk, uint
         hi32[r][k] += ahi + bhi;
       }
     }
-  }, [&](int tt) { store_word_pairs<RB, NW>(g, tt, T, wbase, kStride, lo32, hi32); });
+  });
+  if (P.failed) return;
+#pragma unroll
+  for (int r = 0; r < RB; ++r) {
+    if (r >= g.nrows) break;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      const int64_t t = static_cast<int64_t>(wbase + kStride * k) * 2;
+      if (t >= g.valid) continue;
+      uint32_t* dst = reinterpret_cast<uint32_t*>(g.out + r * g.out_pitch) + t;
+      if (t + 2 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
+        *reinterpret_cast<uint2*>(dst) = make_uint2(lo32[r][k], hi32[r][k]);
+      } else {
+        dst[0] = lo32[r][k];
+        if (t + 1 < g.valid) dst[1] = hi32[r][k];
+      }
+    }
+  }
 }
 
 // ------------------------------------------------------------------ 32-bit samples
@@ -622,7 +597,7 @@ __device__ __forceinline__ void sum_u32(const SumLaunch& L, uint3 blk, uint32_t*
   for (int r = 0; r < RB; ++r)
 #pragma unroll
     for (int k = 0; k < NW; ++k) acc[r][k] = 0;
-  run_pipeline<4>(L, g, P, sw, T, [&](int s, const uint32_t* win) {
+  run_pipeline<4>(L, g, P, sw, 4 * T, [&](int s, const uint32_t* win) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
       const int4 rw = row_pair(P, s, r, 0);
@@ -631,23 +606,18 @@ __device__ __forceinline__ void sum_u32(const SumLaunch& L, uint3 blk, uint32_t*
 #pragma unroll
       for (int k = 0; k < NW; ++k) acc[r][k] += w0[32 * k] + w1[32 * k];
     }
-  }, [&](int tt) {
-    char* out = tile_out(g, tt, T);
-    const int64_t valid = tile_valid(g, tt, T);
-#pragma unroll
-    for (int r = 0; r < RB; ++r) {
-      if (r < g.nrows) {
-        uint32_t* row = reinterpret_cast<uint32_t*>(out + r * g.out_pitch);
-#pragma unroll
-        for (int k = 0; k < NW; ++k) {
-          const int64_t t = wbase + 32 * k;
-          if (t < valid) row[t] = acc[r][k];
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < NW; ++k) acc[r][k] = 0;
-    }
   });
+  if (P.failed) return;
+#pragma unroll
+  for (int r = 0; r < RB; ++r) {
+    if (r >= g.nrows) break;
+    uint32_t* row = reinterpret_cast<uint32_t*>(g.out + r * g.out_pitch);
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      const int64_t t = wbase + 32 * k;
+      if (t < g.valid) row[t] = acc[r][k];
+    }
+  }
 }
 
 // ------------------------------------------------------------------ 16-bit sums, four sources per stage
@@ -661,33 +631,19 @@ __device__ __forceinline__ void sum_u32(const SumLaunch& L, uint3 blk, uint32_t*
 // the FMA pipe).  Since no group's low lane carries, the low samples' sum is
 // lo - (hi << 16) at the end.  Shared-memory bytes per sample addition are
 // about half those of 32-bit subband sums.
-#ifndef DD_SUM16Q_BRANCHLESS
-#define DD_SUM16Q_BRANCHLESS 1
-#endif
-// Adds one source's NW aligned words to q.  The branch-free form always loads
-// NW + 1 words and aligns them with a byte permute whose selector is 0x3210 (no
-// shift) or 0x5432 (one sample), so the loads of all sources of a row can be
-// issued together; the branching form skips the extra load and the permutes of
-// even offsets.
+// Adds one source's NW aligned words to q: always NW + 1 loads and one byte
+// permute per word, whose selector is 0x3210 (even offset) or 0x5432 (offset by
+// one sample), so that no branch separates the loads of a row's four sources
+// (the form that skipped the extra load and the permutes of even offsets was
+// 3 ms slower per headline step).
 template <int NW>
 __device__ __forceinline__ void add_u16_src(uint32_t (&q)[NW], const uint32_t* w, int shift) {
-  if (DD_SUM16Q_BRANCHLESS) {
-    const uint32_t sel = shift ? 0x5432u : 0x3210u;
-    uint32_t v[NW + 1];
+  const uint32_t sel = shift ? 0x5432u : 0x3210u;
+  uint32_t v[NW + 1];
 #pragma unroll
-    for (int i = 0; i <= NW; ++i) v[i] = w[i];
+  for (int i = 0; i <= NW; ++i) v[i] = w[i];
 #pragma unroll
-    for (int k = 0; k < NW; ++k) q[k] += __byte_perm(v[k], v[k + 1], sel);
-  } else if (shift == 0) {  // uniform over the block: the source's offset is even
-#pragma unroll
-    for (int k = 0; k < NW; ++k) q[k] += w[k];
-  } else {
-    uint32_t v[NW + 1];
-#pragma unroll
-    for (int i = 0; i <= NW; ++i) v[i] = w[i];
-#pragma unroll
-    for (int k = 0; k < NW; ++k) q[k] += __byte_perm(v[k], v[k + 1], 0x5432);
-  }
+  for (int k = 0; k < NW; ++k) q[k] += __byte_perm(v[k], v[k + 1], sel);
 }
 
 template <int RB, int NW>
@@ -703,7 +659,7 @@ __device__ __forceinline__ void sum_u16_quad(const SumLaunch& L, uint3 blk, uint
   for (int r = 0; r < RB; ++r)
 #pragma unroll
     for (int k = 0; k < NW; ++k) lo[r][k] = hi[r][k] = 0;
-  run_pipeline<2, 4>(L, g, P, sw, T, [&](int s, const uint32_t* win) {
+  run_pipeline<2, 4>(L, g, P, sw, 2 * T, [&](int s, const uint32_t* win) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
       const int4 a = row_pair(P, s, r, 0), b = row_pair(P, s, r, 1);
@@ -720,13 +676,25 @@ __device__ __forceinline__ void sum_u16_quad(const SumLaunch& L, uint3 blk, uint
         hi[r][k] = __umulhi(q[k], 0x10000u) + hi[r][k];
       }
     }
-  }, [&](int tt) {
-#pragma unroll
-    for (int r = 0; r < RB; ++r)
-#pragma unroll
-      for (int k = 0; k < NW; ++k) lo[r][k] -= hi[r][k] << 16;  // the low samples' sums
-    store_word_pairs<RB, NW>(g, tt, T, wbase, 1, lo, hi);
   });
+  if (P.failed) return;
+#pragma unroll
+  for (int r = 0; r < RB; ++r) {
+    if (r >= g.nrows) break;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      const int64_t t = static_cast<int64_t>(wbase + k) * 2;
+      if (t >= g.valid) continue;
+      const uint32_t s0 = lo[r][k] - (hi[r][k] << 16), s1 = hi[r][k];
+      uint32_t* dst = reinterpret_cast<uint32_t*>(g.out + r * g.out_pitch) + t;
+      if (t + 2 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
+        *reinterpret_cast<uint2*>(dst) = make_uint2(s0, s1);
+      } else {
+        dst[0] = s0;
+        if (t + 1 < g.valid) dst[1] = s1;
+      }
+    }
+  }
 }
 
 template <int RB, int NW, bool OUT16, bool FLUSH>
@@ -954,31 +922,7 @@ std::vector<SumDesc> build_sum_desc(const std::vector<int32_t>& tab, int64_t nro
   return d;
 }
 
-#ifndef DD_SUM_MIN_WAVES
-#define DD_SUM_MIN_WAVES 16
-#endif
-// Tiles per block of a plain launch: as many as keep at least DD_SUM_MIN_WAVES
-// waves of two blocks per SM (at most 8), spread evenly over the blocks of a row.
-// A block that sums several tiles keeps its staging ring running from one tile
-// into the next, so its start-up (barrier set-up, first copies) is paid once.
-int sum_tiles_per_block(const SumLaunch& L) {
-  static int sms[64] = {};
-  int dev = 0;
-  DD_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return 1;
-  if (!sms[dev]) DD_CUDA_TRY(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
-  const int T = sum_kind_tile(sum_kind(L));
-  const long long tiles = (L.ncols + T - 1) / T;
-  const long long total = tiles * L.grid_y * L.grid_z;
-  long long tmax = total / (static_cast<long long>(sms[dev]) * 2 * DD_SUM_MIN_WAVES);
-  tmax = std::max(1LL, std::min(8LL, std::min(tmax, tiles)));
-  const long long nxb = (tiles + tmax - 1) / tmax;
-  return static_cast<int>((tiles + nxb - 1) / nxb);
-}
-
-void launch_sum(const SumLaunch& L0, cudaStream_t st) {
-  SumLaunch L = L0;
-  L.tiles_per_block = sum_tiles_per_block(L0);
+void launch_sum(const SumLaunch& L, cudaStream_t st) {
   dim3 grid(sum_grid_x(L), L.grid_y, L.grid_z);
   if (L.stages < 2 || L.stages > kMaxStages) throw Error{DD_ERR_RUNTIME, "bad stage count"};
   if (!L.desc || !L.err) throw Error{DD_ERR_RUNTIME, "staged sum without descriptors"};
@@ -1006,9 +950,7 @@ int sum_kind(const SumLaunch& L) {
 
 unsigned sum_grid_x(const SumLaunch& L) {
   const int T = sum_kind_tile(sum_kind(L));
-  const int64_t tiles = (L.ncols + T - 1) / T;
-  const int tpb = L.tiles_per_block > 1 ? L.tiles_per_block : 1;
-  return static_cast<unsigned>((tiles + tpb - 1) / tpb);
+  return static_cast<unsigned>((L.ncols + T - 1) / T);
 }
 
 int sum_batch_blocks_per_sm(size_t smem) {
