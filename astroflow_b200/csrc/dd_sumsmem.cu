@@ -106,6 +106,22 @@ __device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t b
 // the shifts and byte permutes keep busy (stage 1: 78.0 -> 74.8 ms at the
 // headline size; the widening variant is faster with plain adds).
 constexpr bool kSumImad = DD_SUM_IMAD != 0;
+// High word of a*b plus c on the FMA pipe (b a runtime value, e.g. 2^k built
+// from L.one, so the compiler cannot turn it into a shift on the integer pipe).
+__device__ __forceinline__ uint32_t madhi_u32(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t d;
+  asm("mad.hi.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+// How 8-bit samples are split into 16-bit lanes (DD_SUM8_SPLIT):
+//  0: two byte permutes per word (integer pipe), lanes added by multiply-adds;
+//  1: even lanes = word & 0x00ff00ff (integer pipe), odd lanes accumulated as the
+//     high word of (word - even) * 2^24 (FMA pipe), even lanes added by
+//     multiply-adds: one integer-pipe operation per word fewer than 0;
+//  2: as 1, with two sources' even lanes added by one three-input add.
+#ifndef DD_SUM8_SPLIT
+#define DD_SUM8_SPLIT 2
+#endif
 __device__ __forceinline__ uint32_t mad_u32(uint32_t a, uint32_t b, uint32_t c) {
   uint32_t d;
   asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
@@ -328,6 +344,7 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
   constexpr int kStride = kConsec ? 1 : 32;
   const int wbase = kConsec ? warp * 32 * NW + lane * NW : warp * 32 * NW + lane;
   const uint32_t one = L.one;
+  const uint32_t neg1 = 0u - one, sh24 = one << 24;  // runtime -1 and 2^24
   uint32_t ev[RB][NW], od[RB][NW];  // 16-bit lanes: samples (4w, 4w+2) and (4w+1, 4w+3)
 #pragma unroll
   for (int r = 0; r < RB; ++r)
@@ -393,7 +410,18 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
                                    : __funnelshift_r(w0[32 * k], w0[32 * k + 1], rw.y);
         const uint32_t b = kConsec ? __funnelshift_r(vb[k], vb[k + 1], rw.w)
                                    : __funnelshift_r(w1[32 * k], w1[32 * k + 1], rw.w);
-        if constexpr (kSumImad) {
+        if constexpr (DD_SUM8_SPLIT == 1) {
+          const uint32_t ea = a & 0x00ff00ffu, eb = b & 0x00ff00ffu;
+          ev[r][k] = mad_u32(ea, one, ev[r][k]);
+          ev[r][k] = mad_u32(eb, one, ev[r][k]);
+          od[r][k] = madhi_u32(mad_u32(ea, neg1, a), sh24, od[r][k]);
+          od[r][k] = madhi_u32(mad_u32(eb, neg1, b), sh24, od[r][k]);
+        } else if constexpr (DD_SUM8_SPLIT == 2) {
+          const uint32_t ea = a & 0x00ff00ffu, eb = b & 0x00ff00ffu;
+          ev[r][k] += ea + eb;
+          od[r][k] = madhi_u32(mad_u32(ea, neg1, a), sh24, od[r][k]);
+          od[r][k] = madhi_u32(mad_u32(eb, neg1, b), sh24, od[r][k]);
+        } else if constexpr (kSumImad) {
           ev[r][k] = mad_u32(__byte_perm(a, 0u, 0x4240), one, ev[r][k]);
           ev[r][k] = mad_u32(__byte_perm(b, 0u, 0x4240), one, ev[r][k]);
           od[r][k] = mad_u32(__byte_perm(a, 0u, 0x4341), one, od[r][k]);
@@ -654,6 +682,7 @@ __device__ __forceinline__ void sum_u16_quad(const SumLaunch& L, uint3 blk, uint
   if (g.nrows <= 0) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wbase = warp * 32 * NW + lane * NW;
+  const uint32_t sh16 = L.one << 16;  // 2^16, a runtime value: the multiply-high stays on the FMA pipe
   uint32_t lo[RB][NW], hi[RB][NW];
 #pragma unroll
   for (int r = 0; r < RB; ++r)
@@ -673,7 +702,7 @@ __device__ __forceinline__ void sum_u16_quad(const SumLaunch& L, uint3 blk, uint
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
         lo[r][k] += q[k];
-        hi[r][k] = __umulhi(q[k], 0x10000u) + hi[r][k];
+        hi[r][k] = madhi_u32(q[k], sh16, hi[r][k]);
       }
     }
   });
