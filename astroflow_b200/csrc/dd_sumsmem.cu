@@ -119,8 +119,10 @@ __device__ __forceinline__ uint32_t madhi_u32(uint32_t a, uint32_t b, uint32_t c
 //     high word of (word - even) * 2^24 (FMA pipe), even lanes added by
 //     multiply-adds: one integer-pipe operation per word fewer than 0;
 //  2: as 1, with two sources' even lanes added by one three-input add.
+// Measured at the headline size (stage 1, ms): 0 -> 76.5, 1 -> 107, 2 -> 92; the
+// multiply-high chains cost more than the integer-pipe operations they save.
 #ifndef DD_SUM8_SPLIT
-#define DD_SUM8_SPLIT 2
+#define DD_SUM8_SPLIT 0
 #endif
 __device__ __forceinline__ uint32_t mad_u32(uint32_t a, uint32_t b, uint32_t c) {
   uint32_t d;
@@ -682,7 +684,6 @@ __device__ __forceinline__ void sum_u16_quad(const SumLaunch& L, uint3 blk, uint
   if (g.nrows <= 0) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wbase = warp * 32 * NW + lane * NW;
-  const uint32_t sh16 = L.one << 16;  // 2^16, a runtime value: the multiply-high stays on the FMA pipe
   uint32_t lo[RB][NW], hi[RB][NW];
 #pragma unroll
   for (int r = 0; r < RB; ++r)
@@ -702,7 +703,7 @@ __device__ __forceinline__ void sum_u16_quad(const SumLaunch& L, uint3 blk, uint
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
         lo[r][k] += q[k];
-        hi[r][k] = madhi_u32(q[k], sh16, hi[r][k]);
+        hi[r][k] = __umulhi(q[k], 0x10000u) + hi[r][k];
       }
     }
   });
