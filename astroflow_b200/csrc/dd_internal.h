@@ -242,6 +242,13 @@ void launch_brute(const BruteArgs& a, cudaStream_t st);
 
 // ---- shared-memory staged sums (dd_sumsmem.cu) ----
 constexpr int kSumRows = 8;  // output rows per block
+// Groups of warps the block's rows are split over in the 8-bit and the quad
+// 16-bit kernels: each group covers the whole tile for kSumRows/DD_SUM_ROWSPLIT
+// rows (fewer accumulators per thread, a shorter tile).
+#ifndef DD_SUM_ROWSPLIT
+#define DD_SUM_ROWSPLIT 1
+#endif
+constexpr int kSumRowsPT = kSumRows / DD_SUM_ROWSPLIT;
 // Staging descriptor of one (row group, source) pair of a staged sum: the
 // smallest offset of the group's rows for that source, the spread of their
 // offsets, and each row's offset relative to the smallest.  Built on the host
@@ -338,9 +345,9 @@ constexpr int kSum16QNW = DD_SUM16Q_NW;
 // flush: 8-bit lanes added into the output every 256 sources; 16-bit sources summed into
 // 32-bit lanes (the k_sum_u16w variant).
 inline int sum_variant_tile(int src_bytes, bool flush) {
-  return sum_tile_samples(src_bytes, src_bytes == 4   ? kSum32NW
-                                     : src_bytes == 2 ? (flush ? DD_SUM16W_NW : DD_SUM16_NW)
-                                                      : (flush ? DD_SUM8F_NW : DD_SUM8_NW));
+  return src_bytes == 4   ? sum_tile_samples(4, kSum32NW)
+         : src_bytes == 2 ? sum_tile_samples(2, flush ? DD_SUM16W_NW : DD_SUM16_NW)
+                          : sum_tile_samples(1, flush ? DD_SUM8F_NW : DD_SUM8_NW) / DD_SUM_ROWSPLIT;
 }
 // Tile (samples per block) of a kernel variant (SumKind below).
 inline int sum_kind_tile(int kind);
@@ -352,11 +359,11 @@ constexpr int kSumKinds = 7;
 int sum_kind(const SumLaunch& L);
 inline int sum_kind_tile(int kind) {
   switch (kind) {
-    case kSumKindU8Out16: case kSumKindU8: return sum_tile_samples(1, DD_SUM8_NW);
-    case kSumKindU8Flush: return sum_tile_samples(1, DD_SUM8F_NW);
+    case kSumKindU8Out16: case kSumKindU8: return sum_tile_samples(1, DD_SUM8_NW) / DD_SUM_ROWSPLIT;
+    case kSumKindU8Flush: return sum_tile_samples(1, DD_SUM8F_NW) / DD_SUM_ROWSPLIT;
     case kSumKindU16: return sum_tile_samples(2, DD_SUM16_NW);
     case kSumKindU16Wide: return sum_tile_samples(2, DD_SUM16W_NW);
-    case kSumKindU16Quad: return sum_tile_samples(2, kSum16QNW);
+    case kSumKindU16Quad: return sum_tile_samples(2, kSum16QNW) / DD_SUM_ROWSPLIT;
     default: return sum_tile_samples(4, kSum32NW);
   }
 }

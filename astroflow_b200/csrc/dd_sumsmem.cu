@@ -121,6 +121,9 @@ __device__ __forceinline__ uint32_t madhi_u32(uint32_t a, uint32_t b, uint32_t c
 //  2: as 1, with two sources' even lanes added by one three-input add.
 // Measured at the headline size (stage 1, ms): 0 -> 76.5, 1 -> 107, 2 -> 92; the
 // multiply-high chains cost more than the integer-pipe operations they save.
+#ifndef DD_SUM16Q_MINB
+#define DD_SUM16Q_MINB 2
+#endif
 #ifndef DD_SUM8_SPLIT
 #define DD_SUM8_SPLIT 0
 #endif
@@ -336,15 +339,20 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
 template <int RB, int NW, bool OUT16, bool FLUSH>
 __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* sw, Pipe& P) {
   static_assert(!(OUT16 && FLUSH), "16-bit outputs hold at most 257 sources: no flushes");
-  constexpr int T = kWarps * 32 * NW * 4;
+  // RB rows per thread: the block's kSumRows rows are split over kSumRows/RB
+  // groups of warps, each group covering the whole tile for its RB rows
+  constexpr int kGroups = kSumRows / RB;
+  constexpr int kWarpsPerTile = kWarps / kGroups;
+  constexpr int T = kWarpsPerTile * 32 * NW * 4;
   const Geo g = make_geo(L, T, blk);
   if (g.nrows <= 0) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rbase = (warp / kWarpsPerTile) * RB, wt = warp % kWarpsPerTile;
   // odd NW: lane owns NW consecutive words (NW+1 conflict-free loads per row and
   // source); even NW: lane owns words lane, lane+32, ... (2 loads per word)
   constexpr bool kConsec = (NW & 1) != 0;
   constexpr int kStride = kConsec ? 1 : 32;
-  const int wbase = kConsec ? warp * 32 * NW + lane * NW : warp * 32 * NW + lane;
+  const int wbase = kConsec ? wt * 32 * NW + lane * NW : wt * 32 * NW + lane;
   const uint32_t one = L.one;
   const uint32_t neg1 = 0u - one, sh24 = one << 24;  // runtime -1 and 2^24
   uint32_t ev[RB][NW], od[RB][NW];  // 16-bit lanes: samples (4w, 4w+2) and (4w+1, 4w+3)
@@ -357,14 +365,14 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
   auto emit = [&](bool add) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
-      if (r >= g.nrows) break;
+      if (rbase + r >= g.nrows) break;
 #pragma unroll
       for (int k = 0; k < NW; ++k) {
         const int64_t t = static_cast<int64_t>(wbase + kStride * k) * 4;  // block-local sample
         if (t < g.valid) {
           const uint32_t s0 = ev[r][k] & 0xffffu, s1 = od[r][k] & 0xffffu;
           const uint32_t s2 = ev[r][k] >> 16, s3 = od[r][k] >> 16;
-          char* row = g.out + r * g.out_pitch;
+          char* row = g.out + (rbase + r) * g.out_pitch;
           if constexpr (OUT16) {
             uint16_t* dst = reinterpret_cast<uint16_t*>(row) + t;
             if (t + 4 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
@@ -398,7 +406,7 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
   run_pipeline<1>(L, g, P, sw, T, [&](int s, const uint32_t* win) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
-      const int4 rw = row_pair(P, s, r, 0);
+      const int4 rw = row_pair(P, s, rbase + r, 0);
       const uint32_t* w0 = win + rw.x + wbase;
       const uint32_t* w1 = win + rw.z + wbase;
       uint32_t va[NW + 1], vb[NW + 1];
@@ -679,11 +687,14 @@ __device__ __forceinline__ void add_u16_src(uint32_t (&q)[NW], const uint32_t* w
 template <int RB, int NW>
 __device__ __forceinline__ void sum_u16_quad(const SumLaunch& L, uint3 blk, uint32_t* sw, Pipe& P) {
   static_assert(NW & 1, "an odd number of consecutive words per lane keeps the loads conflict-free");
-  constexpr int T = kWarps * 32 * NW * 2;
+  constexpr int kGroups = kSumRows / RB;  // warp groups sharing the rows, as in sum_u8
+  constexpr int kWarpsPerTile = kWarps / kGroups;
+  constexpr int T = kWarpsPerTile * 32 * NW * 2;
   const Geo g = make_geo(L, T, blk);
   if (g.nrows <= 0) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wbase = warp * 32 * NW + lane * NW;
+  const int rbase = (warp / kWarpsPerTile) * RB;
+  const int wbase = (warp % kWarpsPerTile) * 32 * NW + lane * NW;
   uint32_t lo[RB][NW], hi[RB][NW];
 #pragma unroll
   for (int r = 0; r < RB; ++r)
@@ -692,7 +703,7 @@ __device__ __forceinline__ void sum_u16_quad(const SumLaunch& L, uint3 blk, uint
   run_pipeline<2, 4>(L, g, P, sw, 2 * T, [&](int s, const uint32_t* win) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
-      const int4 a = row_pair(P, s, r, 0), b = row_pair(P, s, r, 1);
+      const int4 a = row_pair(P, s, rbase + r, 0), b = row_pair(P, s, rbase + r, 1);
       uint32_t q[NW];
 #pragma unroll
       for (int k = 0; k < NW; ++k) q[k] = 0;
@@ -710,13 +721,13 @@ __device__ __forceinline__ void sum_u16_quad(const SumLaunch& L, uint3 blk, uint
   if (P.failed) return;
 #pragma unroll
   for (int r = 0; r < RB; ++r) {
-    if (r >= g.nrows) break;
+    if (rbase + r >= g.nrows) break;
 #pragma unroll
     for (int k = 0; k < NW; ++k) {
       const int64_t t = static_cast<int64_t>(wbase + k) * 2;
       if (t >= g.valid) continue;
       const uint32_t s0 = lo[r][k] - (hi[r][k] << 16), s1 = hi[r][k];
-      uint32_t* dst = reinterpret_cast<uint32_t*>(g.out + r * g.out_pitch) + t;
+      uint32_t* dst = reinterpret_cast<uint32_t*>(g.out + (rbase + r) * g.out_pitch) + t;
       if (t + 2 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
         *reinterpret_cast<uint2*>(dst) = make_uint2(s0, s1);
       } else {
@@ -746,7 +757,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sum_u16w(SumLaunch L) {
   sum_u16_wide<RB, NW>(L, blockIdx, sw, P);
 }
 template <int RB, int NW>
-__global__ void __launch_bounds__(kThreads, 2) k_sum_u16q(SumLaunch L) {
+__global__ void __launch_bounds__(kThreads, DD_SUM16Q_MINB) k_sum_u16q(SumLaunch L) {
   extern __shared__ __align__(128) uint32_t sw[];
   __shared__ Pipe P;
   sum_u16_quad<RB, NW>(L, blockIdx, sw, P);
@@ -788,12 +799,12 @@ __device__ __forceinline__ uint3 group_block(long long local, unsigned gx, unsig
 
 template <int KIND>
 __device__ __forceinline__ void run_one(const SumLaunch& L, uint3 blk, uint32_t* sw, Pipe& P) {
-  if constexpr (KIND == kSumKindU8Out16) sum_u8<kSumRows, DD_SUM8_NW, true, false>(L, blk, sw, P);
-  else if constexpr (KIND == kSumKindU8Flush) sum_u8<kSumRows, DD_SUM8F_NW, false, true>(L, blk, sw, P);
-  else if constexpr (KIND == kSumKindU8) sum_u8<kSumRows, DD_SUM8_NW, false, false>(L, blk, sw, P);
+  if constexpr (KIND == kSumKindU8Out16) sum_u8<kSumRowsPT, DD_SUM8_NW, true, false>(L, blk, sw, P);
+  else if constexpr (KIND == kSumKindU8Flush) sum_u8<kSumRowsPT, DD_SUM8F_NW, false, true>(L, blk, sw, P);
+  else if constexpr (KIND == kSumKindU8) sum_u8<kSumRowsPT, DD_SUM8_NW, false, false>(L, blk, sw, P);
   else if constexpr (KIND == kSumKindU16) sum_u16<kSumRows, DD_SUM16_NW>(L, blk, sw, P);
   else if constexpr (KIND == kSumKindU16Wide) sum_u16_wide<kSumRows, DD_SUM16W_NW>(L, blk, sw, P);
-  else if constexpr (KIND == kSumKindU16Quad) sum_u16_quad<kSumRows, kSum16QNW>(L, blk, sw, P);
+  else if constexpr (KIND == kSumKindU16Quad) sum_u16_quad<kSumRowsPT, kSum16QNW>(L, blk, sw, P);
   else sum_u32<kSumRows, kSum32NW>(L, blk, sw, P);
 }
 
@@ -959,12 +970,12 @@ void launch_sum(const SumLaunch& L, cudaStream_t st) {
   const size_t smem = sum_launch_smem(L);
   if (L.rows_per_block != kSumRows) throw Error{DD_ERR_RUNTIME, "unsupported rows per block"};
   switch (sum_kind(L)) {
-    case kSumKindU8Out16: launch_k(k_sum_u8<kSumRows, DD_SUM8_NW, true, false>, grid, smem, L, st); break;
-    case kSumKindU8Flush: launch_k(k_sum_u8<kSumRows, DD_SUM8F_NW, false, true>, grid, smem, L, st); break;
-    case kSumKindU8: launch_k(k_sum_u8<kSumRows, DD_SUM8_NW, false, false>, grid, smem, L, st); break;
+    case kSumKindU8Out16: launch_k(k_sum_u8<kSumRowsPT, DD_SUM8_NW, true, false>, grid, smem, L, st); break;
+    case kSumKindU8Flush: launch_k(k_sum_u8<kSumRowsPT, DD_SUM8F_NW, false, true>, grid, smem, L, st); break;
+    case kSumKindU8: launch_k(k_sum_u8<kSumRowsPT, DD_SUM8_NW, false, false>, grid, smem, L, st); break;
     case kSumKindU16: launch_k(k_sum_u16<kSumRows, DD_SUM16_NW>, grid, smem, L, st); break;
     case kSumKindU16Wide: launch_k(k_sum_u16w<kSumRows, DD_SUM16W_NW>, grid, smem, L, st); break;
-    case kSumKindU16Quad: launch_k(k_sum_u16q<kSumRows, kSum16QNW>, grid, smem, L, st); break;
+    case kSumKindU16Quad: launch_k(k_sum_u16q<kSumRowsPT, kSum16QNW>, grid, smem, L, st); break;
     default: launch_k(k_sum_u32<kSumRows, kSum32NW>, grid, smem, L, st); break;
   }
 }
