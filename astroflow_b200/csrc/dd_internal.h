@@ -242,13 +242,20 @@ void launch_brute(const BruteArgs& a, cudaStream_t st);
 
 // ---- shared-memory staged sums (dd_sumsmem.cu) ----
 constexpr int kSumRows = 8;  // output rows per block
-// Groups of warps the block's rows are split over in the 8-bit and the quad
-// 16-bit kernels: each group covers the whole tile for kSumRows/DD_SUM_ROWSPLIT
-// rows (fewer accumulators per thread, a shorter tile).
+// Groups of warps the block's rows are split over: each group covers the whole
+// tile for kSumRows/ROWSPLIT rows (fewer accumulators per thread, more words per
+// lane).  Measured at the headline size (ms, stage 1 / stage 2): one group, 5
+// words per lane 77.0 / 53.9; two groups, 5 words 80.0 / 51.4; two groups, 9
+// words 77.6 / 50.9; two groups, 7 words 82.1 / 52.1.  The quad kernel (stage 2)
+// takes two groups of 9 words, the 8-bit kernels one group of 5.
 #ifndef DD_SUM_ROWSPLIT
 #define DD_SUM_ROWSPLIT 1
 #endif
+#ifndef DD_SUM16Q_ROWSPLIT
+#define DD_SUM16Q_ROWSPLIT 2
+#endif
 constexpr int kSumRowsPT = kSumRows / DD_SUM_ROWSPLIT;
+constexpr int kSumRowsPTQ = kSumRows / DD_SUM16Q_ROWSPLIT;
 // Staging descriptor of one (row group, source) pair of a staged sum: the
 // smallest offset of the group's rows for that source, the spread of their
 // offsets, and each row's offset relative to the smallest.  Built on the host
@@ -339,7 +346,7 @@ constexpr int kSum32NW = DD_SUM32_NW;  // words per lane of the 32-bit staged su
 #endif
 // Words per lane of the 16-bit quad stage-2 kernel (odd: conflict-free consecutive words).
 #ifndef DD_SUM16Q_NW
-#define DD_SUM16Q_NW 5
+#define DD_SUM16Q_NW 9
 #endif
 constexpr int kSum16QNW = DD_SUM16Q_NW;
 // flush: 8-bit lanes added into the output every 256 sources; 16-bit sources summed into
@@ -363,7 +370,7 @@ inline int sum_kind_tile(int kind) {
     case kSumKindU8Flush: return sum_tile_samples(1, DD_SUM8F_NW) / DD_SUM_ROWSPLIT;
     case kSumKindU16: return sum_tile_samples(2, DD_SUM16_NW);
     case kSumKindU16Wide: return sum_tile_samples(2, DD_SUM16W_NW);
-    case kSumKindU16Quad: return sum_tile_samples(2, kSum16QNW) / DD_SUM_ROWSPLIT;
+    case kSumKindU16Quad: return sum_tile_samples(2, kSum16QNW) / DD_SUM16Q_ROWSPLIT;
     default: return sum_tile_samples(4, kSum32NW);
   }
 }

@@ -82,6 +82,43 @@ __global__ void k_iqrm_stats(const T* __restrict__ x, int64_t nsamp, int64_t nch
   }
 }
 
+// 8-bit samples, four channels per thread (one aligned 32-bit load per row, a
+// warp reading 128 contiguous bytes): thread k covers channels (cs & ~3) + 4k ..
+// + 3; per window and time chunk it keeps 32-bit partial sums (a chunk of at
+// most 1024 rows: 1024 x 255^2 < 2^32) and adds them to the 64-bit sums of the
+// channels inside [cs, cs+csub).  Needs nchans % 4 == 0 and an aligned input.
+__global__ void k_iqrm_stats_u8w(const uint8_t* __restrict__ x, int64_t nsamp, int64_t nchans,
+                                 int64_t cs, int64_t csub, const uint32_t* __restrict__ win,
+                                 int nwin, int64_t chunk, unsigned long long* __restrict__ sums) {
+  const int64_t c4 = (cs & ~int64_t(3)) + 4 * (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x);
+  if (c4 >= cs + csub) return;
+  const int64_t lo = static_cast<int64_t>(blockIdx.y) * chunk;
+  const int64_t hi = lo + chunk < nsamp ? lo + chunk : nsamp;
+  for (int w = 0; w < nwin; ++w) {
+    const int64_t a = win[2 * w] > lo ? win[2 * w] : lo;
+    const int64_t b = win[2 * w + 1] < hi ? win[2 * w + 1] : hi;
+    if (a >= b) continue;
+    uint32_t s[4] = {0u, 0u, 0u, 0u}, q[4] = {0u, 0u, 0u, 0u};
+    for (int64_t t = a; t < b; ++t) {
+      const uint32_t v = __ldg(reinterpret_cast<const uint32_t*>(x + t * nchans + c4));
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const uint32_t e = (v >> (8 * k)) & 0xffu;
+        s[k] += e;
+        q[k] += e * e;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int64_t ch = c4 + k;
+      if (ch < cs || ch >= cs + csub) continue;
+      const int64_t i = ch - cs;
+      atomicAdd(&sums[(static_cast<int64_t>(w) * 2) * csub + i], static_cast<unsigned long long>(s[k]));
+      atomicAdd(&sums[(static_cast<int64_t>(w) * 2 + 1) * csub + i], static_cast<unsigned long long>(q[k]));
+    }
+  }
+}
+
 __device__ __forceinline__ int iqrm_target(int lag, int i, int csub) {
   if (lag < 0) return i < csub + lag ? i - lag : csub - 1;
   return i < lag ? 0 : i - lag;
@@ -330,29 +367,35 @@ __global__ void k_prep(PrepArgs a) {
 }
 
 // 8-bit samples without downsampling (the subband layout), as k_prep but four
-// channels per load and four samples per store: a block takes 64 samples x 64
-// channels, applies the masks and the zero-DM offset to whole words with
-// byte-wise SIMD operations, and transposes 4x4 byte blocks in registers.
-// Needs nchans % 4 == 0 (aligned word loads); channel words are read from
-// c0 & ~3 and channels outside [c0, c1) are not stored.
+// channels per load and four samples per store: a block takes kPrepU8Subtiles
+// consecutive tiles of 64 samples x 64 channels, one after another; for each it
+// applies the masks and the zero-DM offset to whole words with byte-wise SIMD
+// operations and transposes 4x4 byte blocks in registers.  Needs
+// nchans % 4 == 0 (aligned word loads); channel words are read from c0 & ~3 and
+// channels outside [c0, c1) are not stored.
+constexpr int kPrepU8Subtiles = 4;
 __global__ void __launch_bounds__(256) k_prep_u8(PrepArgs a) {
   __shared__ uint32_t tile[64][17];  // [sample][channel word], padded
   const uint8_t* x = static_cast<const uint8_t*>(a.x);
-  const int64_t tb = static_cast<int64_t>(blockIdx.x) * 64;
   const int64_t cb = (a.c0 & ~int64_t(3)) + static_cast<int64_t>(blockIdx.y) * 64;
-  {
-    const int w = threadIdx.x & 15;  // channel word of the tile
-    const int64_t c = cb + 4 * w;
-    const bool cvalid = c < a.nchans;
-    uint32_t drop = 0, inrange = 0;  // per byte: bad channel / zero-DM applies
-    if (cvalid) {
+  const int w = threadIdx.x & 15;  // channel word of the tile (load phase)
+  const int64_t c = cb + 4 * w;
+  const bool cvalid = c < a.nchans;
+  uint32_t drop = 0, inrange = 0;  // per byte: bad channel / zero-DM applies
+  if (cvalid) {
 #pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int64_t ch = c + b;
-        if (a.keep && !a.keep[ch]) drop |= 0xffu << (8 * b);
-        if (a.zdm_off && ch >= a.zdm_cs && ch < a.zdm_ce) inrange |= 0xffu << (8 * b);
-      }
+    for (int b = 0; b < 4; ++b) {
+      const int64_t ch = c + b;
+      if (a.keep && !a.keep[ch]) drop |= 0xffu << (8 * b);
+      if (a.zdm_off && ch >= a.zdm_cs && ch < a.zdm_ce) inrange |= 0xffu << (8 * b);
     }
+  }
+  const int i = threadIdx.x & 15;  // store phase: samples 4i .. 4i+3
+  const int j = threadIdx.x >> 4;  // channel word j: channels 4j .. 4j+3
+  uint8_t* out = static_cast<uint8_t*>(a.out);
+  for (int sub = 0; sub < kPrepU8Subtiles; ++sub) {
+    const int64_t tb = (static_cast<int64_t>(blockIdx.x) * kPrepU8Subtiles + sub) * 64;
+    if (tb >= a.nsamp) break;
     for (int r = threadIdx.x >> 4; r < 64; r += 16) {
       const int64_t t = tb + r;
       uint32_t v = 0;
@@ -372,23 +415,22 @@ __global__ void __launch_bounds__(256) k_prep_u8(PrepArgs a) {
       }
       tile[r][w] = v;
     }
-  }
-  __syncthreads();
-  if (!a.out) return;
-  const int i = threadIdx.x & 15;  // samples 4i .. 4i+3
-  const int j = threadIdx.x >> 4;  // channel word j: channels 4j .. 4j+3
-  const uint32_t q0 = tile[4 * i][j], q1 = tile[4 * i + 1][j];
-  const uint32_t q2 = tile[4 * i + 2][j], q3 = tile[4 * i + 3][j];
-  const uint32_t lo01 = __byte_perm(q0, q1, 0x5140), hi01 = __byte_perm(q0, q1, 0x7362);
-  const uint32_t lo23 = __byte_perm(q2, q3, 0x5140), hi23 = __byte_perm(q2, q3, 0x7362);
-  const uint32_t o[4] = {__byte_perm(lo01, lo23, 0x5410), __byte_perm(lo01, lo23, 0x7632),
-                         __byte_perm(hi01, hi23, 0x5410), __byte_perm(hi01, hi23, 0x7632)};
-  uint8_t* out = static_cast<uint8_t*>(a.out);
+    __syncthreads();
+    if (out) {
+      const uint32_t q0 = tile[4 * i][j], q1 = tile[4 * i + 1][j];
+      const uint32_t q2 = tile[4 * i + 2][j], q3 = tile[4 * i + 3][j];
+      const uint32_t lo01 = __byte_perm(q0, q1, 0x5140), hi01 = __byte_perm(q0, q1, 0x7362);
+      const uint32_t lo23 = __byte_perm(q2, q3, 0x5140), hi23 = __byte_perm(q2, q3, 0x7362);
+      const uint32_t o[4] = {__byte_perm(lo01, lo23, 0x5410), __byte_perm(lo01, lo23, 0x7632),
+                             __byte_perm(hi01, hi23, 0x5410), __byte_perm(hi01, hi23, 0x7632)};
 #pragma unroll
-  for (int b = 0; b < 4; ++b) {
-    const int64_t cc = cb + 4 * j + b;
-    if (cc >= a.c0 && cc < a.c1)
-      *reinterpret_cast<uint32_t*>(out + (cc - a.c0) * a.pitch + tb + 4 * i) = o[b];
+      for (int b = 0; b < 4; ++b) {
+        const int64_t cc = cb + 4 * j + b;
+        if (cc >= a.c0 && cc < a.c1)
+          *reinterpret_cast<uint32_t*>(out + (cc - a.c0) * a.pitch + tb + 4 * i) = o[b];
+      }
+    }
+    __syncthreads();  // the tile is refilled by the next sub-tile
   }
 }
 
@@ -507,6 +549,14 @@ void launch_iqrm_stats(const void* x, int nbits, int64_t nsamp, int64_t nchans, 
   DD_CUDA_TRY(cudaMemsetAsync(d_sums, 0, sizeof(unsigned long long) * 2 * csub * nwin, st));
   const int64_t chunk = 1024;
   dim3 grid(static_cast<unsigned>((csub + 255) / 256), static_cast<unsigned>((nsamp + chunk - 1) / chunk));
+  if (nbits == 8 && nchans % 4 == 0 && reinterpret_cast<uintptr_t>(x) % 4 == 0) {
+    const int64_t words = (csub + (cs & 3) + 3) / 4;
+    dim3 g4(static_cast<unsigned>((words + 255) / 256), grid.y);
+    k_iqrm_stats_u8w<<<g4, 256, 0, st>>>(static_cast<const uint8_t*>(x), nsamp, nchans, cs, csub,
+                                         d_win, nwin, chunk, d_sums);
+    DD_LAUNCHED();
+    return;
+  }
   switch (nbits) {
     case 8: k_iqrm_stats<uint8_t><<<grid, 256, 0, st>>>(static_cast<const uint8_t*>(x), nsamp, nchans, cs, csub, d_win, nwin, chunk, d_sums); break;
     case 16: k_iqrm_stats<uint16_t><<<grid, 256, 0, st>>>(static_cast<const uint16_t*>(x), nsamp, nchans, cs, csub, d_win, nwin, chunk, d_sums); break;
@@ -599,7 +649,8 @@ void launch_prep(const PrepArgs& a, cudaStream_t st) {
   if (a.out && !a.zdm_mean && a.nbits == 8 && a.ds == 1 && a.nchans % 4 == 0 && a.pitch % 4 == 0 &&
       reinterpret_cast<uintptr_t>(a.x) % 4 == 0 && reinterpret_cast<uintptr_t>(a.out) % 4 == 0) {
     const int64_t cw0 = a.c0 & ~int64_t(3);
-    dim3 grid(static_cast<unsigned>((a.nsamp + 63) / 64), static_cast<unsigned>((a.c1 - cw0 + 63) / 64));
+    const int64_t span = 64 * kPrepU8Subtiles;
+    dim3 grid(static_cast<unsigned>((a.nsamp + span - 1) / span), static_cast<unsigned>((a.c1 - cw0 + 63) / 64));
     k_prep_u8<<<grid, 256, 0, st>>>(a);
     DD_LAUNCHED();
   } else if (a.out && !a.zdm_mean && a.nbits == 16 && a.ds == 1 && a.nchans % 4 == 0 && a.pitch % 4 == 0 &&

@@ -804,7 +804,7 @@ __device__ __forceinline__ void run_one(const SumLaunch& L, uint3 blk, uint32_t*
   else if constexpr (KIND == kSumKindU8) sum_u8<kSumRowsPT, DD_SUM8_NW, false, false>(L, blk, sw, P);
   else if constexpr (KIND == kSumKindU16) sum_u16<kSumRows, DD_SUM16_NW>(L, blk, sw, P);
   else if constexpr (KIND == kSumKindU16Wide) sum_u16_wide<kSumRows, DD_SUM16W_NW>(L, blk, sw, P);
-  else if constexpr (KIND == kSumKindU16Quad) sum_u16_quad<kSumRowsPT, kSum16QNW>(L, blk, sw, P);
+  else if constexpr (KIND == kSumKindU16Quad) sum_u16_quad<kSumRowsPTQ, kSum16QNW>(L, blk, sw, P);
   else sum_u32<kSumRows, kSum32NW>(L, blk, sw, P);
 }
 
@@ -975,7 +975,7 @@ void launch_sum(const SumLaunch& L, cudaStream_t st) {
     case kSumKindU8: launch_k(k_sum_u8<kSumRowsPT, DD_SUM8_NW, false, false>, grid, smem, L, st); break;
     case kSumKindU16: launch_k(k_sum_u16<kSumRows, DD_SUM16_NW>, grid, smem, L, st); break;
     case kSumKindU16Wide: launch_k(k_sum_u16w<kSumRows, DD_SUM16W_NW>, grid, smem, L, st); break;
-    case kSumKindU16Quad: launch_k(k_sum_u16q<kSumRowsPT, kSum16QNW>, grid, smem, L, st); break;
+    case kSumKindU16Quad: launch_k(k_sum_u16q<kSumRowsPTQ, kSum16QNW>, grid, smem, L, st); break;
     default: launch_k(k_sum_u32<kSumRows, kSum32NW>, grid, smem, L, st); break;
   }
 }
