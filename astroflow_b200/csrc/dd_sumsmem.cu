@@ -119,6 +119,8 @@ __device__ __forceinline__ uint32_t madhi_u32(uint32_t a, uint32_t b, uint32_t c
 //     high word of (word - even) * 2^24 (FMA pipe), even lanes added by
 //     multiply-adds: one integer-pipe operation per word fewer than 0;
 //  2: as 1, with two sources' even lanes added by one three-input add.
+//  3: even lanes by mask (as 1), whole words summed as they are, top bytes summed
+//     by a multiply-high; the odd lanes are recovered once per output word.
 // Measured at the headline size (stage 1, ms): 0 -> 76.5, 1 -> 107, 2 -> 92; the
 // multiply-high chains cost more than the integer-pipe operations they save.
 #ifndef DD_SUM16Q_MINB
@@ -356,13 +358,33 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
   const uint32_t one = L.one;
   const uint32_t neg1 = 0u - one, sh24 = one << 24;  // runtime -1 and 2^24
   uint32_t ev[RB][NW], od[RB][NW];  // 16-bit lanes: samples (4w, 4w+2) and (4w+1, 4w+3)
+  // DD_SUM8_SPLIT 3: od holds the wrapping sum of whole words and hd the sum of
+  // their top bytes; the odd lanes are recovered at the end (see emit)
+  constexpr bool kWord = DD_SUM8_SPLIT == 3;
+  uint32_t hd[kWord ? RB : 1][kWord ? NW : 1];
+  const uint32_t sh8 = L.one << 8;  // 256, a runtime value: the multiply-high stays an IMAD
 #pragma unroll
   for (int r = 0; r < RB; ++r)
 #pragma unroll
-    for (int k = 0; k < NW; ++k) ev[r][k] = od[r][k] = 0;
+    for (int k = 0; k < NW; ++k) {
+      ev[r][k] = od[r][k] = 0;
+      if constexpr (kWord) hd[r][k] = 0;
+    }
   // Writes the lane sums of rows [0, nrows) to the output, adding them to the
   // partial sums an earlier flush stored there when `add`, and clears the lanes.
   auto emit = [&](bool add) {
+    if constexpr (kWord) {
+      // whole-word sum = E0 + 2^8 O1 + 2^16 E2 + 2^24 O3 (mod 2^32), with ev = E0 + 2^16 E2
+      // exact and hd = O3: O1 = (sum - ev - 2^24 O3) / 2^8 (O1 < 2^16, no wrap)
+#pragma unroll
+      for (int r = 0; r < RB; ++r)
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+          const uint32_t o1 = (od[r][k] - ev[r][k] - (hd[r][k] << 24)) >> 8;
+          od[r][k] = o1 | (hd[r][k] << 16);
+          hd[r][k] = 0;
+        }
+    }
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
       if (rbase + r >= g.nrows) break;
@@ -420,7 +442,12 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
                                    : __funnelshift_r(w0[32 * k], w0[32 * k + 1], rw.y);
         const uint32_t b = kConsec ? __funnelshift_r(vb[k], vb[k + 1], rw.w)
                                    : __funnelshift_r(w1[32 * k], w1[32 * k + 1], rw.w);
-        if constexpr (DD_SUM8_SPLIT == 1) {
+        if constexpr (kWord) {
+          ev[r][k] += (a & 0x00ff00ffu) + (b & 0x00ff00ffu);
+          od[r][k] += a + b;
+          hd[r][k] = madhi_u32(a, sh8, hd[r][k]);
+          hd[r][k] = madhi_u32(b, sh8, hd[r][k]);
+        } else if constexpr (DD_SUM8_SPLIT == 1) {
           const uint32_t ea = a & 0x00ff00ffu, eb = b & 0x00ff00ffu;
           ev[r][k] = mad_u32(ea, one, ev[r][k]);
           ev[r][k] = mad_u32(eb, one, ev[r][k]);
