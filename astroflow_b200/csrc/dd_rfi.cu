@@ -99,7 +99,8 @@ __global__ void k_iqrm_stats_u8w(const uint8_t* __restrict__ x, int64_t nsamp, i
     const int64_t b = win[2 * w + 1] < hi ? win[2 * w + 1] : hi;
     if (a >= b) continue;
     uint32_t s[4] = {0u, 0u, 0u, 0u}, q[4] = {0u, 0u, 0u, 0u};
-    for (int64_t t = a; t < b; ++t) {
+#pragma unroll 8
+    for (int64_t t = a; t < b; ++t) {  // unrolled: eight rows' loads in flight
       const uint32_t v = __ldg(reinterpret_cast<const uint32_t*>(x + t * nchans + c4));
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
@@ -392,15 +393,28 @@ __global__ void __launch_bounds__(256) k_prep_u8(PrepArgs a) {
   }
   const int i = threadIdx.x & 15;  // store phase: samples 4i .. 4i+3
   const int j = threadIdx.x >> 4;  // channel word j: channels 4j .. 4j+3
+  const int r0 = threadIdx.x >> 4;  // load phase: rows r0, r0 + 16, r0 + 32, r0 + 48
   uint8_t* out = static_cast<uint8_t*>(a.out);
+  const int64_t tile0 = static_cast<int64_t>(blockIdx.x) * kPrepU8Subtiles * 64;
+  // the raw words of sub-tile `sub` (loads only; masks applied when staged)
+  auto fetch = [&](int sub, uint32_t (&v)[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int64_t t = tile0 + sub * 64 + r0 + 16 * k;
+      v[k] = (cvalid && t < a.nsamp) ? __ldg(reinterpret_cast<const uint32_t*>(x + t * a.nchans + c)) : 0u;
+    }
+  };
+  uint32_t cur[4], nxt[4];
+  fetch(0, cur);
   for (int sub = 0; sub < kPrepU8Subtiles; ++sub) {
-    const int64_t tb = (static_cast<int64_t>(blockIdx.x) * kPrepU8Subtiles + sub) * 64;
+    const int64_t tb = tile0 + sub * 64;
     if (tb >= a.nsamp) break;
-    for (int r = threadIdx.x >> 4; r < 64; r += 16) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int r = r0 + 16 * k;
       const int64_t t = tb + r;
-      uint32_t v = 0;
+      uint32_t v = cur[k];
       if (cvalid && t < a.nsamp) {
-        v = *reinterpret_cast<const uint32_t*>(x + t * a.nchans + c);
         if (a.segmask) {
           const int sg = find_seg(a.seg_t0, a.nseg, t);
           const uint32_t m = *reinterpret_cast<const uint32_t*>(
@@ -416,6 +430,7 @@ __global__ void __launch_bounds__(256) k_prep_u8(PrepArgs a) {
       tile[r][w] = v;
     }
     __syncthreads();
+    if (sub + 1 < kPrepU8Subtiles) fetch(sub + 1, nxt);  // in flight during the stores
     if (out) {
       const uint32_t q0 = tile[4 * i][j], q1 = tile[4 * i + 1][j];
       const uint32_t q2 = tile[4 * i + 2][j], q3 = tile[4 * i + 3][j];
@@ -431,6 +446,8 @@ __global__ void __launch_bounds__(256) k_prep_u8(PrepArgs a) {
       }
     }
     __syncthreads();  // the tile is refilled by the next sub-tile
+#pragma unroll
+    for (int k = 0; k < 4; ++k) cur[k] = nxt[k];
   }
 }
 

@@ -641,6 +641,10 @@ EXTRAS = [
                                             "--steps", "2", "--warmup", "1", "--no-autotune"]),
     ("batched-256-short-subband32", ["--workload", "batched-256-short-subband32",
                                      "--steps", "3", "--warmup", "1", "--no-autotune"]),
+    ("large-8192ch-u16-2^21-multirange-subband64-rfi", ["--workload",
+                                                       "large-8192ch-u16-2^21-multirange-subband64-rfi",
+                                                       "--steps", "3", "--warmup", "3",
+                                                       "--e2e-steps", "1"]),
     ("serving-19beams-4096ch-u8-3001dm-files", ["--workload",
                                                 "serving-19beams-4096ch-u8-3001dm-files",
                                                 "--steps", "10", "--warmup", "3"]),
