@@ -406,6 +406,8 @@ __global__ void __launch_bounds__(256) k_prep_u8(PrepArgs a) {
   };
   uint32_t cur[4], nxt[4];
   fetch(0, cur);
+  int seg = -1;          // IQRM segment whose mask word is cached in seg_keep
+  uint32_t seg_keep = ~0u;
   for (int sub = 0; sub < kPrepU8Subtiles; ++sub) {
     const int64_t tb = tile0 + sub * 64;
     if (tb >= a.nsamp) break;
@@ -417,9 +419,13 @@ __global__ void __launch_bounds__(256) k_prep_u8(PrepArgs a) {
       if (cvalid && t < a.nsamp) {
         if (a.segmask) {
           const int sg = find_seg(a.seg_t0, a.nseg, t);
-          const uint32_t m = *reinterpret_cast<const uint32_t*>(
-              a.segmask + static_cast<int64_t>(sg) * a.nchans + c);
-          v &= ~__vcmpne4(m, 0u);
+          if (sg != seg) {  // segments span many rows: the mask word changes rarely
+            seg = sg;
+            seg_keep = ~__vcmpne4(*reinterpret_cast<const uint32_t*>(
+                                      a.segmask + static_cast<int64_t>(sg) * a.nchans + c),
+                                  0u);
+          }
+          v &= seg_keep;
         }
         if (a.zdm_off) {
           const uint32_t m = min(a.zdm_off[t], 255u) * 0x01010101u;
