@@ -650,8 +650,8 @@ EXTRAS = [
                                                 "--steps", "10", "--warmup", "3"]),
 ]
 EXTRA_KEYS = ("impl", "value", "unit", "ms_per_step", "steps", "warmup", "e2e", "cpu_baseline",
-              "batched_over_plain", "forms", "latency", "clocks", "gpu_launches", "unavailable",
-              "reference_timers_ms", "files", "chunks")
+              "batched_over_plain", "forms", "serving", "clocks", "gpu_launches", "unavailable",
+              "reference_timers_ms")
 
 
 def run_extras(dev):
