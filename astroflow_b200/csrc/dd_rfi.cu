@@ -396,12 +396,24 @@ __global__ void __launch_bounds__(256) k_prep_u8(PrepArgs a) {
   const int r0 = threadIdx.x >> 4;  // load phase: rows r0, r0 + 16, r0 + 32, r0 + 48
   uint8_t* out = static_cast<uint8_t*>(a.out);
   const int64_t tile0 = static_cast<int64_t>(blockIdx.x) * kPrepU8Subtiles * 64;
+  // this thread's source word in row tile0 + r0, and the stride of 16 rows
+  const uint8_t* src = x + (tile0 + r0) * a.nchans + c;
+  const int64_t step16 = 16 * a.nchans;
+  // this thread's four output rows (channels 4j .. 4j+3) at sample tile0 + 4i
+  uint8_t* dst[4];
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int64_t cc = cb + 4 * j + b;
+    dst[b] = (out && cc >= a.c0 && cc < a.c1) ? out + (cc - a.c0) * a.pitch + tile0 + 4 * i : nullptr;
+  }
   // the raw words of sub-tile `sub` (loads only; masks applied when staged)
   auto fetch = [&](int sub, uint32_t (&v)[4]) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int64_t t = tile0 + sub * 64 + r0 + 16 * k;
-      v[k] = (cvalid && t < a.nsamp) ? __ldg(reinterpret_cast<const uint32_t*>(x + t * a.nchans + c)) : 0u;
+      v[k] = (cvalid && t < a.nsamp)
+                 ? __ldg(reinterpret_cast<const uint32_t*>(src + (4 * sub + k) * step16))
+                 : 0u;
     }
   };
   uint32_t cur[4], nxt[4];
@@ -445,11 +457,8 @@ __global__ void __launch_bounds__(256) k_prep_u8(PrepArgs a) {
       const uint32_t o[4] = {__byte_perm(lo01, lo23, 0x5410), __byte_perm(lo01, lo23, 0x7632),
                              __byte_perm(hi01, hi23, 0x5410), __byte_perm(hi01, hi23, 0x7632)};
 #pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int64_t cc = cb + 4 * j + b;
-        if (cc >= a.c0 && cc < a.c1)
-          *reinterpret_cast<uint32_t*>(out + (cc - a.c0) * a.pitch + tb + 4 * i) = o[b];
-      }
+      for (int b = 0; b < 4; ++b)
+        if (dst[b]) *reinterpret_cast<uint32_t*>(dst[b] + sub * 64) = o[b];
     }
     __syncthreads();  // the tile is refilled by the next sub-tile
 #pragma unroll

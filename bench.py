@@ -635,12 +635,11 @@ def reference_gpu_arm(args, wl, spec, hdr, config, dist, dev):
 EXTRAS = [
     # (key, bench.py arguments): short runs, each in its own process on this GPU
     ("reference-gpu", ["--impl", "reference-gpu", "--steps", "2", "--warmup", "1"]),
+    # (the 256-short-chunk batch workload runs on request: --workload batched-256-short-subband32)
     ("plain-1024ch-u8-2^17-1001dm-brute", ["--workload", "plain-1024ch-u8-2^17-1001dm-brute",
                                            "--steps", "10", "--warmup", "3", "--e2e-steps", "2"]),
     ("batched-64-heterogeneous-subband32", ["--workload", "batched-64-heterogeneous-subband32",
                                             "--steps", "2", "--warmup", "1", "--no-autotune"]),
-    ("batched-256-short-subband32", ["--workload", "batched-256-short-subband32",
-                                     "--steps", "3", "--warmup", "1", "--no-autotune"]),
     ("large-8192ch-u16-2^21-multirange-subband64-rfi", ["--workload",
                                                        "large-8192ch-u16-2^21-multirange-subband64-rfi",
                                                        "--steps", "3", "--warmup", "3",
