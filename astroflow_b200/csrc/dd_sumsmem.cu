@@ -9,11 +9,12 @@
 // [base + min_r off, base + max_r off + T), is brought into shared memory by one
 // bulk asynchronous copy (cp.async.bulk, completion counted in bytes on an
 // mbarrier); up to `stages` source pairs are in flight in a ring of buffers.
-// Lanes 0-1 of warp 0 act as the producer: before summing pair p they refill
-// the buffer pair p-1 used with pair p+stages-1, once every warp has released it
-// (an "empty" mbarrier with one arrival per warp).  The window bounds and each
-// row's offset inside its window come from descriptors precomputed on the host
-// (SumDesc), so the producer does no per-row work beyond unpacking them.
+// Warp 0 acts as the producer: before summing pair p it refills the buffer pair
+// p-1 used with pair p+stages-1, once every warp has released it (an "empty"
+// mbarrier with one arrival per warp).  The window bounds and each row's offset
+// inside its window come from descriptors precomputed on the host (SumDesc),
+// which reach shared memory by bulk copies of 32 sources, a chunk ahead, so the
+// producer only unpacks them (one lane per source and row).
 //
 // Summing: lanes own interleaved 32-bit output words (lane l: words l, l+32, ...),
 // so each shared load touches 32 consecutive words, free of bank conflicts; a
@@ -32,6 +33,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstdint>
 #include <vector>
 
@@ -197,60 +199,89 @@ __device__ __forceinline__ Geo make_geo(const SumLaunch& L, int T, uint3 blk) {
   return g;
 }
 
+// Source descriptors come into shared memory in chunks of kDescChunk sources by
+// bulk copies, two chunks in flight, so that the producer never waits on a
+// global load between two stages.
+constexpr int kDescChunk = 32;
+
 // Shared state of the pipeline.  A stage holds QS (2 or 4) source windows.
 struct __align__(16) Pipe {
   uint64_t full[kMaxStages];   // completes when a stage's windows have landed
   uint64_t empty[kMaxStages];  // completes when all warps released a stage
+  SumDesc desc[2][kDescChunk]; // descriptors of chunks k (half k & 1)
+  uint64_t dfull[2];           // completes when a half's chunk has landed
   // per row: word index and shift (bits) of sample 0 in the window of source
   // i of the stage at [2i], [2i+1]
   int row[kMaxStages][kSumRows][8];
   int failed;
 };
+static_assert(offsetof(Pipe, desc) % 16 == 0, "bulk copies land on 16-byte boundaries");
+
+// Bulk copy of descriptor chunk k of the block's sources into half k & 1.
+__device__ __forceinline__ void fetch_desc(const Geo& g, Pipe& P, int k) {
+  const int n = min(kDescChunk, g.nsrc - k * kDescChunk);
+  const uint32_t bytes = static_cast<uint32_t>(n * sizeof(SumDesc));
+  mbar_arrive_expect_tx(&P.dfull[k & 1], bytes);
+  bulk_copy(&P.desc[k & 1][0], g.desc + static_cast<int64_t>(k) * kDescChunk, bytes,
+            &P.dfull[k & 1]);
+}
 __device__ __forceinline__ int4 row_pair(const Pipe& P, int s, int r, int half) {
   return *reinterpret_cast<const int4*>(&P.row[s][r][4 * half]);
 }
 
-// Producer step for source group q in stage s (warp 0, lanes 0..QS-1; lane l
-// handles source QS*q + l).  The caller has made sure stage s is free.
+// Producer step for source group q in stage s, by all lanes of warp 0: lane
+// 8i + r writes row r's offsets into the window of source QS*q + i, and lane 8i
+// issues that window's copy.  The caller has made sure stage s is free.  False
+// when the wait for the group's descriptors gave up.
 template <int SB, int QS>
-__device__ __forceinline__ void produce(const Geo& g, Pipe& P, uint32_t* sw, int ww, int zero_q,
-                                        int tile_bytes, int q, int s, int lane) {
-  const int src = QS * q + lane;
-  uint32_t nbytes = 0;
-  const char* gsrc = nullptr;
-  uint32_t* dst = sw + (QS * s + lane) * ww;
-  if (lane < QS) {
-    int* rw = &P.row[s][0][0] + 2 * lane;
-    if (src < g.nsrc) {
-      const SumDesc d = g.desc[src];
-      const int64_t first = (g.base + d.lo) * SB;
-      const int64_t a0 = first & ~int64_t(15);
-      const int64_t last = (g.base + d.lo + d.span) * SB + tile_bytes + 8;  // + funnel word
-      nbytes = static_cast<uint32_t>((last - a0 + 15) & ~int64_t(15));
-      gsrc = g.src + static_cast<int64_t>(src) * g.src_pitch + a0;
-      const int qbase = (QS * s + lane) * ww;
-      const int ob0 = static_cast<int>(first - a0);
-#pragma unroll
-      for (int r = 0; r < kSumRows; ++r) {
-        // rows past nrows take offset lo (rel 0): their reads stay in the window
-        const int ob = ob0 + (r < g.nrows ? static_cast<int>(d.rel[r]) : 0) * SB;
-        rw[8 * r] = qbase + (ob >> 2);
-        rw[8 * r + 1] = (ob & 3) * 8;
-      }
-    } else {
-#pragma unroll
-      for (int r = 0; r < kSumRows; ++r) {
-        rw[8 * r] = zero_q;
-        rw[8 * r + 1] = 0;
-      }
+__device__ __forceinline__ bool produce(const Geo& g, Pipe& P, uint32_t* sw, int ww, int zero_q,
+                                        int tile_bytes, int q, int s, int lane,
+                                        volatile int* failed, volatile int* gerr) {
+  static_assert(kSumRows == 8 && kDescChunk % QS == 0, "lane = 8 * source + row");
+  const int first = QS * q;
+  const int chunk = first / kDescChunk;
+  if (first % kDescChunk == 0) {
+    // the group opens a chunk: wait for its descriptors, then refill the other
+    // half (the previous chunk, read by this warp only) with the next chunk
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(&P.dfull[chunk & 1], (chunk >> 1) & 1,
+                                                      failed, gerr));
+    if (!ok) return false;
+    if (lane == 0 && chunk >= 1 && (chunk + 1) * kDescChunk < g.nsrc) {
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      fetch_desc(g, P, chunk + 1);
     }
   }
-  uint32_t total = nbytes + __shfl_xor_sync(0xffffffffu, nbytes, 1);
-  if (QS == 4) total += __shfl_xor_sync(0xffffffffu, total, 2);
+  const int i = lane >> 3, r = lane & 7;
+  const int src = first + i;
+  uint32_t nbytes = 0;
+  const char* gsrc = nullptr;
+  if (i < QS) {
+    int* rw = &P.row[s][r][2 * i];
+    if (src < g.nsrc) {
+      const SumDesc& d = P.desc[chunk & 1][src % kDescChunk];
+      const int64_t firstb = (g.base + d.lo) * SB;
+      const int64_t a0 = firstb & ~int64_t(15);
+      // rows past nrows take offset lo (rel 0): their reads stay in the window
+      const int ob = static_cast<int>(firstb - a0) + (r < g.nrows ? static_cast<int>(d.rel[r]) : 0) * SB;
+      rw[0] = (QS * s + i) * ww + (ob >> 2);
+      rw[1] = (ob & 3) * 8;
+      if (r == 0) {
+        const int64_t last = (g.base + d.lo + d.span) * SB + tile_bytes + 8;  // + funnel word
+        nbytes = static_cast<uint32_t>((last - a0 + 15) & ~int64_t(15));
+        gsrc = g.src + static_cast<int64_t>(src) * g.src_pitch + a0;
+      }
+    } else {
+      rw[0] = zero_q;
+      rw[1] = 0;
+    }
+  }
+  uint32_t total = nbytes + __shfl_xor_sync(0xffffffffu, nbytes, 8);
+  if (QS == 4) total += __shfl_xor_sync(0xffffffffu, total, 16);
   __syncwarp();
   if (lane == 0) mbar_arrive_expect_tx(&P.full[s], total);
   __syncwarp();
-  if (lane < QS && nbytes) bulk_copy(dst, gsrc, nbytes, &P.full[s]);
+  if (nbytes) bulk_copy(sw + (QS * s + i) * ww, gsrc, nbytes, &P.full[s]);
+  return true;
 }
 
 // Pipeline driver shared by the kernels: calls body(stage, cur) for every
@@ -263,43 +294,59 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
   const int S = L.stages;
   const int zero_q = QS * S * ww;
   const int npairs = (g.nsrc + QS - 1) / QS;
+  const int nchunks = (g.nsrc + kDescChunk - 1) / kDescChunk;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&P.full[s], 1);
       mbar_init(&P.empty[s], kWarps);
     }
+    mbar_init(&P.dfull[0], 1);
+    mbar_init(&P.dfull[1], 1);
     P.failed = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     // order earlier generic accesses to the windows (a previous task of a
     // persistent block) before the bulk copies that refill them
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    fetch_desc(g, P, 0);
+    if (nchunks > 1) fetch_desc(g, P, 1);
   }
   for (int i = threadIdx.x; i < ww; i += kThreads) sw[zero_q + i] = 0u;
   __syncthreads();
   volatile int* failed = &P.failed;
   int issued = 0;  // pairs whose copies warp 0 has issued
+  bool prod_ok = true;
   if (warp == 0)
     for (; issued < min(S - 1, npairs); ++issued)
-      produce<SB, QS>(g, P, sw, ww, zero_q, tile_bytes, issued, issued, lane);
+      if (!(prod_ok = produce<SB, QS>(g, P, sw, ww, zero_q, tile_bytes, issued, issued, lane,
+                                      failed, L.err)))
+        break;
+  if (!prod_ok && lane == 0) {
+    if (!*failed) atomicCAS(L.err, 0, kErrWaitFull);
+    *failed = 1;
+  }
   int s_cur = 0, p = 0;
   uint32_t ph_cur = 0;
-  for (; p < npairs; ++p) {
+  for (; prod_ok && p < npairs; ++p) {
     if (warp == 0 && issued < npairs) {
       const int q = issued;  // == p + S - 1: refills the stage pair p-1 used
       const int s = q % S;
       bool ok = true;
+      int code = kErrWaitEmpty;
       if (q >= S) {
         if (lane == 0) ok = mbar_wait(&P.empty[s], ((q / S) - 1) & 1, failed, L.err);
         ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       }
+      if (ok) {
+        ok = produce<SB, QS>(g, P, sw, ww, zero_q, tile_bytes, q, s, lane, failed, L.err);
+        code = kErrWaitFull;
+      }
       if (!ok) {
         if (lane == 0) {
-          if (!*failed) atomicCAS(L.err, 0, kErrWaitEmpty);
+          if (!*failed) atomicCAS(L.err, 0, code);
           *failed = 1;
         }
         break;
       }
-      produce<SB, QS>(g, P, sw, ww, zero_q, tile_bytes, q, s, lane);
       ++issued;
     }
     const bool ok = mbar_wait(&P.full[s_cur], ph_cur, failed, L.err);
@@ -325,6 +372,15 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
       while (!mbar_try_wait(&P.full[q % S], (q / S) & 1) && clock64() - t0 < kWaitCycles) {
       }
     }
+    // descriptor chunks: 0 and 1 at the start, k + 1 once chunk k >= 1 was
+    // waited for; the chunks up to that of the last issued group were waited for
+    const int opened = issued > 0 ? (QS * (issued - 1)) / kDescChunk : -1;
+    const int last = min(nchunks - 1, max(1, opened + 1));
+    for (int k = opened + 1; k <= last; ++k) {
+      const long long t0 = clock64();
+      while (!mbar_try_wait(&P.dfull[k & 1], (k >> 1) & 1) && clock64() - t0 < kWaitCycles) {
+      }
+    }
   }
   // every phase has completed: retire the barriers so the next task of a
   // persistent block can initialise them again
@@ -334,6 +390,8 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
       asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_addr(&P.full[st])) : "memory");
       asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_addr(&P.empty[st])) : "memory");
     }
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_addr(&P.dfull[0])) : "memory");
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_addr(&P.dfull[1])) : "memory");
   }
 }
 
