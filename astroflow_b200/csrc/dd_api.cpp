@@ -61,8 +61,18 @@ bool stage1_flush(const dd_plan& P) {
 
 // ---- frequency table and band (dedispered.cu:1003-1031, cpucal.hpp:85-116)
 // Kernel variant of stage 2: 16-bit subband sums (8-bit input, subbands of at
-// most 64 channels) four per pipeline stage, else 32-bit sums.
-int stage2_kind(const dd_plan& P) { return P.inter16 ? kSumKindU16Quad : kSumKindU32; }
+// most 64 channels) four per pipeline stage, read from the sums and their
+// shifted twin when stage 1 writes one, else 32-bit sums.
+int stage2_kind(const dd_plan& P) {
+  return P.inter16 ? (P.twin ? kSumKindU16Twin : kSumKindU16Quad) : kSumKindU32;
+}
+#ifndef DD_PAIR_STAGES
+#define DD_PAIR_STAGES 0
+#endif
+// Byte offset from a subband-sum buffer to its twin (0: no twin).
+int64_t twin_offset(const dd_plan& P) {
+  return P.twin ? (DD_PAIR_STAGES ? 2 : 1) * P.inter_bytes : 0;
+}
 
 void build_freq(dd_plan& P) {
   const int n = P.hdr.nchans;
@@ -307,9 +317,6 @@ void upload(DevBuf& b, const void* h, size_t bytes) {
 #ifndef DD_INTER_MB
 #define DD_INTER_MB 2048
 #endif
-#ifndef DD_PAIR_STAGES
-#define DD_PAIR_STAGES 0
-#endif
 // Time tiling of the subband path for a subband-sum budget (bytes per tile): the
 // tile length, the pitches, and the prepared-input and subband-sum buffers
 // (reallocated, zeroed).  Results do not depend on the tiling.
@@ -320,7 +327,7 @@ void set_tiling(dd_plan& P, int64_t budget) {
   // whole stage-1 block tiles T1: L = n*T1 - R with R the halo rounded to the
   // base tile; n grows while one tile of subband sums stays within the budget and
   // the tile is not longer than the chunk.
-  const int64_t per_col = P.ndm_nom * P.nsb * inter_elem(P);
+  const int64_t per_col = P.ndm_nom * P.nsb * inter_elem(P) * (P.twin ? 2 : 1);
   const int64_t T1 = P.win1 ? sum_variant_tile(P.elem, stage1_flush(P)) : kT;
   const int64_t R = round_up(std::max<int64_t>(P.max_res, 1), kT);
   int64_t n = 1;
@@ -338,7 +345,8 @@ void set_tiling(dd_plan& P, int64_t budget) {
   P.d_x.alloc(static_cast<size_t>(P.dch * P.xpitch) * P.elem);
   DD_CUDA_TRY(cudaMemsetAsync(P.d_x.p, 0, P.d_x.bytes, cudaStreamLegacy));
   P.inter_bytes = P.ndm_nom * P.nsb * P.tile_pitch * inter_elem(P);
-  P.d_inter.alloc(static_cast<size_t>((DD_PAIR_STAGES ? 2 : 1) * P.inter_bytes));
+  // (+256: the twin's staged windows may start one 16-byte block past the sums')
+  P.d_inter.alloc(static_cast<size_t>((DD_PAIR_STAGES ? 2 : 1) * (P.twin ? 2 : 1) * P.inter_bytes) + 256);
   DD_CUDA_TRY(cudaMemsetAsync(P.d_inter.p, 0, P.d_inter.bytes, cudaStreamLegacy));
   DD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
 }
@@ -407,6 +415,8 @@ void create_subband(dd_plan& P) {
     const int T1 = sum_variant_tile(P.elem, stage1_flush(P));
     P.win1 = window_bytes(table_spread(P.h_delay, P.ndm_nom, P.dch, kSumRows, 0), T1, P.elem);
   }
+  // the twin needs the staged stage 1 (which writes it) and the staged stage 2
+  P.twin = (P.inter16 && P.win1 && DD_SUM16_TWIN) ? 1 : 0;
   if (P.nbits <= 16) {
     // stage-2 sources: the stage-1 sums (uint16 or uint32)
     const int e2 = static_cast<int>(inter_elem(P));
@@ -414,6 +424,7 @@ void create_subband(dd_plan& P) {
     P.win2 = window_bytes(table_spread(P.h_res, P.dm_steps, P.nsb, kSumRows, P.ndm0), T2, e2,
                           sum_kind_qs(stage2_kind(P)));
   }
+  if (!P.win2) P.twin = 0;
   if (P.win1) upload_desc(P.d_desc1, build_sum_desc(P.h_delay, P.ndm_nom, P.dch, 0));
   if (P.win2) upload_desc(P.d_desc2, build_sum_desc(P.h_res, P.dm_steps, P.nsb, P.ndm0));
   set_tiling(P, int64_t(DD_INTER_MB) << 20);
@@ -619,6 +630,7 @@ SumLaunch stage1_launch(const dd_plan& P, int64_t t0, int buf = 0) {
   L.stages = P.stages_override ? P.stages_override : sum_stages(P.win1);
   L.err = P.d_err.as<int>();
   L.one = 1;
+  L.twin_off = twin_offset(P);
   return L;
 }
 
@@ -650,6 +662,7 @@ SumLaunch stage2_launch(const dd_plan& P, int64_t t0, void* output, int buf = 0)
   L.stages = P.stages_override ? P.stages_override : sum_stages(P.win2, sum_kind_qs(stage2_kind(P)));
   L.err = P.d_err.as<int>();
   L.one = 1;
+  L.twin_off = twin_offset(P);
   return L;
 }
 

@@ -77,6 +77,7 @@ struct dd_plan {
   int sbw = 32, ndm0 = 32;
   int max_delay = 0, max_res = 0;
   int inter16 = 0;           // stage-1 sums stored as uint16 (8-bit input, narrow subbands)
+  int twin = 0;              // stage 1 also writes the one-sample-shifted twin of its uint16 sums
   int64_t tile = 0;          // time tile of the stage-1 -> stage-2 pipeline
   int64_t tile_pitch = 0;    // row pitch of the inter tile (elements)
   int64_t xpitch = 0;        // row pitch of the channel-major prepared input (elements)
@@ -295,6 +296,11 @@ struct SumLaunch {
   int stages;              // staged source pairs in flight (2..4)
   int* err;                // device error word: set when a bounded wait gives up
   unsigned one;            // 1 (a multiplier the compiler cannot fold)
+  // 16-bit subband sums with a one-sample-shifted twin (0: none): the twin of the
+  // element at byte address a sits at a + twin_off and holds the element before
+  // it, twin[i] = sums[i - 1].  Stage 1 writes both; stage 2 reads a source whose
+  // offset is odd from the twin, so every read is a whole aligned word.
+  int64_t twin_off;
 };
 #ifndef DD_SUM_MAX_STAGES
 #define DD_SUM_MAX_STAGES 8
@@ -349,6 +355,25 @@ constexpr int kSum32NW = DD_SUM32_NW;  // words per lane of the 32-bit staged su
 #define DD_SUM16Q_NW 9
 #endif
 constexpr int kSum16QNW = DD_SUM16Q_NW;
+// Stage 2 on 16-bit sums with a shifted twin (k_sum_u16t): words per lane (lanes
+// own interleaved words, so any count is conflict-free) and warp groups the
+// block's rows are split over.
+#ifndef DD_SUM16T_NW
+#define DD_SUM16T_NW 6
+#endif
+#ifndef DD_SUM16T_ROWSPLIT
+#define DD_SUM16T_ROWSPLIT 2
+#endif
+constexpr int kSum16TNW = DD_SUM16T_NW;
+constexpr int kSumRowsPTT = kSumRows / DD_SUM16T_ROWSPLIT;
+// Stage 2 of 8-bit input reads a twin of the subband sums (1) or aligns odd
+// offsets with byte permutes (0, the quad kernel).  Measured at the headline
+// size (ms, stage 1 / stage 2 / step): quad 69.3 / 46.8 / 120.6; twin with the
+// stage-1 twin stored lane by lane 81.2 / 36.6 / 122.1; twin stored in 16-byte
+// chunks through shared memory 71.1 / 36.6 / 112.0.
+#ifndef DD_SUM16_TWIN
+#define DD_SUM16_TWIN 1
+#endif
 // flush: 8-bit lanes added into the output every 256 sources; 16-bit sources summed into
 // 32-bit lanes (the k_sum_u16w variant).
 inline int sum_variant_tile(int src_bytes, bool flush) {
@@ -361,8 +386,8 @@ inline int sum_kind_tile(int kind);
 // Kernel variant of a staged sum: 8-bit sources into 16-bit sums, 8-bit sources
 // widened to 32 bits (many sources), 8-bit, 16-bit and 32-bit sources.
 enum SumKind { kSumKindU8Out16 = 0, kSumKindU8Flush = 1, kSumKindU8 = 2, kSumKindU16 = 3,
-               kSumKindU32 = 4, kSumKindU16Wide = 5, kSumKindU16Quad = 6 };
-constexpr int kSumKinds = 7;
+               kSumKindU32 = 4, kSumKindU16Wide = 5, kSumKindU16Quad = 6, kSumKindU16Twin = 7 };
+constexpr int kSumKinds = 8;
 int sum_kind(const SumLaunch& L);
 inline int sum_kind_tile(int kind) {
   switch (kind) {
@@ -371,11 +396,15 @@ inline int sum_kind_tile(int kind) {
     case kSumKindU16: return sum_tile_samples(2, DD_SUM16_NW);
     case kSumKindU16Wide: return sum_tile_samples(2, DD_SUM16W_NW);
     case kSumKindU16Quad: return sum_tile_samples(2, kSum16QNW) / DD_SUM16Q_ROWSPLIT;
+    case kSumKindU16Twin: return sum_tile_samples(2, kSum16TNW) / DD_SUM16T_ROWSPLIT;
     default: return sum_tile_samples(4, kSum32NW);
   }
 }
-// Source windows per pipeline stage of a kernel variant (4 for kSumKindU16Quad, else 2).
-inline int sum_kind_qs(int kind) { return kind == kSumKindU16Quad ? 4 : 2; }
+// Source windows per pipeline stage of a kernel variant: 4 for kSumKindU16Quad, 8
+// for kSumKindU16Twin (four sources, each with its twin), else 2.
+inline int sum_kind_qs(int kind) {
+  return kind == kSumKindU16Quad ? 4 : kind == kSumKindU16Twin ? 8 : 2;
+}
 // Shared memory of a launch (its variant's windows per stage).
 size_t sum_launch_smem(const SumLaunch& L);
 // Stage 1 of one tile and stage 2 of another in one launch (false: no paired

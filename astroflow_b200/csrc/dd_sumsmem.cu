@@ -125,6 +125,11 @@ __device__ __forceinline__ uint32_t madhi_u32(uint32_t a, uint32_t b, uint32_t c
 //     by a multiply-high; the odd lanes are recovered once per output word.
 // Measured at the headline size (stage 1, ms): 0 -> 76.5, 1 -> 107, 2 -> 92; the
 // multiply-high chains cost more than the integer-pipe operations they save.
+// 16-bit stage-1 sums leave through shared memory as 16-byte chunks (1) or as
+// each lane's words (0).
+#ifndef DD_SUM8_STAGED_OUT
+#define DD_SUM8_STAGED_OUT 1
+#endif
 #ifndef DD_SUM16Q_MINB
 #define DD_SUM16Q_MINB 2
 #endif
@@ -284,15 +289,81 @@ __device__ __forceinline__ bool produce(const Geo& g, Pipe& P, uint32_t* sw, int
   return true;
 }
 
+// Producer step of the twin-window sums (16-bit sources with a one-sample-shifted
+// twin, twin[i] = sums[i - 1], four sources per stage): each source is staged
+// twice, the sums and the twin, each from the 16-byte boundary at or below the
+// first element the block's rows read there, and lane 8i + r points row r of
+// source 4q + i into the copy in which its first element starts a 32-bit word:
+// an even element index e at byte 2e of the sums, an odd one at byte 2(e + 1)
+// of the twin.  Lane 8i issues both copies.
+__device__ __forceinline__ bool produce_twin(const Geo& g, Pipe& P, uint32_t* sw, int ww, int zero_q,
+                                             int tile_bytes, int64_t twin_off, int q, int s,
+                                             int lane, volatile int* failed, volatile int* gerr) {
+  constexpr int QS = 4;
+  static_assert(kSumRows == 8 && kDescChunk % QS == 0, "lane = 8 * source + row");
+  const int first = QS * q;
+  const int chunk = first / kDescChunk;
+  if (first % kDescChunk == 0) {
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(&P.dfull[chunk & 1], (chunk >> 1) & 1,
+                                                      failed, gerr));
+    if (!ok) return false;
+    if (lane == 0 && chunk >= 1 && (chunk + 1) * kDescChunk < g.nsrc) {
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      fetch_desc(g, P, chunk + 1);
+    }
+  }
+  const int i = lane >> 3, r = lane & 7;
+  const int src = first + i;
+  const int win0 = 2 * (QS * s + i) * ww;  // the sums; the twin follows at win0 + ww
+  uint32_t n0 = 0, n1 = 0;
+  const char *c0 = nullptr, *c1 = nullptr;
+  int* rw = &P.row[s][r][2 * i];
+  if (src < g.nsrc) {
+    const SumDesc& d = P.desc[chunk & 1][src % kDescChunk];
+    const int64_t e0 = g.base + d.lo;  // first element any row of the block reads
+    // element e sits at byte 2e of the sums and at byte 2(e + 1) of the twin
+    const int64_t a0 = (2 * e0) & ~int64_t(15);
+    const int64_t a1 = (2 * (e0 + 1)) & ~int64_t(15);
+    // rows past nrows take offset lo (rel 0): their reads stay in the windows
+    const int64_t o = e0 + (r < g.nrows ? static_cast<int64_t>(d.rel[r]) : 0);
+    rw[0] = (o & 1) ? win0 + ww + static_cast<int>((2 * (o + 1) - a1) >> 2)
+                    : win0 + static_cast<int>((2 * o - a0) >> 2);
+    rw[1] = 0;
+    if (r == 0) {
+      const int64_t last = 2 * (e0 + d.span) + tile_bytes;  // past the last byte any row reads
+      n0 = static_cast<uint32_t>((last - a0 + 15) & ~int64_t(15));
+      n1 = static_cast<uint32_t>((last + 2 - a1 + 15) & ~int64_t(15));
+      c0 = g.src + static_cast<int64_t>(src) * g.src_pitch + a0;
+      c1 = g.src + static_cast<int64_t>(src) * g.src_pitch + twin_off + a1;
+    }
+  } else {
+    rw[0] = zero_q;
+    rw[1] = 0;
+  }
+  uint32_t total = n0 + n1;
+  total += __shfl_xor_sync(0xffffffffu, total, 8);
+  total += __shfl_xor_sync(0xffffffffu, total, 16);
+  __syncwarp();
+  if (lane == 0) mbar_arrive_expect_tx(&P.full[s], total);
+  __syncwarp();
+  if (n0) {
+    bulk_copy(sw + win0, c0, n0, &P.full[s]);
+    bulk_copy(sw + win0 + ww, c1, n1, &P.full[s]);
+  }
+  return true;
+}
+
 // Pipeline driver shared by the kernels: calls body(stage, cur) for every
-// group of QS sources once their windows are in shared memory.
-template <int SB, int QS = 2, typename Body>
+// group of QS sources once their windows are in shared memory (TWIN: each
+// source is staged with its shifted twin, see produce_twin; QS is 4).
+template <int SB, int QS = 2, bool TWIN = false, typename Body>
 __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, Pipe& P,
                                              uint32_t* sw, int tile_bytes, Body&& body) {
+  static_assert(!TWIN || QS == 4, "twin windows come four sources per stage");
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ww = L.win_bytes >> 2;
   const int S = L.stages;
-  const int zero_q = QS * S * ww;
+  const int zero_q = (TWIN ? 2 : 1) * QS * S * ww;
   const int npairs = (g.nsrc + QS - 1) / QS;
   const int nchunks = (g.nsrc + kDescChunk - 1) / kDescChunk;
   if (threadIdx.x == 0) {
@@ -315,11 +386,15 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
   volatile int* failed = &P.failed;
   int issued = 0;  // pairs whose copies warp 0 has issued
   bool prod_ok = true;
+  auto produce_group = [&](int q, int s) -> bool {
+    if constexpr (TWIN)
+      return produce_twin(g, P, sw, ww, zero_q, tile_bytes, L.twin_off, q, s, lane, failed, L.err);
+    else
+      return produce<SB, QS>(g, P, sw, ww, zero_q, tile_bytes, q, s, lane, failed, L.err);
+  };
   if (warp == 0)
     for (; issued < min(S - 1, npairs); ++issued)
-      if (!(prod_ok = produce<SB, QS>(g, P, sw, ww, zero_q, tile_bytes, issued, issued, lane,
-                                      failed, L.err)))
-        break;
+      if (!(prod_ok = produce_group(issued, issued))) break;
   if (!prod_ok && lane == 0) {
     if (!*failed) atomicCAS(L.err, 0, kErrWaitFull);
     *failed = 1;
@@ -337,7 +412,7 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
         ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       }
       if (ok) {
-        ok = produce<SB, QS>(g, P, sw, ww, zero_q, tile_bytes, q, s, lane, failed, L.err);
+        ok = produce_group(q, s);
         code = kErrWaitFull;
       }
       if (!ok) {
@@ -462,6 +537,11 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
               const uint32_t v[4] = {s0, s1, s2, s3};
               for (int q = 0; q < 4 && t + q < g.valid; ++q) dst[q] = static_cast<uint16_t>(v[q]);
             }
+            if (L.twin_off) {  // the twin, twin[i] = sums[i - 1], element by element
+              uint16_t* tw = reinterpret_cast<uint16_t*>(row + L.twin_off) + t;
+              const uint32_t v[4] = {s0, s1, s2, s3};
+              for (int q = 0; q < 4 && t + q < g.valid; ++q) tw[q + 1] = static_cast<uint16_t>(v[q]);
+            }
           } else {
             uint32_t* dst = reinterpret_cast<uint32_t*>(row) + t;
             if (t + 4 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
@@ -537,6 +617,55 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
     }
   });
   if (P.failed) return;
+  if constexpr (OUT16 && kConsec && DD_SUM8_STAGED_OUT) {
+    // 16-bit sums leave through shared memory as whole 16-byte chunks: the ring is
+    // free once the pipeline has ended (every warp passed its final barrier), and
+    // each warp stages one row of its segment at a time in a slice of its own, so
+    // only __syncwarp orders the staging.  With a twin (twin[i] = sums[i - 1]) a
+    // warp writes twin[1 .. seg] of its segment; twin[0] is the element before
+    // the segment, written by the warp (or block) that holds it.
+    constexpr int kSeg = 32 * NW * 4;  // samples of a warp's segment
+    uint16_t* st = reinterpret_cast<uint16_t*>(sw) + warp * kSeg;
+    const int64_t seg0 = static_cast<int64_t>(wt) * kSeg;
+    const int64_t nv = g.valid - seg0;  // samples of the segment to store (may be <= 0)
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+      if (rbase + r >= g.nrows) break;
+#pragma unroll
+      for (int k = 0; k < NW; ++k)
+        *reinterpret_cast<uint2*>(st + 4 * (lane * NW + k)) =
+            make_uint2(__byte_perm(ev[r][k], od[r][k], 0x5410), __byte_perm(ev[r][k], od[r][k], 0x7632));
+      __syncwarp();
+      char* row = g.out + (rbase + r) * g.out_pitch;
+      uint16_t* out = reinterpret_cast<uint16_t*>(row) + seg0;
+      uint16_t* tw = L.twin_off ? reinterpret_cast<uint16_t*>(row + L.twin_off) + seg0 : nullptr;
+      for (int c = lane; c < kSeg / 8; c += 32) {
+        const int e = 8 * c;
+        const uint4 v = *reinterpret_cast<const uint4*>(st + e);
+        if (e + 8 <= nv && (reinterpret_cast<uintptr_t>(out + e) & 15) == 0) {
+          *reinterpret_cast<uint4*>(out + e) = v;
+        } else {
+          for (int q = 0; q < 8; ++q)
+            if (e + q < nv) out[e + q] = st[e + q];
+        }
+        if (tw) {
+          if (c > 0 && e + 7 <= nv && (reinterpret_cast<uintptr_t>(tw + e) & 15) == 0) {
+            const uint32_t p = st[e - 1];
+            *reinterpret_cast<uint4*>(tw + e) =
+                make_uint4(__byte_perm(p, v.x, 0x5410), __byte_perm(v.x, v.y, 0x5432),
+                           __byte_perm(v.y, v.z, 0x5432), __byte_perm(v.z, v.w, 0x5432));
+          } else {
+            for (int q = c == 0 ? 1 : 0; q < 8; ++q)
+              if (e + q <= nv) tw[e + q] = st[e + q - 1];
+          }
+        }
+      }
+      // the first twin element of the next segment (its warp skips it)
+      if (tw && lane == 31 && kSeg <= nv) tw[kSeg] = st[kSeg - 1];
+      __syncwarp();
+    }
+    return;
+  }
   emit(FLUSH && stored);
 }
 
@@ -823,6 +952,72 @@ __device__ __forceinline__ void sum_u16_quad(const SumLaunch& L, uint3 blk, uint
   }
 }
 
+// ------------------------------------------------------------------ 16-bit sums with a shifted twin
+// Stage 2 of 8-bit input when stage 1 also wrote the one-sample-shifted twin of
+// its sums (SumLaunch::twin_off): a row whose offset for a source is odd reads
+// that source's twin, so every source word a row needs is one aligned shared
+// load, with no permute.  Four sources per stage are added in packed 16-bit
+// lanes (each <= 64 x 255, four <= 65280) and folded into two 32-bit sums as in
+// sum_u16_quad; lanes own interleaved words (lane l: l, l + 32, ...), so the
+// loads of a warp are 32 consecutive words for any words per lane.  With half
+// the instructions of the quad kernel it waits on its shared loads instead
+// (long-scoreboard stalls 3.3 per issue at two blocks per SM), so it is built for
+// three blocks per SM: 36.7 ms per headline step against 43.2 at two blocks and
+// 46.8 for the quad kernel.
+#ifndef DD_SUM16T_MINB
+#define DD_SUM16T_MINB 3
+#endif
+template <int RB, int NW>
+__device__ __forceinline__ void sum_u16_twin(const SumLaunch& L, uint3 blk, uint32_t* sw, Pipe& P) {
+  constexpr int kGroups = kSumRows / RB;  // warp groups sharing the rows, as in sum_u8
+  constexpr int kWarpsPerTile = kWarps / kGroups;
+  constexpr int T = kWarpsPerTile * 32 * NW * 2;
+  const Geo g = make_geo(L, T, blk);
+  if (g.nrows <= 0) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rbase = (warp / kWarpsPerTile) * RB;
+  const int wbase = (warp % kWarpsPerTile) * 32 * NW + lane;
+  uint32_t lo[RB][NW], hi[RB][NW];
+#pragma unroll
+  for (int r = 0; r < RB; ++r)
+#pragma unroll
+    for (int k = 0; k < NW; ++k) lo[r][k] = hi[r][k] = 0;
+  run_pipeline<2, 4, true>(L, g, P, sw, 2 * T, [&](int s, const uint32_t* win) {
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+      const int4 a = row_pair(P, s, rbase + r, 0), b = row_pair(P, s, rbase + r, 1);
+      const uint32_t* w0 = win + a.x + wbase;
+      const uint32_t* w1 = win + a.z + wbase;
+      const uint32_t* w2 = win + b.x + wbase;
+      const uint32_t* w3 = win + b.z + wbase;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        const uint32_t q = (w0[32 * k] + w1[32 * k] + w2[32 * k]) + w3[32 * k];
+        lo[r][k] += q;
+        hi[r][k] = __umulhi(q, 0x10000u) + hi[r][k];
+      }
+    }
+  });
+  if (P.failed) return;
+#pragma unroll
+  for (int r = 0; r < RB; ++r) {
+    if (rbase + r >= g.nrows) break;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      const int64_t t = static_cast<int64_t>(wbase + 32 * k) * 2;
+      if (t >= g.valid) continue;
+      const uint32_t s0 = lo[r][k] - (hi[r][k] << 16), s1 = hi[r][k];
+      uint32_t* dst = reinterpret_cast<uint32_t*>(g.out + (rbase + r) * g.out_pitch) + t;
+      if (t + 2 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
+        *reinterpret_cast<uint2*>(dst) = make_uint2(s0, s1);
+      } else {
+        dst[0] = s0;
+        if (t + 1 < g.valid) dst[1] = s1;
+      }
+    }
+  }
+}
+
 template <int RB, int NW, bool OUT16, bool FLUSH>
 __global__ void __launch_bounds__(kThreads, DD_SUM8_MINB) k_sum_u8(SumLaunch L) {
   extern __shared__ __align__(128) uint32_t sw[];
@@ -846,6 +1041,12 @@ __global__ void __launch_bounds__(kThreads, DD_SUM16Q_MINB) k_sum_u16q(SumLaunch
   extern __shared__ __align__(128) uint32_t sw[];
   __shared__ Pipe P;
   sum_u16_quad<RB, NW>(L, blockIdx, sw, P);
+}
+template <int RB, int NW>
+__global__ void __launch_bounds__(kThreads, DD_SUM16T_MINB) k_sum_u16t(SumLaunch L) {
+  extern __shared__ __align__(128) uint32_t sw[];
+  __shared__ Pipe P;
+  sum_u16_twin<RB, NW>(L, blockIdx, sw, P);
 }
 template <int RB, int NW>
 __global__ void __launch_bounds__(kThreads, DD_SUM32_MINB) k_sum_u32(SumLaunch L) {
@@ -890,6 +1091,7 @@ __device__ __forceinline__ void run_one(const SumLaunch& L, uint3 blk, uint32_t*
   else if constexpr (KIND == kSumKindU16) sum_u16<kSumRows, DD_SUM16_NW>(L, blk, sw, P);
   else if constexpr (KIND == kSumKindU16Wide) sum_u16_wide<kSumRows, DD_SUM16W_NW>(L, blk, sw, P);
   else if constexpr (KIND == kSumKindU16Quad) sum_u16_quad<kSumRowsPTQ, kSum16QNW>(L, blk, sw, P);
+  else if constexpr (KIND == kSumKindU16Twin) sum_u16_twin<kSumRowsPTT, kSum16TNW>(L, blk, sw, P);
   else sum_u32<kSumRows, kSum32NW>(L, blk, sw, P);
 }
 
@@ -925,6 +1127,7 @@ __device__ __forceinline__ void run_kind(int kind, const SumLaunch& L, uint3 blk
     case kSumKindU16: run_one<kSumKindU16>(L, blk, sw, P); break;
     case kSumKindU16Wide: run_one<kSumKindU16Wide>(L, blk, sw, P); break;
     case kSumKindU16Quad: run_one<kSumKindU16Quad>(L, blk, sw, P); break;
+    case kSumKindU16Twin: run_one<kSumKindU16Twin>(L, blk, sw, P); break;
     default: run_one<kSumKindU32>(L, blk, sw, P); break;
   }
 }
@@ -1011,9 +1214,16 @@ size_t sum_launch_smem(const SumLaunch& L) {
 #endif
 // Staged source pairs for a window size: as many as fit DD_SUM_SMEM_KB of shared
 // memory (two blocks per SM at the default), at least two.
+// The twin-window stage-2 kernel (eight windows per stage) is limited by the
+// latency of its shared loads rather than by issue: it takes at most
+// DD_SUM16T_SMEM_KB so that three blocks fit an SM.
+#ifndef DD_SUM16T_SMEM_KB
+#define DD_SUM16T_SMEM_KB 68
+#endif
 int sum_stages(int win_bytes, int qs) {
+  const int cap = (qs == 8 ? DD_SUM16T_SMEM_KB : DD_SUM_SMEM_KB) * 1024;
   int s = kMaxStages;
-  while (s > 2 && sum_smem_bytes(win_bytes, s, qs) > DD_SUM_SMEM_KB * 1024) --s;
+  while (s > 2 && sum_smem_bytes(win_bytes, s, qs) > static_cast<size_t>(cap)) --s;
   return s;
 }
 
@@ -1061,6 +1271,7 @@ void launch_sum(const SumLaunch& L, cudaStream_t st) {
     case kSumKindU16: launch_k(k_sum_u16<kSumRows, DD_SUM16_NW>, grid, smem, L, st); break;
     case kSumKindU16Wide: launch_k(k_sum_u16w<kSumRows, DD_SUM16W_NW>, grid, smem, L, st); break;
     case kSumKindU16Quad: launch_k(k_sum_u16q<kSumRowsPTQ, kSum16QNW>, grid, smem, L, st); break;
+    case kSumKindU16Twin: launch_k(k_sum_u16t<kSumRowsPTT, kSum16TNW>, grid, smem, L, st); break;
     default: launch_k(k_sum_u32<kSumRows, kSum32NW>, grid, smem, L, st); break;
   }
 }
@@ -1070,7 +1281,11 @@ int sum_kind(const SumLaunch& L) {
     if (L.out_elem == 2) return kSumKindU8Out16;
     return L.flush ? kSumKindU8Flush : kSumKindU8;
   }
-  if (L.src_bytes == 2) return L.flush ? kSumKindU16Wide : L.lane_per >= 4 ? kSumKindU16Quad : kSumKindU16;
+  if (L.src_bytes == 2)
+    return L.flush              ? kSumKindU16Wide
+           : L.lane_per < 4     ? kSumKindU16
+           : L.twin_off != 0   ? kSumKindU16Twin
+                                : kSumKindU16Quad;
   return kSumKindU32;
 }
 
@@ -1173,6 +1388,7 @@ void launch_sum_grouped(const SumBatchGroup* d_groups, int ngroups, long long to
     case kSumKindU16: launch_grouped_k<kSumKindU16>(d_groups, ngroups, total, smem, st); break;
     case kSumKindU16Wide: launch_grouped_k<kSumKindU16Wide>(d_groups, ngroups, total, smem, st); break;
     case kSumKindU16Quad: launch_grouped_k<kSumKindU16Quad>(d_groups, ngroups, total, smem, st); break;
+    case kSumKindU16Twin: launch_grouped_k<kSumKindU16Twin>(d_groups, ngroups, total, smem, st); break;
     default: launch_grouped_k<kSumKindU32>(d_groups, ngroups, total, smem, st); break;
   }
 }
