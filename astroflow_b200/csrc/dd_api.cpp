@@ -627,7 +627,8 @@ SumLaunch stage1_launch(const dd_plan& P, int64_t t0, int buf = 0) {
   L.grid_z = static_cast<unsigned>(P.nsb);
   L.desc = P.d_desc1.as<SumDesc>();
   L.desc_pitch = P.dch;
-  L.stages = P.stages_override ? P.stages_override : sum_stages(P.win1);
+  L.stages = P.stages_override ? P.stages_override
+                                : sum_stages(P.win1, 2, sum_kind_extra_smem(sum_kind(L)));
   L.err = P.d_err.as<int>();
   L.one = 1;
   L.twin_off = twin_offset(P);
@@ -774,7 +775,7 @@ SumLaunch brute_launch(const dd_plan& P, void* output) {
   L.grid_z = 1;
   L.desc = P.d_descb.as<SumDesc>();
   L.desc_pitch = P.nc;
-  L.stages = sum_stages(P.winb);
+  L.stages = sum_stages(P.winb, 2, sum_kind_extra_smem(sum_kind(L)));
   L.err = P.d_err.as<int>();
   L.one = 1;
   return L;
@@ -1143,7 +1144,7 @@ int dd_plan_autotune(dd_plan* P, const void* input, void* output, int32_t reps, 
     // stage counts that keep two blocks per SM for both stages
     auto fits = [&](int S) {
       return S >= 2 && S <= kSumMaxStages &&
-             sum_smem_bytes(P->win1, S) <= 113 * 1024 &&
+             sum_smem_bytes(P->win1, S) + sum_kind_extra_smem(sum_kind(stage1_launch(*P, 0))) <= 113 * 1024 &&
              sum_smem_bytes(P->win2, S, sum_kind_qs(stage2_kind(*P))) <= 113 * 1024;
     };
     const int64_t budget0 = P->inter_budget;
@@ -1361,7 +1362,7 @@ bool batched_plan(const dd_plan& P, bool persistent) {
   const bool brute = P.p.algorithm == DD_ALGO_BRUTE;
   if (brute ? !P.winb : (!P.win1 || !P.win2)) return false;
   if (!persistent) return true;
-  return brute ? win_smem(P.winb) <= kBatchSmemCap
+  return brute ? sum_launch_smem(brute_launch(P, nullptr)) <= kBatchSmemCap
                : win_smem(P.win1) <= kBatchSmemCap &&
                      win_smem(P.win2, sum_kind_qs(stage2_kind(P))) <= kBatchSmemCap;
 }

@@ -311,8 +311,9 @@ int sum_tile_samples(int src_bytes, int nw);
 // Shared memory of a staged sum with `stages` pairs in flight.
 // qs: source windows per pipeline stage (2, or 4 for the quad kernel).
 size_t sum_smem_bytes(int win_bytes, int stages, int qs = 2);
-// Pairs in flight that fit the shared memory of two blocks per SM (at least 2).
-int sum_stages(int win_bytes, int qs = 2);
+// Pairs in flight that fit the shared memory of two blocks per SM (at least 2),
+// next to `extra` bytes the kernel needs besides its ring.
+int sum_stages(int win_bytes, int qs = 2, size_t extra = 0);
 // Descriptors of a [nrows][ncols] offset table for row groups of kSumRows rows,
 // grouped within blocks of `group` rows (0: one block), in the launch's
 // blockIdx.y order.  Fails if a group's spread exceeds 65535.
@@ -405,8 +406,10 @@ inline int sum_kind_tile(int kind) {
 inline int sum_kind_qs(int kind) {
   return kind == kSumKindU16Quad ? 4 : kind == kSumKindU16Twin ? 8 : 2;
 }
-// Shared memory of a launch (its variant's windows per stage).
+// Shared memory of a launch (its variant's windows per stage, plus the variant's
+// staging past the ring, sum_kind_extra_smem).
 size_t sum_launch_smem(const SumLaunch& L);
+size_t sum_kind_extra_smem(int kind);
 // Stage 1 of one tile and stage 2 of another in one launch (false: no paired
 // kernel for these variants; nothing launched).
 bool launch_sum_pair(const SumLaunch& L1, const SumLaunch& L2, cudaStream_t st);

@@ -130,6 +130,11 @@ __device__ __forceinline__ uint32_t madhi_u32(uint32_t a, uint32_t b, uint32_t c
 #ifndef DD_SUM8_STAGED_OUT
 #define DD_SUM8_STAGED_OUT 1
 #endif
+// The 32-bit flushes of 8-bit sums go through shared memory as 16-byte chunks
+// (1) or as each lane's words (0); the staging takes flush_smem_bytes() past the ring.
+#ifndef DD_SUM8_STAGED_FLUSH
+#define DD_SUM8_STAGED_FLUSH 1
+#endif
 #ifndef DD_SUM16Q_MINB
 #define DD_SUM16Q_MINB 2
 #endif
@@ -561,6 +566,45 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
       }
     }
   };
+  // 32-bit outputs of many 8-bit sources: every 256 sources each warp adds its
+  // lanes into the output through a slice of shared memory past the ring (one row
+  // at a time, ordered by __syncwarp), as whole 16-byte chunks: a read-add-write
+  // of the partial sums an earlier flush stored when `add`.  Clears the lanes.
+  auto flush_staged = [&](bool add) {
+    constexpr int kSeg = 32 * NW * 4;  // samples of a warp's segment
+    uint32_t* st = sw + (2 * L.stages + 1) * (L.win_bytes >> 2) + warp * kSeg;
+    const int64_t seg0 = static_cast<int64_t>(wt) * kSeg;
+    const int64_t nv = g.valid - seg0;  // samples of the segment to store (may be <= 0)
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+      if (rbase + r >= g.nrows) break;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        *reinterpret_cast<uint4*>(st + 4 * (lane * NW + k)) =
+            make_uint4(ev[r][k] & 0xffffu, od[r][k] & 0xffffu, ev[r][k] >> 16, od[r][k] >> 16);
+        ev[r][k] = od[r][k] = 0;
+      }
+      __syncwarp();
+      uint32_t* out = reinterpret_cast<uint32_t*>(g.out + (rbase + r) * g.out_pitch) + seg0;
+      for (int c = lane; c < kSeg / 4; c += 32) {
+        const int e = 4 * c;
+        uint4 v = *reinterpret_cast<const uint4*>(st + e);
+        if (e + 4 <= nv && (reinterpret_cast<uintptr_t>(out + e) & 15) == 0) {
+          if (add) {
+            const uint4 o = *reinterpret_cast<const uint4*>(out + e);
+            v.x += o.x; v.y += o.y; v.z += o.z; v.w += o.w;
+          }
+          *reinterpret_cast<uint4*>(out + e) = v;
+        } else {
+          const uint32_t a[4] = {v.x, v.y, v.z, v.w};
+          for (int q = 0; q < 4; ++q)
+            if (e + q < nv) out[e + q] = add ? out[e + q] + a[q] : a[q];
+        }
+      }
+      __syncwarp();
+    }
+  };
+  constexpr bool kStagedFlush = FLUSH && kConsec && DD_SUM8_STAGED_FLUSH;
   int since = 0;       // sources summed in the 16-bit lanes since the last flush
   bool stored = false; // the output holds partial sums of an earlier flush
   run_pipeline<1>(L, g, P, sw, T, [&](int s, const uint32_t* win) {
@@ -610,7 +654,8 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
     if constexpr (FLUSH) {
       since += 2;
       if (since >= 256) {  // 256 x 255 fits a 16-bit lane: move the lanes to the output
-        emit(stored);
+        if constexpr (kStagedFlush) flush_staged(stored);
+        else emit(stored);
         stored = true;
         since = 0;
       }
@@ -666,7 +711,8 @@ __device__ __forceinline__ void sum_u8(const SumLaunch& L, uint3 blk, uint32_t* 
     }
     return;
   }
-  emit(FLUSH && stored);
+  if constexpr (kStagedFlush) flush_staged(stored);
+  else emit(FLUSH && stored);
 }
 
 // ------------------------------------------------------------------ 16-bit samples
@@ -1205,8 +1251,17 @@ size_t sum_smem_bytes(int win_bytes, int stages, int qs) {
   return static_cast<size_t>(qs * stages + 1) * win_bytes;
 }
 
+size_t sum_kind_extra_smem(int kind) {
+  // the flush staging of the 8-bit kernel with 32-bit outputs: one segment of
+  // 32-bit sums per warp
+  return (kind == kSumKindU8Flush && DD_SUM8_STAGED_FLUSH && (DD_SUM8F_NW & 1))
+             ? static_cast<size_t>(kWarps) * 32 * DD_SUM8F_NW * 4 * sizeof(uint32_t)
+             : 0;
+}
+
 size_t sum_launch_smem(const SumLaunch& L) {
-  return sum_smem_bytes(L.win_bytes, L.stages, sum_kind_qs(sum_kind(L)));
+  const int kind = sum_kind(L);
+  return sum_smem_bytes(L.win_bytes, L.stages, sum_kind_qs(kind)) + sum_kind_extra_smem(kind);
 }
 
 #ifndef DD_SUM_SMEM_KB
@@ -1220,10 +1275,10 @@ size_t sum_launch_smem(const SumLaunch& L) {
 #ifndef DD_SUM16T_SMEM_KB
 #define DD_SUM16T_SMEM_KB 68
 #endif
-int sum_stages(int win_bytes, int qs) {
-  const int cap = (qs == 8 ? DD_SUM16T_SMEM_KB : DD_SUM_SMEM_KB) * 1024;
+int sum_stages(int win_bytes, int qs, size_t extra) {
+  const size_t cap = static_cast<size_t>(qs == 8 ? DD_SUM16T_SMEM_KB : DD_SUM_SMEM_KB) * 1024;
   int s = kMaxStages;
-  while (s > 2 && sum_smem_bytes(win_bytes, s, qs) > static_cast<size_t>(cap)) --s;
+  while (s > 2 && sum_smem_bytes(win_bytes, s, qs) + extra > cap) --s;
   return s;
 }
 
