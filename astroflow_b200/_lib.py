@@ -71,7 +71,8 @@ class PlanInfo(ctypes.Structure):
         "chan_start", "chan_end", "dm_steps", "nsamp_in", "nsamp_binned", "out_cols",
         "out_elem_bytes", "nsb", "ndm_nom", "max_delay", "max_residual", "nslices",
         "n_iqrm_windows", "workspace_bytes", "delay_rows", "delay_cols",
-        "table_mismatch_fp64", "tile_samples")] + [("adds_per_run", ctypes.c_double)]
+        "table_mismatch_fp64", "tile_samples")] + [("adds_per_run", ctypes.c_double),
+                                                    ("subband_sum_copies", ctypes.c_int64)]
 
 
 class BatchInfo(ctypes.Structure):

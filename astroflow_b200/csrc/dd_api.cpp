@@ -627,8 +627,7 @@ SumLaunch stage1_launch(const dd_plan& P, int64_t t0, int buf = 0) {
   L.grid_z = static_cast<unsigned>(P.nsb);
   L.desc = P.d_desc1.as<SumDesc>();
   L.desc_pitch = P.dch;
-  L.stages = P.stages_override ? P.stages_override
-                                : sum_stages(P.win1, 2, sum_kind_extra_smem(sum_kind(L)));
+  L.stages = P.stages_override ? P.stages_override : sum_kind_stages(sum_kind(L), P.win1);
   L.err = P.d_err.as<int>();
   L.one = 1;
   L.twin_off = twin_offset(P);
@@ -660,7 +659,7 @@ SumLaunch stage2_launch(const dd_plan& P, int64_t t0, void* output, int buf = 0)
   L.grid_z = 1;
   L.desc = P.d_desc2.as<SumDesc>();
   L.desc_pitch = P.nsb;
-  L.stages = P.stages_override ? P.stages_override : sum_stages(P.win2, sum_kind_qs(stage2_kind(P)));
+  L.stages = P.stages_override ? P.stages_override : sum_kind_stages(stage2_kind(P), P.win2);
   L.err = P.d_err.as<int>();
   L.one = 1;
   L.twin_off = twin_offset(P);
@@ -775,7 +774,7 @@ SumLaunch brute_launch(const dd_plan& P, void* output) {
   L.grid_z = 1;
   L.desc = P.d_descb.as<SumDesc>();
   L.desc_pitch = P.nc;
-  L.stages = sum_stages(P.winb, 2, sum_kind_extra_smem(sum_kind(L)));
+  L.stages = sum_kind_stages(sum_kind(L), P.winb);
   L.err = P.d_err.as<int>();
   L.one = 1;
   return L;
@@ -1049,6 +1048,7 @@ int dd_plan_get_info(const dd_plan* P, dd_plan_info* info) {
     o.delay_cols = P->p.algorithm == DD_ALGO_BRUTE ? P->nc : P->dch;
     o.table_mismatch_fp64 = P->table_mismatch_fp64;
     o.tile_samples = P->tile;
+    o.subband_sum_copies = P->p.algorithm == DD_ALGO_SUBBAND ? (P->twin ? 2 : 1) : 0;
     o.adds_per_run = P->adds;
     *info = o;
   });
@@ -1143,9 +1143,10 @@ int dd_plan_autotune(dd_plan* P, const void* input, void* output, int32_t reps, 
     };
     // stage counts that keep two blocks per SM for both stages
     auto fits = [&](int S) {
-      return S >= 2 && S <= kSumMaxStages &&
-             sum_smem_bytes(P->win1, S) + sum_kind_extra_smem(sum_kind(stage1_launch(*P, 0))) <= 113 * 1024 &&
-             sum_smem_bytes(P->win2, S, sum_kind_qs(stage2_kind(*P))) <= 113 * 1024;
+      if (S < 2 || S > kSumMaxStages) return false;
+      SumLaunch l1 = stage1_launch(*P, 0), l2 = stage2_launch(*P, 0, output);
+      l1.stages = l2.stages = S;
+      return sum_launch_smem(l1) <= 113 * 1024 && sum_launch_smem(l2) <= 113 * 1024;
     };
     const int64_t budget0 = P->inter_budget;
     const int stages0 = P->stages_override;
@@ -1354,7 +1355,6 @@ namespace {
 // Shared memory of a staged sum that leaves two persistent blocks per SM.
 constexpr size_t kBatchSmemCap = 100 * 1024;
 
-size_t win_smem(int win, int qs = 2) { return win ? sum_smem_bytes(win, sum_stages(win, qs), qs) : 0; }
 
 // Whether plan P's sums run in the batched launches.
 bool batched_plan(const dd_plan& P, bool persistent) {
@@ -1363,8 +1363,8 @@ bool batched_plan(const dd_plan& P, bool persistent) {
   if (brute ? !P.winb : (!P.win1 || !P.win2)) return false;
   if (!persistent) return true;
   return brute ? sum_launch_smem(brute_launch(P, nullptr)) <= kBatchSmemCap
-               : win_smem(P.win1) <= kBatchSmemCap &&
-                     win_smem(P.win2, sum_kind_qs(stage2_kind(P))) <= kBatchSmemCap;
+               : sum_launch_smem(stage1_launch(P, 0)) <= kBatchSmemCap &&
+                     sum_launch_smem(stage2_launch(P, 0, nullptr)) <= kBatchSmemCap;
 }
 
 long long group_blocks(const SumBatchGroup& g) {

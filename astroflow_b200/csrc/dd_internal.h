@@ -305,6 +305,10 @@ struct SumLaunch {
 #ifndef DD_SUM_MAX_STAGES
 #define DD_SUM_MAX_STAGES 8
 #endif
+// Shared memory (KB) the staged sums stay within by default: two blocks per SM.
+#ifndef DD_SUM_SMEM_KB
+#define DD_SUM_SMEM_KB 100
+#endif
 constexpr int kSumMaxStages = DD_SUM_MAX_STAGES;  // staged source pairs in flight, at most
 void launch_sum(const SumLaunch& L, cudaStream_t st);
 int sum_tile_samples(int src_bytes, int nw);
@@ -312,8 +316,12 @@ int sum_tile_samples(int src_bytes, int nw);
 // qs: source windows per pipeline stage (2, or 4 for the quad kernel).
 size_t sum_smem_bytes(int win_bytes, int stages, int qs = 2);
 // Pairs in flight that fit the shared memory of two blocks per SM (at least 2),
-// next to `extra` bytes the kernel needs besides its ring.
-int sum_stages(int win_bytes, int qs = 2, size_t extra = 0);
+// next to `extra` bytes the kernel needs besides its ring (cap_kb: the shared
+// memory to stay within, 0 for the default).
+int sum_stages(int win_bytes, int qs = 2, size_t extra = 0, int cap_kb = 0);
+// Stages of a kernel variant for a window size (its windows per stage, staging
+// and shared-memory cap).
+int sum_kind_stages(int kind, int win_bytes);
 // Descriptors of a [nrows][ncols] offset table for row groups of kSumRows rows,
 // grouped within blocks of `group` rows (0: one block), in the launch's
 // blockIdx.y order.  Fails if a group's spread exceeds 65535.

@@ -361,14 +361,18 @@ __device__ __forceinline__ bool produce_twin(const Geo& g, Pipe& P, uint32_t* sw
 // Pipeline driver shared by the kernels: calls body(stage, cur) for every
 // group of QS sources once their windows are in shared memory (TWIN: each
 // source is staged with its shifted twin, see produce_twin; QS is 4).
-template <int SB, int QS = 2, bool TWIN = false, typename Body>
+// Window modes of the pipeline: one window per source, or a source and its twin
+// (four sources per stage).
+constexpr int kModePlain = 0, kModeTwin = 1;
+template <int SB, int QS = 2, int MODE = kModePlain, typename Body>
 __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, Pipe& P,
                                              uint32_t* sw, int tile_bytes, Body&& body) {
-  static_assert(!TWIN || QS == 4, "twin windows come four sources per stage");
+  static_assert(MODE != kModeTwin || QS == 4, "twin windows come four sources per stage");
+  constexpr int kWinPerSrc = MODE == kModeTwin ? 2 : 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ww = L.win_bytes >> 2;
   const int S = L.stages;
-  const int zero_q = (TWIN ? 2 : 1) * QS * S * ww;
+  const int zero_q = kWinPerSrc * QS * S * ww;
   const int npairs = (g.nsrc + QS - 1) / QS;
   const int nchunks = (g.nsrc + kDescChunk - 1) / kDescChunk;
   if (threadIdx.x == 0) {
@@ -392,7 +396,7 @@ __device__ __forceinline__ void run_pipeline(const SumLaunch& L, const Geo& g, P
   int issued = 0;  // pairs whose copies warp 0 has issued
   bool prod_ok = true;
   auto produce_group = [&](int q, int s) -> bool {
-    if constexpr (TWIN)
+    if constexpr (MODE == kModeTwin)
       return produce_twin(g, P, sw, ww, zero_q, tile_bytes, L.twin_off, q, s, lane, failed, L.err);
     else
       return produce<SB, QS>(g, P, sw, ww, zero_q, tile_bytes, q, s, lane, failed, L.err);
@@ -1028,7 +1032,7 @@ __device__ __forceinline__ void sum_u16_twin(const SumLaunch& L, uint3 blk, uint
   for (int r = 0; r < RB; ++r)
 #pragma unroll
     for (int k = 0; k < NW; ++k) lo[r][k] = hi[r][k] = 0;
-  run_pipeline<2, 4, true>(L, g, P, sw, 2 * T, [&](int s, const uint32_t* win) {
+  run_pipeline<2, 4, kModeTwin>(L, g, P, sw, 2 * T, [&](int s, const uint32_t* win) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
       const int4 a = row_pair(P, s, rbase + r, 0), b = row_pair(P, s, rbase + r, 1);
@@ -1264,9 +1268,6 @@ size_t sum_launch_smem(const SumLaunch& L) {
   return sum_smem_bytes(L.win_bytes, L.stages, sum_kind_qs(kind)) + sum_kind_extra_smem(kind);
 }
 
-#ifndef DD_SUM_SMEM_KB
-#define DD_SUM_SMEM_KB 100
-#endif
 // Staged source pairs for a window size: as many as fit DD_SUM_SMEM_KB of shared
 // memory (two blocks per SM at the default), at least two.
 // The twin-window stage-2 kernel (eight windows per stage) is limited by the
@@ -1275,11 +1276,16 @@ size_t sum_launch_smem(const SumLaunch& L) {
 #ifndef DD_SUM16T_SMEM_KB
 #define DD_SUM16T_SMEM_KB 68
 #endif
-int sum_stages(int win_bytes, int qs, size_t extra) {
-  const size_t cap = static_cast<size_t>(qs == 8 ? DD_SUM16T_SMEM_KB : DD_SUM_SMEM_KB) * 1024;
+int sum_stages(int win_bytes, int qs, size_t extra, int cap_kb) {
+  const size_t cap = static_cast<size_t>(cap_kb > 0 ? cap_kb : DD_SUM_SMEM_KB) * 1024;
   int s = kMaxStages;
   while (s > 2 && sum_smem_bytes(win_bytes, s, qs) + extra > cap) --s;
   return s;
+}
+
+int sum_kind_stages(int kind, int win_bytes) {
+  return sum_stages(win_bytes, sum_kind_qs(kind), sum_kind_extra_smem(kind),
+                    kind == kSumKindU16Twin ? DD_SUM16T_SMEM_KB : DD_SUM_SMEM_KB);
 }
 
 std::vector<SumDesc> build_sum_desc(const std::vector<int32_t>& tab, int64_t nrows,

@@ -168,7 +168,15 @@ class Server:
             try:
                 if kind == "build":
                     host, header, kw = t.payload
-                    plan = Plan(header, device=self.device, **kw)
+                    try:
+                        plan = Plan(header, device=self.device, **kw)
+                    except MemoryError:
+                        # torch's caching allocator may hold the free memory the plan
+                        # needs (the plan allocates from the stream-ordered pool):
+                        # release its unused blocks and build once more
+                        torch.cuda.synchronize(self.device)
+                        torch.cuda.empty_cache()
+                        plan = Plan(header, device=self.device, **kw)
                     t.payload = (host, header, kw, plan)
                     self._built.put(t)
                 else:  # release, stream-ordered on the file's stream (its work is done)
@@ -185,10 +193,11 @@ class Server:
         host, header, kw = t.payload[:3]
         g = (lambda k: header[k]) if isinstance(header, dict) else (lambda k: getattr(header, k))
         n, c, bits = int(g("ndata")), int(g("nchans")), int(g("nbits"))
-        # input, prepared copy, output rows (an upper bound on DM trials), tile
+        # input, prepared copy, output rows (an upper bound on DM trials), one
+        # time tile of subband sums (the library's default budget: 2 GiB)
         lo, hi, step = kw["dm_low"], kw["dm_high"], kw.get("dm_step", 1.0)
         ndm = int((hi - lo) / step) + 1
-        return 2 * n * c * bits // 8 + ndm * n * 4 + (1 << 30)
+        return 2 * n * c * bits // 8 + ndm * n * 4 + (2 << 30)
 
     def step(self) -> bool:
         """One pass: finish completed work, launch ready beam chunks, admit files.

@@ -1039,15 +1039,17 @@ def main():
         # bytes of one subband sum: 16-bit for 8-bit samples in subbands of <= 64
         # channels, else the reference's accumulator type
         inter = 2 if (wl["nbits"] == 8 and wl["subband_width"] <= 64) else (8 if wl["nbits"] == 32 else 4)
+        # stage 1 may also write a one-sample-shifted twin of its sums, which stage 2 reads
+        inter *= max(1, int(info["subband_sum_copies"]))
         if st["stage1_ms"] >= st["stage2_ms"]:
             kname, kms, kn = "stage1", st["stage1_ms"], s1n
             adds_launch = info["ndm_nom"] * dch * tile
-            # the tile's prepared input, read once, and its subband sums, written once
+            # the tile's prepared input, read once, and its subband sums (and twin), written once
             kbytes = dch * tile * elem + info["ndm_nom"] * info["nsb"] * tile * inter
         else:
             kname, kms, kn = "stage2", st["stage2_ms"], s2n
             adds_launch = info["dm_steps"] * info["nsb"] * tile
-            # the tile's subband sums, read once, and its DM-time output, written once
+            # the tile's subband sums (and twin), read once, and its DM-time output, written once
             kbytes = info["ndm_nom"] * info["nsb"] * tile * inter + info["dm_steps"] * tile * 4
         units_launch = info["dm_steps"] * tile
     else:

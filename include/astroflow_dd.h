@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define DD_ABI_VERSION 1
+#define DD_ABI_VERSION 2
 
 /* Status codes.  DD_ERR_INVALID corresponds to the reference's
  * std::invalid_argument (Python ValueError), e.g. a frequency range outside
@@ -172,6 +172,8 @@ typedef struct dd_plan_info {
   int64_t table_mismatch_fp64; /* delay entries where the table differs from the FP64 table */
   int64_t tile_samples;      /* time samples per stage-1/stage-2 launch (subband) */
   double adds_per_run;       /* algorithmic integer additions per dd_run */
+  int64_t subband_sum_copies; /* copies of each stage-1 sum in device memory: 2 when stage 1
+                                 also writes the one-sample-shifted twin stage 2 reads, else 1 */
 } dd_plan_info;
 
 typedef struct dd_plan dd_plan;

@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol():
     assert set(names) == set(_lib.EXPORTS)
     for n in names:
         assert hasattr(L, n), n
-    assert L.dd_abi_version() == 1
+    assert L.dd_abi_version() == 2
 
 
 def test_error_path_without_gpu_is_a_status_not_an_exit():
