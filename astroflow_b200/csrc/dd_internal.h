@@ -241,6 +241,19 @@ struct BruteArgs {
 };
 void launch_brute(const BruteArgs& a, cudaStream_t st);
 
+// Allows `kernel` `dynamic_smem` bytes of dynamic shared memory: above 48 KB per
+// block, counting the kernel's static shared memory, a launch needs the opt-in.
+template <typename K>
+inline void allow_dynamic_smem(K kernel, size_t dynamic_smem) {
+  if (dynamic_smem == 0) return;
+  cudaFuncAttributes fa{};
+  DD_CUDA_TRY(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(kernel)));
+  if (dynamic_smem + fa.sharedSizeBytes > 48 * 1024)
+    DD_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(dynamic_smem)));
+}
+
 // ---- shared-memory staged sums (dd_sumsmem.cu) ----
 constexpr int kSumRows = 8;  // output rows per block
 // Groups of warps the block's rows are split over: each group covers the whole
@@ -359,6 +372,22 @@ constexpr int kSum32NW = DD_SUM32_NW;  // words per lane of the 32-bit staged su
 #ifndef DD_SUM16W_NW
 #define DD_SUM16W_NW 5
 #endif
+// Warp groups the block's rows are split over in the 16-bit-into-32-bit kernel,
+// blocks per SM it is built for and the shared memory (KB) it stays within.  Two
+// warp groups of four rows at three blocks per SM took stage 1 of the
+// 8192-channel 16-bit case on 2^18 samples (DM 0:0.25:500) from 35.4 to 30.6 ms
+// but the full configuration (2^21 samples, three ranges) from 498 to 522 ms, so
+// one group at two blocks per SM stays the default.
+#ifndef DD_SUM16W_ROWSPLIT
+#define DD_SUM16W_ROWSPLIT 1
+#endif
+#ifndef DD_SUM16W_MINB
+#define DD_SUM16W_MINB 2
+#endif
+#ifndef DD_SUM16W_SMEM_KB
+#define DD_SUM16W_SMEM_KB 100
+#endif
+constexpr int kSumRowsPTW = kSumRows / DD_SUM16W_ROWSPLIT;
 // Words per lane of the 16-bit quad stage-2 kernel (odd: conflict-free consecutive words).
 #ifndef DD_SUM16Q_NW
 #define DD_SUM16Q_NW 9
@@ -387,7 +416,8 @@ constexpr int kSumRowsPTT = kSumRows / DD_SUM16T_ROWSPLIT;
 // 32-bit lanes (the k_sum_u16w variant).
 inline int sum_variant_tile(int src_bytes, bool flush) {
   return src_bytes == 4   ? sum_tile_samples(4, kSum32NW)
-         : src_bytes == 2 ? sum_tile_samples(2, flush ? DD_SUM16W_NW : DD_SUM16_NW)
+         : src_bytes == 2 ? (flush ? sum_tile_samples(2, DD_SUM16W_NW) / DD_SUM16W_ROWSPLIT
+                                   : sum_tile_samples(2, DD_SUM16_NW))
                           : sum_tile_samples(1, flush ? DD_SUM8F_NW : DD_SUM8_NW) / DD_SUM_ROWSPLIT;
 }
 // Tile (samples per block) of a kernel variant (SumKind below).
@@ -403,7 +433,7 @@ inline int sum_kind_tile(int kind) {
     case kSumKindU8Out16: case kSumKindU8: return sum_tile_samples(1, DD_SUM8_NW) / DD_SUM_ROWSPLIT;
     case kSumKindU8Flush: return sum_tile_samples(1, DD_SUM8F_NW) / DD_SUM_ROWSPLIT;
     case kSumKindU16: return sum_tile_samples(2, DD_SUM16_NW);
-    case kSumKindU16Wide: return sum_tile_samples(2, DD_SUM16W_NW);
+    case kSumKindU16Wide: return sum_tile_samples(2, DD_SUM16W_NW) / DD_SUM16W_ROWSPLIT;
     case kSumKindU16Quad: return sum_tile_samples(2, kSum16QNW) / DD_SUM16Q_ROWSPLIT;
     case kSumKindU16Twin: return sum_tile_samples(2, kSum16TNW) / DD_SUM16T_ROWSPLIT;
     default: return sum_tile_samples(4, kSum32NW);

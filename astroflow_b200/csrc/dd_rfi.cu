@@ -636,8 +636,7 @@ void launch_iqrm_decide(const unsigned long long* d_sums, int nwin, const uint32
   int sort_n = 1;
   while (sort_n < csub) sort_n <<= 1;
   const size_t smem = sizeof(float) * sort_n;
-  if (smem > 48 * 1024)
-    DD_CUDA_TRY(cudaFuncSetAttribute(k_iqrm_decide, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  allow_dynamic_smem(k_iqrm_decide, smem);
   k_iqrm_decide<<<nwin, 1024, smem, st>>>(d_sums, d_win, nchans, cs, static_cast<int>(csub), mode,
                                           nsigma, d_lags, nlags, variant, xs, ds_, recv, cast_,
                                           flags, sort_n, d_masks);

@@ -822,13 +822,18 @@ __device__ __forceinline__ void sum_u16(const SumLaunch& L, uint3 blk, uint32_t*
 // pipe, and two sources are added per three-input add.
 template <int RB, int NW>
 __device__ __forceinline__ void sum_u16_wide(const SumLaunch& L, uint3 blk, uint32_t* sw, Pipe& P) {
-  constexpr int T = kWarps * 32 * NW * 2;
+  // RB rows per thread: the block's rows are split over kSumRows/RB warp groups,
+  // each covering the whole tile for its RB rows (as in sum_u8)
+  constexpr int kGroups = kSumRows / RB;
+  constexpr int kWarpsPerTile = kWarps / kGroups;
+  constexpr int T = kWarpsPerTile * 32 * NW * 2;
   const Geo g = make_geo(L, T, blk);
   if (g.nrows <= 0) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rbase = (warp / kWarpsPerTile) * RB, wt = warp % kWarpsPerTile;
   constexpr bool kConsec = (NW & 1) != 0;  // lane layout as in k_sum_u8
   constexpr int kStride = kConsec ? 1 : 32;
-  const int wbase = kConsec ? warp * 32 * NW + lane * NW : warp * 32 * NW + lane;
+  const int wbase = kConsec ? wt * 32 * NW + lane * NW : wt * 32 * NW + lane;
   uint32_t lo32[RB][NW], hi32[RB][NW];
 #pragma unroll
   for (int r = 0; r < RB; ++r)
@@ -837,7 +842,7 @@ __device__ __forceinline__ void sum_u16_wide(const SumLaunch& L, uint3 blk, uint
   run_pipeline<2>(L, g, P, sw, 2 * T, [&](int s, const uint32_t* win) {
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
-      const int4 rw = row_pair(P, s, r, 0);
+      const int4 rw = row_pair(P, s, rbase + r, 0);
       const uint32_t* w0 = win + rw.x + wbase;
       const uint32_t* w1 = win + rw.z + wbase;
       uint32_t va[NW + 1], vb[NW + 1];
@@ -868,12 +873,12 @@ __device__ __forceinline__ void sum_u16_wide(const SumLaunch& L, uint3 blk, uint
   if (P.failed) return;
 #pragma unroll
   for (int r = 0; r < RB; ++r) {
-    if (r >= g.nrows) break;
+    if (rbase + r >= g.nrows) break;
 #pragma unroll
     for (int k = 0; k < NW; ++k) {
       const int64_t t = static_cast<int64_t>(wbase + kStride * k) * 2;
       if (t >= g.valid) continue;
-      uint32_t* dst = reinterpret_cast<uint32_t*>(g.out + r * g.out_pitch) + t;
+      uint32_t* dst = reinterpret_cast<uint32_t*>(g.out + (rbase + r) * g.out_pitch) + t;
       if (t + 2 <= g.valid && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
         *reinterpret_cast<uint2*>(dst) = make_uint2(lo32[r][k], hi32[r][k]);
       } else {
@@ -1081,7 +1086,7 @@ __global__ void __launch_bounds__(kThreads, DD_SUM16_MINB) k_sum_u16(SumLaunch L
   sum_u16<RB, NW>(L, blockIdx, sw, P);
 }
 template <int RB, int NW>
-__global__ void __launch_bounds__(kThreads, 2) k_sum_u16w(SumLaunch L) {
+__global__ void __launch_bounds__(kThreads, DD_SUM16W_MINB) k_sum_u16w(SumLaunch L) {
   extern __shared__ __align__(128) uint32_t sw[];
   __shared__ Pipe P;
   sum_u16_wide<RB, NW>(L, blockIdx, sw, P);
@@ -1139,7 +1144,7 @@ __device__ __forceinline__ void run_one(const SumLaunch& L, uint3 blk, uint32_t*
   else if constexpr (KIND == kSumKindU8Flush) sum_u8<kSumRowsPT, DD_SUM8F_NW, false, true>(L, blk, sw, P);
   else if constexpr (KIND == kSumKindU8) sum_u8<kSumRowsPT, DD_SUM8_NW, false, false>(L, blk, sw, P);
   else if constexpr (KIND == kSumKindU16) sum_u16<kSumRows, DD_SUM16_NW>(L, blk, sw, P);
-  else if constexpr (KIND == kSumKindU16Wide) sum_u16_wide<kSumRows, DD_SUM16W_NW>(L, blk, sw, P);
+  else if constexpr (KIND == kSumKindU16Wide) sum_u16_wide<kSumRowsPTW, DD_SUM16W_NW>(L, blk, sw, P);
   else if constexpr (KIND == kSumKindU16Quad) sum_u16_quad<kSumRowsPTQ, kSum16QNW>(L, blk, sw, P);
   else if constexpr (KIND == kSumKindU16Twin) sum_u16_twin<kSumRowsPTT, kSum16TNW>(L, blk, sw, P);
   else sum_u32<kSumRows, kSum32NW>(L, blk, sw, P);
@@ -1239,9 +1244,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_sum_batch(const SumBatchGroup* 
 
 template <typename K>
 void launch_k(K kernel, dim3 grid, size_t smem, const SumLaunch& L, cudaStream_t st) {
-  if (smem > 48 * 1024)
-    DD_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
+  allow_dynamic_smem(kernel, smem);
   kernel<<<grid, kThreads, smem, st>>>(L);
   DD_LAUNCHED();
 }
@@ -1285,7 +1288,9 @@ int sum_stages(int win_bytes, int qs, size_t extra, int cap_kb) {
 
 int sum_kind_stages(int kind, int win_bytes) {
   return sum_stages(win_bytes, sum_kind_qs(kind), sum_kind_extra_smem(kind),
-                    kind == kSumKindU16Twin ? DD_SUM16T_SMEM_KB : DD_SUM_SMEM_KB);
+                    kind == kSumKindU16Twin   ? DD_SUM16T_SMEM_KB
+                    : kind == kSumKindU16Wide ? DD_SUM16W_SMEM_KB
+                                              : DD_SUM_SMEM_KB);
 }
 
 std::vector<SumDesc> build_sum_desc(const std::vector<int32_t>& tab, int64_t nrows,
@@ -1330,7 +1335,7 @@ void launch_sum(const SumLaunch& L, cudaStream_t st) {
     case kSumKindU8Flush: launch_k(k_sum_u8<kSumRowsPT, DD_SUM8F_NW, false, true>, grid, smem, L, st); break;
     case kSumKindU8: launch_k(k_sum_u8<kSumRowsPT, DD_SUM8_NW, false, false>, grid, smem, L, st); break;
     case kSumKindU16: launch_k(k_sum_u16<kSumRows, DD_SUM16_NW>, grid, smem, L, st); break;
-    case kSumKindU16Wide: launch_k(k_sum_u16w<kSumRows, DD_SUM16W_NW>, grid, smem, L, st); break;
+    case kSumKindU16Wide: launch_k(k_sum_u16w<kSumRowsPTW, DD_SUM16W_NW>, grid, smem, L, st); break;
     case kSumKindU16Quad: launch_k(k_sum_u16q<kSumRowsPTQ, kSum16QNW>, grid, smem, L, st); break;
     case kSumKindU16Twin: launch_k(k_sum_u16t<kSumRowsPTT, kSum16TNW>, grid, smem, L, st); break;
     default: launch_k(k_sum_u32<kSumRows, kSum32NW>, grid, smem, L, st); break;
@@ -1364,9 +1369,7 @@ int sum_batch_blocks_per_sm(size_t smem) {
 void launch_sum_batch(const SumBatchGroup* d_groups, int ngroups, long long total, int* d_ctrs,
                       unsigned long long* d_next, int* d_err, size_t smem, unsigned grid,
                       cudaStream_t st) {
-  if (smem > 48 * 1024)
-    DD_CUDA_TRY(cudaFuncSetAttribute(k_sum_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
+  allow_dynamic_smem(k_sum_batch, smem);
   k_sum_batch<<<grid, kThreads, smem, st>>>(d_groups, ngroups, total, d_ctrs, d_next, d_err);
   DD_LAUNCHED();
 }
@@ -1374,10 +1377,7 @@ void launch_sum_batch(const SumBatchGroup* d_groups, int ngroups, long long tota
 template <int KIND>
 void launch_grouped_k(const SumBatchGroup* d_groups, int ngroups, long long total, size_t smem,
                       cudaStream_t st) {
-  if (smem > 48 * 1024)
-    DD_CUDA_TRY(cudaFuncSetAttribute(k_sum_grouped<KIND>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
+  allow_dynamic_smem(k_sum_grouped<KIND>, smem);
   k_sum_grouped<KIND><<<static_cast<unsigned>(total), kThreads, smem, st>>>(d_groups, ngroups);
   DD_LAUNCHED();
 }
@@ -1416,9 +1416,7 @@ void launch_pair_k(const SumLaunch& L1, const SumLaunch& L2, cudaStream_t st) {
   const long long n2 = static_cast<long long>(gx2) * L2.grid_y * L2.grid_z;
   const size_t smem = std::max(sum_launch_smem(L1), sum_launch_smem(L2));
   if (n1 + n2 >= (1LL << 31)) throw Error{DD_ERR_RUNTIME, "paired launch too large"};
-  if (smem > 48 * 1024)
-    DD_CUDA_TRY(cudaFuncSetAttribute(k_sum_pair<K1, K2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
+  allow_dynamic_smem(k_sum_pair<K1, K2>, smem);
   k_sum_pair<K1, K2><<<static_cast<unsigned>(n1 + n2), kThreads, smem, st>>>(L1, L2, n1, n2, gx1, gx2);
   DD_LAUNCHED();
 }
