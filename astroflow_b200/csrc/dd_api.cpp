@@ -430,6 +430,11 @@ void create_subband(dd_plan& P) {
   set_tiling(P, int64_t(DD_INTER_MB) << 20);
   if (ds > 1 || callsite_zdm_active(P))
     P.d_binned.alloc(static_cast<size_t>(P.nbin * P.hdr.nchans) * P.elem);
+  if (ds > 1 && binning_lut_entries(P.nbits, ds)) {
+    P.d_bin_lut.alloc(static_cast<size_t>(binning_lut_entries(P.nbits, ds)) * P.elem);
+    launch_binning_lut(P.d_bin_lut.p, P.nbits, ds, cudaStreamLegacy);
+    DD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
+  }
   P.adds = static_cast<double>(P.ndm_nom) * P.dch * P.nout +
            static_cast<double>(P.dm_steps) * P.nsb * P.nout;
 }
@@ -524,7 +529,8 @@ void run_rfi_and_prep(dd_plan& P, const void* input, uint8_t* masks_out, uint32_
   const void* src = input;
   const int ds = P.p.time_downsample;
   if (ds > 1) {
-    launch_time_binning(input, P.d_binned.p, P.nbits, P.nin, n, ds, st);
+    launch_time_binning(input, P.d_binned.p, P.nbits, P.nin, n, ds,
+                        P.d_bin_lut.bytes ? P.d_bin_lut.p : nullptr, st);
     src = P.d_binned.p;
   }
   const bool callsite = callsite_zdm_active(P);
@@ -848,7 +854,7 @@ void check_device_error(dd_plan& P, cudaStream_t st) {
 
 int64_t workspace_of(const dd_plan& P) {
   const DevBuf* bufs[] = {&P.d_delay, &P.d_res, &P.d_lags, &P.d_bad_keep, &P.d_win, &P.d_seg_t0,
-                          &P.d_binned, &P.d_x, &P.d_inter, &P.d_stats, &P.d_iqrm_scratch,
+                          &P.d_binned, &P.d_bin_lut, &P.d_x, &P.d_inter, &P.d_stats, &P.d_iqrm_scratch,
                           &P.d_masks, &P.d_segmask, &P.d_zdm, &P.d_desc1, &P.d_desc2,
                           &P.d_descb, &P.d_err};
   int64_t t = 0;

@@ -113,6 +113,7 @@ struct dd_plan {
   dd::DevBuf d_host_in, d_host_out;  // device side of dd_run_host (kept across calls)
   cudaStream_t copy_stream = nullptr; // dd_run_host: output copies overlapping the sums
   dd::DevBuf d_inter;    // stage-1 tile (two buffers in a DD_PAIR_STAGES build)
+  dd::DevBuf d_bin_lut;  // full-bin values of the time binning (8/16-bit samples, ds > 1)
   int64_t inter_bytes = 0; // bytes of one buffer
   int64_t inter_budget = 0; // subband-sum bytes per time tile the tiling was set for
   int stages_override = 0;  // staged source pairs in flight (0: as many as fit)
@@ -152,8 +153,14 @@ void launch_zdm_range_mean(const void* x, int nbits, int64_t nsamp, int64_t ncha
                            int nseg, float* d_mean, cudaStream_t st);
 
 // ---- RFI and layout (dd_rfi.cu) ----
+// Time binning (dedispered.cu:337-376).  lut: the plan's table of full-bin values
+// (launch_binning_lut; nullptr evaluates every bin directly).
 void launch_time_binning(const void* in, void* out, int nbits, int64_t ndata, int64_t nchans,
-                         int ds, cudaStream_t st);
+                         int ds, const void* lut, cudaStream_t st);
+// Entries of the full-bin table for these samples and bin width (0: no table).
+int64_t binning_lut_entries(int nbits, int ds);
+// Fills the full-bin table: lut[sum] for every sum of ds samples.
+void launch_binning_lut(void* lut, int nbits, int ds, cudaStream_t st);
 // d_win: [nwin][2] (t0, t1); d_sums: [nwin][2][csub] (sum, sum of squares).
 void launch_iqrm_stats(const void* x, int nbits, int64_t nsamp, int64_t nchans, int64_t cs,
                        int64_t csub, const uint32_t* d_win, int nwin,

@@ -56,6 +56,58 @@ __global__ void k_time_binning(const T* __restrict__ in, T* __restrict__ out, in
   }
 }
 
+// The value of a full bin depends only on the integer sum of its ds samples, so
+// for 8- and 16-bit samples every value is tabulated once per plan (lut[sum],
+// sum in [0, ds * vmax]) by the same expression as k_time_binning, and the
+// binning becomes a gather: V channels per thread (V * sizeof(T) = 4 bytes, one
+// word per load and store).  A last, partial bin uses the expression directly.
+template <typename T>
+__global__ void k_binning_lut(T* __restrict__ lut, int64_t n, double smax_full) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t vmax = Lim<T>::vmax;
+  const double s = sqrt(static_cast<double>(i));
+  const double v = __dmul_rn(__ddiv_rn(s, smax_full > 0.0 ? smax_full : 1.0), static_cast<double>(vmax));
+  lut[i] = static_cast<T>(v < static_cast<double>(vmax) ? v : static_cast<double>(vmax));
+}
+
+template <typename T>
+__device__ __forceinline__ T binned_value(uint64_t sum, uint64_t cnt) {
+  const uint64_t vmax = Lim<T>::vmax;
+  const double s = sqrt(static_cast<double>(sum));
+  const double smax = sqrt(static_cast<double>(vmax * (cnt ? cnt : 1)));
+  const double v = __dmul_rn(__ddiv_rn(s, smax > 0.0 ? smax : 1.0), static_cast<double>(vmax));
+  return static_cast<T>(v < static_cast<double>(vmax) ? v : static_cast<double>(vmax));
+}
+
+template <typename T>
+__global__ void k_time_binning_lut(const T* __restrict__ in, T* __restrict__ out, int64_t nchans,
+                                   int64_t ndata, int ds, int64_t nout, const T* __restrict__ lut) {
+  constexpr int V = 4 / sizeof(T);
+  const int64_t c = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * V;
+  if (c >= nchans) return;
+  for (int64_t k = blockIdx.y; k < nout; k += gridDim.y) {
+    const int64_t t0 = k * ds;
+    const int64_t t1 = t0 + ds < ndata ? t0 + ds : ndata;
+    uint32_t sum[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) sum[v] = 0;
+    for (int64_t t = t0; t < t1; ++t) {
+      const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(in + t * nchans + c));
+#pragma unroll
+      for (int v = 0; v < V; ++v) sum[v] += (w >> (8 * sizeof(T) * v)) & static_cast<uint32_t>(Lim<T>::vmax);
+    }
+    const bool full = t1 - t0 == ds;
+    uint32_t o = 0;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const T b = full ? __ldg(lut + sum[v]) : binned_value<T>(sum[v], static_cast<uint64_t>(t1 - t0));
+      o |= static_cast<uint32_t>(b) << (8 * sizeof(T) * v);
+    }
+    *reinterpret_cast<uint32_t*>(out + k * nchans + c) = o;
+  }
+}
+
 // ---------------------------------------------------------------- IQRM sums
 // Block: 256 consecutive channels of [cs, cs+csub); grid.y: time chunks.
 template <typename T>
@@ -560,9 +612,40 @@ __global__ void k_prep_full(PrepArgs a) {
 
 }  // namespace
 
+int64_t binning_lut_entries(int nbits, int ds) {
+  if (nbits != 8 && nbits != 16) return 0;
+  const int64_t n = static_cast<int64_t>(ds) * (nbits == 8 ? 255 : 65535) + 1;
+  return n <= (int64_t(1) << 24) ? n : 0;
+}
+
+void launch_binning_lut(void* lut, int nbits, int ds, cudaStream_t st) {
+  const int64_t n = binning_lut_entries(nbits, ds);
+  if (!n) throw Error{DD_ERR_RUNTIME, "no binning table for these samples"};
+  const uint64_t vmax = nbits == 8 ? 255u : 65535u;
+  const double smax_full = std::sqrt(static_cast<double>(vmax * static_cast<uint64_t>(ds)));
+  const unsigned grid = static_cast<unsigned>((n + 255) / 256);
+  if (nbits == 8) k_binning_lut<uint8_t><<<grid, 256, 0, st>>>(static_cast<uint8_t*>(lut), n, smax_full);
+  else k_binning_lut<uint16_t><<<grid, 256, 0, st>>>(static_cast<uint16_t*>(lut), n, smax_full);
+  DD_LAUNCHED();
+}
+
 void launch_time_binning(const void* in, void* out, int nbits, int64_t ndata, int64_t nchans,
-                         int ds, cudaStream_t st) {
+                         int ds, const void* lut, cudaStream_t st) {
   const int64_t nout = (ndata + ds - 1) / ds;
+  if (lut && (nbits == 8 || nbits == 16) && nchans % (32 / nbits) == 0 &&
+      reinterpret_cast<uintptr_t>(in) % 4 == 0 && reinterpret_cast<uintptr_t>(out) % 4 == 0) {
+    const int64_t nthreads = nchans / (32 / nbits);
+    const dim3 g(static_cast<unsigned>((nthreads + 255) / 256),
+                 static_cast<unsigned>(std::min<int64_t>(nout, 65535)));
+    if (nbits == 8)
+      k_time_binning_lut<uint8_t><<<g, 256, 0, st>>>(static_cast<const uint8_t*>(in), static_cast<uint8_t*>(out),
+                                                     nchans, ndata, ds, nout, static_cast<const uint8_t*>(lut));
+    else
+      k_time_binning_lut<uint16_t><<<g, 256, 0, st>>>(static_cast<const uint16_t*>(in), static_cast<uint16_t*>(out),
+                                                      nchans, ndata, ds, nout, static_cast<const uint16_t*>(lut));
+    DD_LAUNCHED();
+    return;
+  }
   const dim3 grid(static_cast<unsigned>((nchans + 255) / 256),
                   static_cast<unsigned>(std::min<int64_t>(nout, 65535)));
   const uint64_t vmax = nbits == 8 ? 255u : nbits == 16 ? 65535u : 4294967295u;
