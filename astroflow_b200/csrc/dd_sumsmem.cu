@@ -813,13 +813,21 @@ __device__ __forceinline__ void sum_u16(const SumLaunch& L, uint3 blk, uint32_t*
   }
 }
 
+// DD_SUM16W_WHOLE 1: each 32-bit pair of samples is aligned by one byte permute and
+// summed whole (wrapping) beside the sum of its high halves; 0: low and high
+// halves are taken apart per word by masks and shifts chosen by the offset.
+#ifndef DD_SUM16W_WHOLE
+#define DD_SUM16W_WHOLE 1
+#endif
 // 16-bit samples into 32-bit sums (stage 1 and brute force of 16-bit input).
-// A 16-bit sample sits in the low or high half of a window word, so no funnel
-// shift is needed: for output word k (samples 2k, 2k+1 of the block) a source
-// whose offset is word-aligned gives (w[k] & 0xffff, w[k] >> 16) and one offset
-// by a sample gives (w[k] >> 16, w[k+1] & 0xffff).  The high halves are taken
-// with a multiply-high on the FMA pipe, the low ones with a mask on the integer
-// pipe, and two sources are added per three-input add.
+// For output word k (samples 2k, 2k+1 of the block) a source whose offset is
+// word-aligned gives the pair w[k] and one offset by a sample the pair
+// (w[k] >> 16, w[k+1] & 0xffff), one byte permute of two words (selector 0x3210
+// or 0x5432, so no branch separates a row's sources).  The aligned pairs are
+// summed whole into a wrapping 32-bit word and their high halves into another
+// (two sources per three-input add); the low samples' sums come out at the end
+// as whole - (high << 16).  Three integer-pipe operations per word and source,
+// where taking the halves apart by masks and offset-dependent selects took five.
 template <int RB, int NW>
 __device__ __forceinline__ void sum_u16_wide(const SumLaunch& L, uint3 blk, uint32_t* sw, Pipe& P) {
   // RB rows per thread: the block's rows are split over kSumRows/RB warp groups,
@@ -856,20 +864,42 @@ __device__ __forceinline__ void sum_u16_wide(const SumLaunch& L, uint3 blk, uint
           vb[i] = w1[kStride * (NW - 1) + 1];
         }
       }
+      if constexpr (DD_SUM16W_WHOLE) {
+        // rw.y / rw.w: 0 (word-aligned) or 16 (one sample in): one byte permute
+        // aligns the pair; whole words are summed (wrapping) and high halves apart
+        const uint32_t sa = rw.y ? 0x5432u : 0x3210u, sb = rw.w ? 0x5432u : 0x3210u;
 #pragma unroll
-      for (int k = 0; k < NW; ++k) {
-        const uint32_t an = kConsec ? va[k + 1] : w0[kStride * k + 1];
-        const uint32_t bn = kConsec ? vb[k + 1] : w1[kStride * k + 1];
-        // rw.y / rw.w: 0 (word-aligned) or 16 (one sample in)
-        const uint32_t alo = rw.y ? __umulhi(va[k], 0x10000u) : (va[k] & 0xffffu);
-        const uint32_t ahi = rw.y ? (an & 0xffffu) : __umulhi(va[k], 0x10000u);
-        const uint32_t blo = rw.w ? __umulhi(vb[k], 0x10000u) : (vb[k] & 0xffffu);
-        const uint32_t bhi = rw.w ? (bn & 0xffffu) : __umulhi(vb[k], 0x10000u);
-        lo32[r][k] += alo + blo;
-        hi32[r][k] += ahi + bhi;
+        for (int k = 0; k < NW; ++k) {
+          const uint32_t an = kConsec ? va[k + 1] : w0[kStride * k + 1];
+          const uint32_t bn = kConsec ? vb[k + 1] : w1[kStride * k + 1];
+          const uint32_t a = __byte_perm(va[k], an, sa), b = __byte_perm(vb[k], bn, sb);
+          lo32[r][k] += a + b;
+          hi32[r][k] += (a >> 16) + (b >> 16);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+          const uint32_t an = kConsec ? va[k + 1] : w0[kStride * k + 1];
+          const uint32_t bn = kConsec ? vb[k + 1] : w1[kStride * k + 1];
+          // rw.y / rw.w: 0 (word-aligned) or 16 (one sample in)
+          const uint32_t alo = rw.y ? __umulhi(va[k], 0x10000u) : (va[k] & 0xffffu);
+          const uint32_t ahi = rw.y ? (an & 0xffffu) : __umulhi(va[k], 0x10000u);
+          const uint32_t blo = rw.w ? __umulhi(vb[k], 0x10000u) : (vb[k] & 0xffffu);
+          const uint32_t bhi = rw.w ? (bn & 0xffffu) : __umulhi(vb[k], 0x10000u);
+          lo32[r][k] += alo + blo;
+          hi32[r][k] += ahi + bhi;
+        }
       }
     }
   });
+  if constexpr (DD_SUM16W_WHOLE) {
+    // lo32 holds sum(low) + 2^16 sum(high) mod 2^32 and sum(low) < 2^32 (at most
+    // 65537 sources of 65535), so the low sums are lo32 - (hi32 << 16)
+#pragma unroll
+    for (int r = 0; r < RB; ++r)
+#pragma unroll
+      for (int k = 0; k < NW; ++k) lo32[r][k] -= hi32[r][k] << 16;
+  }
   if (P.failed) return;
 #pragma unroll
   for (int r = 0; r < RB; ++r) {
