@@ -381,10 +381,11 @@ constexpr int kSum32NW = DD_SUM32_NW;  // words per lane of the 32-bit staged su
 #endif
 // Warp groups the block's rows are split over in the 16-bit-into-32-bit kernel,
 // blocks per SM it is built for and the shared memory (KB) it stays within.  Two
-// warp groups of four rows at three blocks per SM took stage 1 of the
-// 8192-channel 16-bit case on 2^18 samples (DM 0:0.25:500) from 35.4 to 30.6 ms
-// but the full configuration (2^21 samples, three ranges) from 498 to 522 ms, so
-// one group at two blocks per SM stays the default.
+// warp groups of four rows at three blocks per SM take stage 1 of the
+// 8192-channel 16-bit case on 2^18 samples (DM 0:0.25:500) from 29.5 to 24.5 ms
+// but leave the full configuration (2^21 samples, three ranges) unchanged (first
+// range 194.8 against 195.6 ms), so one group at two blocks per SM stays the
+// default.
 #ifndef DD_SUM16W_ROWSPLIT
 #define DD_SUM16W_ROWSPLIT 1
 #endif
