@@ -59,6 +59,9 @@ BRUTE = [
     (50, 5000, 8, 1.26646875e-3, 1130.0, 1.0, 10.0, 600.0, 1.0, 1, 0.5),
     (33, 1500, 32, 64e-6, 1300.0, 2.0, 0.0, 300.0, 1.5, 1, 0.04),
     (300, 1024, 8, 64e-6, 1000.0, 1.6, 0.0, 50.0, 0.5, 4, 0.0655),
+    # 16-bit samples through the staged 32-bit sums: 512 full-range channels, so the
+    # whole-pair sum wraps many times before the low halves are recovered
+    (512, 3000, 16, 64e-6, 1000.0, 0.9, 0.0, 200.0, 1.0, 1, 0.1),
 ]
 
 
