@@ -16,16 +16,18 @@
 // which reach shared memory by bulk copies of 32 sources, a chunk ahead, so the
 // producer only unpacks them (one lane per source and row).
 //
-// Summing: lanes own interleaved 32-bit output words (lane l: words l, l+32, ...),
-// so each shared load touches 32 consecutive words, free of bank conflicts; a
-// shift that is not a multiple of 4 bytes costs one funnel shift of two words.
-// 8-bit samples are split into two 16-bit-lane words by byte permutes and two
-// sources are added by one three-input add (four sample additions per add);
-// with more than 256 sources the lanes are added into the 32-bit output every
-// 256 sources (the block owns its output tile, so it reads back its own sums).
-// 16-bit samples are added as lane pairs and widened before they can overflow;
-// 16-bit stage-1 sums are added four at a time (sum_u16_quad).  A missing
-// source (source count not a multiple of the group) reads a zeroed window.
+// Summing: lanes own 32-bit output words (an odd number of consecutive words, or
+// interleaved words l, l+32, ...), so a warp's shared loads are free of bank
+// conflicts; a shift that is not a multiple of 4 bytes costs one funnel shift of
+// two words.  8-bit samples are split into two 16-bit-lane words by byte
+// permutes; 16-bit stage-1 sums come with a twin shifted by one sample so that
+// stage 2 reads aligned words only (sum_u16_twin), four sources at a time in
+// packed 16-bit lanes; 16-bit samples are aligned pairwise and summed whole
+// beside their high halves (sum_u16_wide).  Outputs leave through shared memory
+// as 16-byte chunks where a lane's words are scattered (16-bit stage-1 sums and
+// their twin; the 32-bit flushes of 8-bit sums of more than 256 sources, which
+// read back the block's own partial sums).  A missing source (source count not
+// a multiple of the group) reads a zeroed window.
 //
 // Every wait on an mbarrier is bounded (about two seconds of SM clock); a wait
 // that gives up records an error code in L.err and the block stops summing, and
