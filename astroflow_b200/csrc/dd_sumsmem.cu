@@ -1462,6 +1462,7 @@ bool launch_sum_pair(const SumLaunch& L1, const SumLaunch& L2, cudaStream_t st) 
   const int k1 = sum_kind(L1), k2 = sum_kind(L2);
   if (k1 == kSumKindU8 && k2 == kSumKindU32) launch_pair_k<kSumKindU8, kSumKindU32>(L1, L2, st);
   else if (k1 == kSumKindU8Out16 && k2 == kSumKindU16Quad) launch_pair_k<kSumKindU8Out16, kSumKindU16Quad>(L1, L2, st);
+  else if (k1 == kSumKindU8Out16 && k2 == kSumKindU16Twin) launch_pair_k<kSumKindU8Out16, kSumKindU16Twin>(L1, L2, st);
   else if (k1 == kSumKindU16Wide && k2 == kSumKindU32) launch_pair_k<kSumKindU16Wide, kSumKindU32>(L1, L2, st);
   else if (k1 == kSumKindU8Flush && k2 == kSumKindU32) launch_pair_k<kSumKindU8Flush, kSumKindU32>(L1, L2, st);
   else return false;
