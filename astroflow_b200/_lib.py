@@ -28,7 +28,8 @@ FREQ_HEADER, FREQ_FIL = 0, 1
 # Every symbol include/astroflow_dd.h declares.
 EXPORTS = ("dd_plan_create", "dd_plan_destroy", "dd_plan_destroy_async", "dd_plan_get_info",
            "dd_plan_get_tables", "dd_brute_delay_table",
-           "dd_plan_set_delay_table", "dd_run", "dd_run_ex", "dd_run_host", "dd_run_profiled",
+           "dd_plan_set_delay_table", "dd_run", "dd_run_ex", "dd_run_host", "dd_run_host_async",
+           "dd_run_host_join", "dd_run_profiled",
            "dd_measure_int_add_rate", "dd_iqrm_masks_noalloc", "dd_batch_create",
            "dd_batch_run", "dd_batch_status", "dd_batch_get_info", "dd_batch_destroy",
            "dd_stream_open", "dd_stream_push", "dd_stream_get_info", "dd_stream_plan",
@@ -146,6 +147,8 @@ def load():
     L.dd_run.argtypes = [P, P, P, P]
     L.dd_run_ex.argtypes = [P, P, P, P, P, P, P]
     L.dd_run_host.argtypes = [P, P, P, P]
+    L.dd_run_host_async.argtypes = [P, P, P, P]
+    L.dd_run_host_join.argtypes = [P, P, ctypes.c_int32]
     L.dd_run_profiled.argtypes = [P, P, P, P, ctypes.POINTER(RunStats)]
     L.dd_measure_int_add_rate.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
     L.dd_iqrm_masks_noalloc.argtypes = [P, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32,

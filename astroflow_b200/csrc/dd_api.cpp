@@ -676,12 +676,16 @@ SumLaunch stage2_launch(const dd_plan& P, int64_t t0, void* output, int buf = 0)
 // [t0, t0 + cols) of every DM row has been queued on the stream.
 using TileHook = std::function<void(int64_t, int64_t)>;
 
+// before_sums: called once the RFI stages and the layout are queued, before the
+// first sum that writes `output`.
 void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out,
                  uint32_t* bounds_out, void* prepped, cudaStream_t st, Prof* pf = nullptr,
-                 const TileHook& after_tile = TileHook()) {
+                 const TileHook& after_tile = TileHook(),
+                 const std::function<void()>& before_sums = std::function<void()>()) {
   cudaEvent_t a = pf ? pf->mark() : nullptr;
   run_rfi_and_prep(P, input, masks_out, bounds_out, prepped, st);
   if (pf) pf->prep.emplace_back(a, pf->mark());
+  if (before_sums) before_sums();
   // With DD_PAIR_STAGES, stage 1 of tile k+1 shares a launch with stage 2 of tile
   // k (alternating subband-sum buffers).  Measured on B200 at the headline size it
   // is no faster than running the stages one after another (148.6 vs 145.8 ms per
@@ -1239,68 +1243,122 @@ int dd_measure_int_add_rate(int32_t device, double* adds_per_second) {
   });
 }
 
+namespace {
+// Queues one host-path run on `st`: input copy, run, output copies (each time
+// tile's columns on the plan's copy stream while the next tile is summed).  The
+// run's sums wait for the output copies an earlier queued run left on the copy
+// stream (they write the same device output), its input copy and RFI stages do
+// not: consecutive runs overlap one run's output copy with the next one's input
+// copy.  P.host_done marks this run's last output copy.
+void enqueue_host_run(dd_plan& P, const void* h_input, void* h_output, cudaStream_t st) {
+  const size_t in_bytes = static_cast<size_t>(P.nin * P.hdr.nchans) * P.elem;
+  const int64_t cols = P.p.algorithm == DD_ALGO_BRUTE ? P.out_cols : P.nout;
+  const size_t oelem = P.nbits == 32 ? 8 : 4;
+  const size_t out_bytes = static_cast<size_t>(P.dm_steps) * cols * oelem;
+  // device buffers of the host path, kept by the plan across calls
+  if (P.d_host_in.bytes < in_bytes || P.d_host_out.bytes < out_bytes) {
+    // earlier queued runs may still use the old buffers
+    if (P.copy_stream) DD_CUDA_TRY(cudaStreamSynchronize(P.copy_stream));
+    DD_CUDA_TRY(cudaStreamSynchronize(st));
+    P.host_pending = false;
+  }
+  if (P.d_host_in.bytes < in_bytes) P.d_host_in.alloc(in_bytes);
+  if (P.d_host_out.bytes < out_bytes) {
+    P.d_host_out.release();
+    try {
+      P.d_host_out.alloc(out_bytes);
+    } catch (const Error& er) {
+      throw Error{DD_ERR_NOMEM, "output allocation failed: " + er.msg};
+    }
+  }
+  // buffers are allocated stream-ordered on the legacy stream: make them visible to `st`
+  DD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
+  char* d_out = P.d_host_out.as<char>();
+  if (!P.copy_stream) DD_CUDA_TRY(cudaStreamCreateWithFlags(&P.copy_stream, cudaStreamNonBlocking));
+  if (!P.host_done) DD_CUDA_TRY(cudaEventCreateWithFlags(&P.host_done, cudaEventDisableTiming));
+  auto wait_output_free = [&]() {
+    if (P.host_pending) DD_CUDA_TRY(cudaStreamWaitEvent(st, P.host_done, 0));
+  };
+  DD_CUDA_TRY(cudaMemcpyAsync(P.d_host_in.p, h_input, in_bytes, cudaMemcpyHostToDevice, st));
+  if (P.p.algorithm == DD_ALGO_BRUTE) {
+    wait_output_free();
+    run_brute(P, P.d_host_in.p, d_out, nullptr, st);
+    cudaEvent_t ev;
+    DD_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    DD_CUDA_TRY(cudaEventRecord(ev, st));
+    DD_CUDA_TRY(cudaStreamWaitEvent(P.copy_stream, ev, 0));
+    cudaEventDestroy(ev);
+    DD_CUDA_TRY(cudaMemcpyAsync(h_output, d_out, out_bytes, cudaMemcpyDeviceToHost, P.copy_stream));
+  } else {
+    std::vector<cudaEvent_t> evs;
+    auto cleanup = [&]() {
+      for (cudaEvent_t ev : evs) cudaEventDestroy(ev);
+    };
+    try {
+      run_subband(P, P.d_host_in.p, d_out, nullptr, nullptr, nullptr, st, nullptr,
+                  [&](int64_t t0, int64_t n) {
+                    cudaEvent_t ev;
+                    DD_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+                    evs.push_back(ev);
+                    DD_CUDA_TRY(cudaEventRecord(ev, st));
+                    DD_CUDA_TRY(cudaStreamWaitEvent(P.copy_stream, ev, 0));
+                    const size_t pitch = static_cast<size_t>(cols) * oelem;
+                    DD_CUDA_TRY(cudaMemcpy2DAsync(static_cast<char*>(h_output) + t0 * oelem, pitch,
+                                                  d_out + t0 * oelem, pitch, n * oelem,
+                                                  static_cast<size_t>(P.dm_steps),
+                                                  cudaMemcpyDeviceToHost, P.copy_stream));
+                  },
+                  wait_output_free);
+    } catch (...) {
+      cudaStreamSynchronize(P.copy_stream);
+      cleanup();
+      P.host_pending = false;
+      throw;
+    }
+    cleanup();
+  }
+  DD_CUDA_TRY(cudaEventRecord(P.host_done, P.copy_stream));
+  P.host_pending = true;
+}
+
+// Makes `st` wait for every host-path output copy queued so far.
+void join_host_runs(dd_plan& P, cudaStream_t st) {
+  if (P.host_pending) DD_CUDA_TRY(cudaStreamWaitEvent(st, P.host_done, 0));
+}
+}  // namespace
+
 int dd_run_host(dd_plan* P, const void* h_input, void* h_output, void* stream) {
   if (!P || !h_input || !h_output) { set_error("NULL argument"); return DD_ERR_INVALID; }
   return guarded([&] {
     DeviceGuard g(P->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const size_t in_bytes = static_cast<size_t>(P->nin * P->hdr.nchans) * P->elem;
-    const int64_t cols = P->p.algorithm == DD_ALGO_BRUTE ? P->out_cols : P->nout;
-    const size_t oelem = P->nbits == 32 ? 8 : 4;
-    const size_t out_bytes = static_cast<size_t>(P->dm_steps) * cols * oelem;
-    // device buffers of the host path, kept by the plan across calls
-    if (P->d_host_in.bytes < in_bytes) P->d_host_in.alloc(in_bytes);
-    if (P->d_host_out.bytes < out_bytes) {
-      P->d_host_out.release();
-      try {
-        P->d_host_out.alloc(out_bytes);
-      } catch (const Error& er) {
-        throw Error{DD_ERR_NOMEM, "output allocation failed: " + er.msg};
-      }
-    }
-    // buffers are allocated stream-ordered on the legacy stream: make them visible to `st`
-    DD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
-    char* d_out = P->d_host_out.as<char>();
-    DD_CUDA_TRY(cudaMemcpyAsync(P->d_host_in.p, h_input, in_bytes, cudaMemcpyHostToDevice, st));
-    if (P->p.algorithm == DD_ALGO_BRUTE) {
-      run_brute(*P, P->d_host_in.p, d_out, nullptr, st);
-      DD_CUDA_TRY(cudaMemcpyAsync(h_output, d_out, out_bytes, cudaMemcpyDeviceToHost, st));
-    } else {
-      // each time tile's output columns go to the host on a second stream while
-      // the next tile is summed
-      if (!P->copy_stream) DD_CUDA_TRY(cudaStreamCreateWithFlags(&P->copy_stream, cudaStreamNonBlocking));
-      std::vector<cudaEvent_t> evs;
-      auto cleanup = [&]() {
-        for (cudaEvent_t ev : evs) cudaEventDestroy(ev);
-      };
-      try {
-        run_subband(*P, P->d_host_in.p, d_out, nullptr, nullptr, nullptr, st, nullptr,
-                    [&](int64_t t0, int64_t n) {
-                      cudaEvent_t ev;
-                      DD_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-                      evs.push_back(ev);
-                      DD_CUDA_TRY(cudaEventRecord(ev, st));
-                      DD_CUDA_TRY(cudaStreamWaitEvent(P->copy_stream, ev, 0));
-                      const size_t pitch = static_cast<size_t>(cols) * oelem;
-                      DD_CUDA_TRY(cudaMemcpy2DAsync(static_cast<char*>(h_output) + t0 * oelem, pitch,
-                                                    d_out + t0 * oelem, pitch, n * oelem,
-                                                    static_cast<size_t>(P->dm_steps),
-                                                    cudaMemcpyDeviceToHost, P->copy_stream));
-                    });
-        cudaEvent_t done;
-        DD_CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
-        evs.push_back(done);
-        DD_CUDA_TRY(cudaEventRecord(done, P->copy_stream));
-        DD_CUDA_TRY(cudaStreamWaitEvent(st, done, 0));
-      } catch (...) {
-        cudaStreamSynchronize(P->copy_stream);
-        cleanup();
-        throw;
-      }
-      cleanup();
-    }
+    enqueue_host_run(*P, h_input, h_output, st);
+    join_host_runs(*P, st);
     DD_CUDA_TRY(cudaStreamSynchronize(st));
+    P->host_pending = false;
     check_device_error(*P, st);
+  });
+}
+
+int dd_run_host_async(dd_plan* P, const void* h_input, void* h_output, void* stream) {
+  if (!P || !h_input || !h_output) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  return guarded([&] {
+    DeviceGuard g(P->device);
+    enqueue_host_run(*P, h_input, h_output, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int dd_run_host_join(dd_plan* P, void* stream, int32_t sync) {
+  if (!P) { set_error("NULL argument"); return DD_ERR_INVALID; }
+  return guarded([&] {
+    DeviceGuard g(P->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    join_host_runs(*P, st);
+    if (sync) {
+      DD_CUDA_TRY(cudaStreamSynchronize(st));
+      P->host_pending = false;
+      check_device_error(*P, st);
+    }
   });
 }
 

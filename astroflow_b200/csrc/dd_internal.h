@@ -112,6 +112,8 @@ struct dd_plan {
   dd::DevBuf d_x;        // prepared channel-major input
   dd::DevBuf d_host_in, d_host_out;  // device side of dd_run_host (kept across calls)
   cudaStream_t copy_stream = nullptr; // dd_run_host: output copies overlapping the sums
+  cudaEvent_t host_done = nullptr;    // the last host-path output copy enqueued
+  bool host_pending = false;          // host_done marks copies a later run must wait for
   dd::DevBuf d_inter;    // stage-1 tile (two buffers in a DD_PAIR_STAGES build)
   dd::DevBuf d_bin_lut;  // full-bin values of the time binning (8/16-bit samples, ds > 1)
   int64_t inter_bytes = 0; // bytes of one buffer
@@ -133,6 +135,7 @@ struct dd_plan {
       cudaStreamSynchronize(copy_stream);
       cudaStreamDestroy(copy_stream);
     }
+    if (host_done) cudaEventDestroy(host_done);
   }
 };
 

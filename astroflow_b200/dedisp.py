@@ -202,6 +202,30 @@ class Plan:
         _lib.check(_lib.load().dd_run_host(self._h, x.ctypes.data, out.ctypes.data, h))
         return out
 
+    def run_host_async(self, x: np.ndarray, out: np.ndarray, stream=None):
+        """Queue a run of a host array through dd_run_host_async and return at once:
+        `out` holds the result after run_host_join(stream, sync=True) (or once a
+        stream joined with run_host_join(stream) has reached that point).  Chunks
+        queued one after another overlap one chunk's output copy with the next
+        one's input copy; both arrays should be in pinned memory and stay alive
+        until then."""
+        if x.dtype != _NP[self.nbits] or not x.flags.c_contiguous:
+            raise ValueError(f"input must be a C-contiguous uint{self.nbits} array")
+        if x.size < self.in_shape[0] * self.in_shape[1]:
+            raise ValueError("input holds fewer than ndata * nchans samples")
+        want = np.uint64 if self.out_bits == 64 else np.uint32
+        if out.dtype != want or out.shape != self.out_shape or not out.flags.c_contiguous:
+            raise ValueError(f"output must be a C-contiguous {want.__name__} array of shape {self.out_shape}")
+        h = None if stream is None else ctypes.c_void_p(stream.cuda_stream)
+        _lib.check(_lib.load().dd_run_host_async(self._h, x.ctypes.data, out.ctypes.data, h))
+        return out
+
+    def run_host_join(self, stream=None, sync: bool = False):
+        """Make `stream` wait for the output copies of the queued run_host_async
+        calls; with sync=True also wait on the host and report device errors."""
+        h = None if stream is None else ctypes.c_void_p(stream.cuda_stream)
+        _lib.check(_lib.load().dd_run_host_join(self._h, h, 1 if sync else 0))
+
     @property
     def closed(self) -> bool:
         return not (getattr(self, "_h", None) and self._h.value)

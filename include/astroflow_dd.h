@@ -235,6 +235,25 @@ int dd_run_ex(dd_plan* plan, const void* input, void* output, uint8_t* iqrm_mask
  * later calls and released with it. */
 int dd_run_host(dd_plan* plan, const void* h_input, void* h_output, void* stream);
 
+/* dd_run_host without waiting: queues the input copy, the run and the output
+ * copies and returns.  It has no counterpart in the reference (whose call,
+ * dedispered.cu:988-1304, blocks until its output is on the host); it serves
+ * callers that stream chunk after chunk: one chunk's output copy (device to
+ * host) overlaps the next chunk's input copy (host to device) and RFI stages,
+ * and only the next chunk's sums wait for the copy of the output they
+ * overwrite.  h_input may be reused once the call's input copy is done (the
+ * stream reaches it), h_output holds the result once dd_run_host_join has made
+ * a stream wait for it and that stream has reached that point; pinned host
+ * buffers are needed for the copies to overlap.  The calls of one plan must use
+ * one stream. */
+int dd_run_host_async(dd_plan* plan, const void* h_input, void* h_output, void* stream);
+
+/* Makes `stream` wait (without blocking the host) for every output copy the
+ * plan's dd_run_host_async calls have queued; with sync != 0 it also
+ * synchronises the stream and reports a device-side failure of those runs
+ * (a bounded wait that gave up) as dd_run_host does. */
+int dd_run_host_join(dd_plan* plan, void* stream, int32_t sync);
+
 /* Device-time breakdown of one run, measured with CUDA events on the run's
  * stream (the role of the reference's AF_DEBUG stage timers,
  * dedispered.cu:41-73, without their device-wide synchronisations). */
