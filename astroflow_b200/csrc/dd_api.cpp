@@ -678,10 +678,13 @@ using TileHook = std::function<void(int64_t, int64_t)>;
 
 // before_sums: called once the RFI stages and the layout are queued, before the
 // first sum that writes `output`.
+// before_out(t0, cols): called before the first launch that writes output
+// columns [t0, t0 + cols) of the DM rows.
 void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out,
                  uint32_t* bounds_out, void* prepped, cudaStream_t st, Prof* pf = nullptr,
                  const TileHook& after_tile = TileHook(),
-                 const std::function<void()>& before_sums = std::function<void()>()) {
+                 const std::function<void()>& before_sums = std::function<void()>(),
+                 const TileHook& before_out = TileHook()) {
   cudaEvent_t a = pf ? pf->mark() : nullptr;
   run_rfi_and_prep(P, input, masks_out, bounds_out, prepped, st);
   if (pf) pf->prep.emplace_back(a, pf->mark());
@@ -696,6 +699,7 @@ void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out
     bool paired = true;
     for (int64_t k = 1; k <= ntiles; ++k) {
       const int64_t tprev = (k - 1) * P.tile;
+      if (before_out) before_out(tprev, std::min<int64_t>(P.tile, P.nout - tprev));
       const SumLaunch s2 = stage2_launch(P, tprev, output, static_cast<int>((k - 1) & 1));
       if (k < ntiles) {
         const SumLaunch s1 = stage1_launch(P, k * P.tile, static_cast<int>(k & 1));
@@ -733,6 +737,7 @@ void run_subband(dd_plan& P, const void* input, void* output, uint8_t* masks_out
       launch_stage1(s1, st);
     }
     if (pf) pf->s1.emplace_back(b1, pf->mark());
+    if (before_out) before_out(t0, std::min<int64_t>(P.tile, P.nout - t0));
     cudaEvent_t b2 = pf ? pf->mark() : nullptr;
     if (P.win2) {
       launch_sum(stage2_launch(P, t0, output), st);
@@ -1245,11 +1250,12 @@ int dd_measure_int_add_rate(int32_t device, double* adds_per_second) {
 
 namespace {
 // Queues one host-path run on `st`: input copy, run, output copies (each time
-// tile's columns on the plan's copy stream while the next tile is summed).  The
-// run's sums wait for the output copies an earlier queued run left on the copy
-// stream (they write the same device output), its input copy and RFI stages do
+// tile's columns on the plan's copy stream while the next tile is summed).  Each
+// time tile's sums wait for the earlier queued run's copy of the same output
+// columns (they write the same device output), the input copy and RFI stages do
 // not: consecutive runs overlap one run's output copy with the next one's input
-// copy.  P.host_done marks this run's last output copy.
+// copy, and the output copies run back to back.  P.host_done marks this run's
+// last output copy.
 void enqueue_host_run(dd_plan& P, const void* h_input, void* h_output, cudaStream_t st) {
   const size_t in_bytes = static_cast<size_t>(P.nin * P.hdr.nchans) * P.elem;
   const int64_t cols = P.p.algorithm == DD_ALGO_BRUTE ? P.out_cols : P.nout;
@@ -1290,16 +1296,23 @@ void enqueue_host_run(dd_plan& P, const void* h_input, void* h_output, cudaStrea
     cudaEventDestroy(ev);
     DD_CUDA_TRY(cudaMemcpyAsync(h_output, d_out, out_bytes, cudaMemcpyDeviceToHost, P.copy_stream));
   } else {
-    std::vector<cudaEvent_t> evs;
+    // each tile's sums wait only for the earlier run's copy of the same columns
+    // (events kept per tile; any other tiling waits for the earlier run's last copy)
+    std::vector<cudaEvent_t> evs, copied;
     auto cleanup = [&]() {
       for (cudaEvent_t ev : evs) cudaEventDestroy(ev);
+      for (cudaEvent_t ev : copied) cudaEventDestroy(ev);
     };
+    const bool same_tiling = P.host_pending && P.host_tile == P.tile &&
+                             P.host_tile_copied.size() == static_cast<size_t>((P.nout + P.tile - 1) / P.tile);
     try {
       run_subband(P, P.d_host_in.p, d_out, nullptr, nullptr, nullptr, st, nullptr,
                   [&](int64_t t0, int64_t n) {
-                    cudaEvent_t ev;
+                    cudaEvent_t ev, done;
                     DD_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
                     evs.push_back(ev);
+                    DD_CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+                    copied.push_back(done);
                     DD_CUDA_TRY(cudaEventRecord(ev, st));
                     DD_CUDA_TRY(cudaStreamWaitEvent(P.copy_stream, ev, 0));
                     const size_t pitch = static_cast<size_t>(cols) * oelem;
@@ -1307,15 +1320,25 @@ void enqueue_host_run(dd_plan& P, const void* h_input, void* h_output, cudaStrea
                                                   d_out + t0 * oelem, pitch, n * oelem,
                                                   static_cast<size_t>(P.dm_steps),
                                                   cudaMemcpyDeviceToHost, P.copy_stream));
+                    DD_CUDA_TRY(cudaEventRecord(done, P.copy_stream));
                   },
-                  wait_output_free);
+                  [&]() {
+                    if (!same_tiling) wait_output_free();
+                  },
+                  [&](int64_t t0, int64_t) {
+                    if (same_tiling)
+                      DD_CUDA_TRY(cudaStreamWaitEvent(st, P.host_tile_copied[t0 / P.tile], 0));
+                  });
     } catch (...) {
       cudaStreamSynchronize(P.copy_stream);
       cleanup();
       P.host_pending = false;
       throw;
     }
-    cleanup();
+    for (cudaEvent_t ev : evs) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : P.host_tile_copied) cudaEventDestroy(ev);
+    P.host_tile_copied.swap(copied);
+    P.host_tile = P.tile;
   }
   DD_CUDA_TRY(cudaEventRecord(P.host_done, P.copy_stream));
   P.host_pending = true;

@@ -114,6 +114,8 @@ struct dd_plan {
   cudaStream_t copy_stream = nullptr; // dd_run_host: output copies overlapping the sums
   cudaEvent_t host_done = nullptr;    // the last host-path output copy enqueued
   bool host_pending = false;          // host_done marks copies a later run must wait for
+  std::vector<cudaEvent_t> host_tile_copied;  // per time tile: its output copy of the last run
+  int64_t host_tile = 0;                      // the time tile those copies were made with
   dd::DevBuf d_inter;    // stage-1 tile (two buffers in a DD_PAIR_STAGES build)
   dd::DevBuf d_bin_lut;  // full-bin values of the time binning (8/16-bit samples, ds > 1)
   int64_t inter_bytes = 0; // bytes of one buffer
@@ -136,6 +138,7 @@ struct dd_plan {
       cudaStreamDestroy(copy_stream);
     }
     if (host_done) cudaEventDestroy(host_done);
+    for (cudaEvent_t e : host_tile_copied) cudaEventDestroy(e);
   }
 };
 

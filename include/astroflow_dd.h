@@ -240,8 +240,8 @@ int dd_run_host(dd_plan* plan, const void* h_input, void* h_output, void* stream
  * dedispered.cu:988-1304, blocks until its output is on the host); it serves
  * callers that stream chunk after chunk: one chunk's output copy (device to
  * host) overlaps the next chunk's input copy (host to device) and RFI stages,
- * and only the next chunk's sums wait for the copy of the output they
- * overwrite.  h_input may be reused once the call's input copy is done (the
+ * and each time tile's sums of the next chunk wait only for the copy of the
+ * output columns they overwrite.  h_input may be reused once the call's input copy is done (the
  * stream reaches it), h_output holds the result once dd_run_host_join has made
  * a stream wait for it and that stream has reached that point; pinned host
  * buffers are needed for the copies to overlap.  The calls of one plan must use
